@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Benchmark of the pointing-operator hot path (planned map2tod + tod2map) on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--ndet-rows R]
+
+Workload (default): the large plain GPU run -- 1024 detectors x 2^18 samples (nsamp = 2^28) of a
+synthetic raster scan (0.7 px/sample x sweep, 2e-4 px/sample y drift, 32x32 detector grid at 2 px)
+into a 3x8192x32768 periodic map whose LocalPixelization holds only the cells the scan hits.
+
+A step is one planned map2tod followed by one planned tod2map over all samples, with the plan built
+once beforehand and reused (the reference's plan-reuse loop).  value = samples processed by the
+step (per GPU, times the number of GPUs) / device time of the step, in Gsamples/s.  The 4 GiB of
+xpointing + TOD streamed per step is larger than L2, so no flush is needed between steps.
+
+Other numbers on the JSON line:
+  roofline     the dominant kernel's algorithmic bytes per launch / its CUDA-event duration, against
+               the measured HBM copy bandwidth (MEASURED_PEAKS.json)
+  e2e          the same metric through the public API from pinned HOST buffers: H2D of xpointing,
+               TOD and map, preplan + plan, map2tod, tod2map, D2H of the TOD and map results
+  cpu_baseline the reference's CPU operators (oracle/_ref: the reference header; else the oracle
+               port) on all host cores over a bounded prefix of the same workload
+  clocks       NVML SM clock samples during the timed region
+
+N > 1 (torchrun): every rank runs its own replica of the workload on its own GPU (weak scaling, no
+data-path collective); the step time is the max over ranks.  --impl reference runs the CPU
+reference on rank 0 only.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gsamples/s map2tod+tod2map, % HBM peak; batched/served vs plain at stated err"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--ndet-rows", type=int, default=32, help="detector rows (32 = full 2^28-sample workload)")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--only", default="", help="profiling aid: 'map2tod' or 'tod2map' runs only that operator")
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def workload_config(ndet_rows, nsamp, ncells, npix):
+    return {
+        "workload": f"raster scan {ndet_rows}x32 detectors x 2^18 samples (nsamp={nsamp}), map 3x8192x32768 "
+                    f"periodic, LocalPixelization = {ncells} hit cells (npix={npix})",
+        "nsamp_per_gpu": nsamp,
+        "step": "planned map2tod + planned tod2map, plan reused",
+        "l2": "no flush: inputs (16 B/sample streamed, > 126 MB L2) exceed L2",
+        "parallelism": "replicas (one TOD per GPU, weak scaling)",
+    }
+
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons with NVML while the timed region runs."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+        0x100: "display_clock_setting",
+    }
+
+    def __init__(self, device_index):
+        self.ok = False
+        self.samples, self.reasons = [], set()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+        self._stop = threading.Event()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nvml.nvmlDeviceGetClockInfo(self.h, self.nvml.NVML_CLOCK_SM))
+                r = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.02)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["nvml unavailable"]}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons - {"gpu_idle"}), "n_samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------------------------------------
+
+
+def cpu_reference_run(xp, tod, m, lp, nthreads, use_ref):
+    import numpy as np
+    import oracle
+    out_tod = np.zeros_like(tod)
+    out_map = np.zeros_like(m)
+    t0 = time.perf_counter()
+    e1 = oracle.map2tod_mt(out_tod, m, xp, lp, nthreads, use_ref=use_ref)
+    e2 = oracle.tod2map_mt(out_map, tod, xp, lp, nthreads, use_ref=use_ref)
+    dt = time.perf_counter() - t0
+    assert e1 == 0 and e2 == 0
+    return dt
+
+
+def cpu_sample(ndet, ndet_rows_cfg):
+    """The first 'ndet' detectors of the workload, on the host: xpointing, tod, map, oracle Lpix."""
+    import numpy as np
+    import torch
+    import oracle
+    from gpu_mm_b200 import synthetic
+    rows = max(1, ndet // 32)
+    xp = synthetic.raster_xpointing(rows, 32, 2 ** 18, 2.0, 0.7, 32768, 100.0, 2.0e-4, device="cpu").numpy()
+    xp = np.ascontiguousarray(xp[:, :ndet])
+    mt, _, err = oracle.plan(xp, 8192, 32768, True)
+    cells = sorted({(int(c) >> 10, int(c) & 1023) for c in np.unique(mt & np.uint64(0xFFFFF))})
+    offs = np.full((128, 512), -1, dtype=np.int64)
+    for i, (a, b) in enumerate(cells):
+        offs[a, b] = 3 * 4096 * i
+    lp = oracle.Lpix(8192, 32768, offs, 64, 4096, True)
+    g = torch.Generator().manual_seed(0)
+    m = torch.randn(3 * lp.npix, generator=g).numpy()
+    tod = torch.randn(xp.shape[1:], generator=g).numpy()
+    return xp, tod, m, lp
+
+
+def cpu_baseline(ndet_rows):
+    import oracle
+    use_ref = oracle.ref_available()
+    nthreads = os.cpu_count() or 1
+    ndet = 64
+    xp, tod, m, lp = cpu_sample(ndet, ndet_rows)
+    nsamp = xp.size // 3
+    cpu_reference_run(xp, tod, m, lp, nthreads, use_ref)   # warm
+    dt = min(cpu_reference_run(xp, tod, m, lp, nthreads, use_ref) for _ in range(3))
+    return {"value": round(nsamp / dt / 1e9, 4), "unit": "Gsamples/s", "cores": nthreads,
+            "kind": "reference" if use_ref else "port",
+            "sample": f"first {ndet} detectors ({nsamp} samples) of the workload, map2tod + tod2map, "
+                      f"best of 3, {nthreads} threads"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    use_ref = oracle.ref_available()
+    nthreads = os.cpu_count() or 1
+    ndet = 16
+    xp, tod, m, lp = cpu_sample(ndet, args.ndet_rows)
+    nsamp = xp.size // 3
+    for _ in range(args.warmup):
+        cpu_reference_run(xp, tod, m, lp, nthreads, use_ref)
+    times = [cpu_reference_run(xp, tod, m, lp, nthreads, use_ref) for _ in range(args.steps)]
+    dt = sum(times) / len(times)
+    value = nsamp / dt / 1e9
+    kind = "reference" if use_ref else "port"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Gsamples/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args.ndet_rows, 2 ** 18 * 32 * args.ndet_rows, len(lp.cell_offsets[lp.cell_offsets >= 0]), lp.npix)
+        | {"reference_sample": f"first {ndet} detectors ({nsamp} samples) per step"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Gsamples/s", "cores": nthreads, "kind": kind,
+                         "sample": f"first {ndet} detectors ({nsamp} samples) per step, map2tod + tod2map, "
+                                   f"{nthreads} threads"},
+        "e2e": {"value": round(value, 4), "unit": "Gsamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    import gpu_mm_b200 as g
+    from gpu_mm_b200 import synthetic
+    peak, peak_kind = measured_peaks()
+
+    # ---- workload (per rank: its own replica) ----
+    xp = synthetic.raster_xpointing(args.ndet_rows, 32, 2 ** 18, 2.0, 0.7, 32768, 100.0 + rank, 2.0e-4, device="cuda")
+    nsamp = xp.numel() // 3
+    ny, nx = 8192, 32768
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pp = g.PointingPrePlan(xp, ny, nx)
+    plan = g.PointingPlan(pp, xp)
+    torch.cuda.synchronize()
+    first_plan_s = time.perf_counter() - t0
+    cells = synthetic.cells_of_plan(plan.get_plan_mt())
+    lp = g.LocalPixelization.make_cells(ny, nx, cells)
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    lmap = g.LocalMap(lp, torch.randn(3 * lp.npix, generator=gen, device="cuda"))
+    tod_in = torch.randn(xp.shape[1:], generator=gen, device="cuda")
+    tod_out = torch.empty_like(tod_in)
+    map_out = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+    err_a = torch.zeros(1, dtype=torch.int32, device="cuda")
+    err_b = torch.zeros(1, dtype=torch.int32, device="cuda")
+    m = g.gpu_mm_pybind11
+
+    # Plan build timing (preplan + plan into preallocated buffers), reused below.
+    buf = torch.empty(pp.plan_nbytes, dtype=torch.uint8, device="cuda")
+    tmp = torch.empty(pp.plan_constructor_tmp_nbytes, dtype=torch.uint8, device="cuda")
+    nmt_buf = torch.empty(1024, dtype=torch.int32, device="cuda")
+    pbuf = torch.empty(1024, dtype=torch.int32, device="cuda")
+    plan_ms = []
+    for i in range(4):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        pp2 = g.PointingPrePlan(xp, ny, nx, buf=nmt_buf, tmp_buf=pbuf)
+        g.PointingPlan(pp2, xp, buf=buf, tmp_buf=tmp)
+        e1.record()
+        torch.cuda.synchronize()
+        if i > 0:
+            plan_ms.append(e0.elapsed_time(e1))
+
+    do_m2t = args.only in ("", "map2tod")
+    do_t2m = args.only in ("", "tod2map")
+
+    def step(evs=None):
+        if evs is not None:
+            evs[0].record()
+        if do_m2t:
+            m.planned_map2tod_async(tod_out, lmap.arr, xp, lp, plan, False, False, err_a, 0)
+        if evs is not None:
+            evs[1].record()
+        if do_t2m:
+            m.planned_tod2map_async(map_out.arr, tod_in, xp, lp, plan, False, err_b, 0)
+        if evs is not None:
+            evs[2].record()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    m.check_errword(err_a, 0, 0)
+    m.check_errword(err_b, 0, 0)
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        start.record()
+        for k in range(args.steps):
+            step(evs[k])
+        stop.record()
+        torch.cuda.synchronize()
+    barrier()
+    m.check_errword(err_a, 0, 0)
+    m.check_errword(err_b, 0, 0)
+    ms_step = max_over_ranks(start.elapsed_time(stop) / args.steps)
+    m2t_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    t2m_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+
+    npix = lp.npix
+    m2t_bytes = 16 * nsamp + 12 * npix
+    t2m_bytes = 16 * nsamp + 24 * npix
+    dom = "tod2map" if t2m_ms >= m2t_ms else "map2tod"
+    dom_ms, dom_bytes = (t2m_ms, t2m_bytes) if dom == "tod2map" else (m2t_ms, m2t_bytes)
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"{'planned_tod2map' if dom == 'tod2map' else 'planned_map2tod'}_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            td = json.load(f)
+        traffic = int(td["bytes_per_sample"] * nsamp + td.get("bytes_per_pixel", 0) * npix)
+
+    # Unplanned operators (for context).
+    unplanned = {}
+    for name, fn in (("unplanned_map2tod_ms", lambda: m.unplanned_map2tod_async(tod_out, lmap.arr, xp, lp, False, False, err_a, 0)),
+                     ("unplanned_tod2map_ms", lambda: m.unplanned_tod2map_async(map_out.arr, tod_in, xp, lp, False, err_b, 0))):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        unplanned[name] = round(e0.elapsed_time(e1) / 3, 4)
+
+    # ---- e2e through the public API from pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        xp_h = torch.empty(xp.shape, dtype=torch.float32, pin_memory=True)
+        xp_h.copy_(xp)
+        tod_h = torch.empty(tod_in.shape, dtype=torch.float32, pin_memory=True)
+        tod_h.copy_(tod_in)
+        map_h = torch.empty(3 * npix, dtype=torch.float32, pin_memory=True)
+        map_h.copy_(lmap.arr)
+        tod_out_h = torch.empty_like(tod_h, pin_memory=True)
+        map_out_h = torch.empty_like(map_h, pin_memory=True)
+        xp_d = torch.empty_like(xp)
+        tod_d = torch.empty_like(tod_in)
+        map_d = torch.empty(3 * npix, dtype=torch.float32, device="cuda")
+        out_tod_d = torch.empty_like(tod_in)
+        out_map_d = torch.empty(3 * npix, dtype=torch.float32, device="cuda")
+
+        def e2e_step():
+            xp_d.copy_(xp_h, non_blocking=True)
+            tod_d.copy_(tod_h, non_blocking=True)
+            map_d.copy_(map_h, non_blocking=True)
+            pre = g.PointingPrePlan(xp_d, ny, nx, buf=nmt_buf, tmp_buf=pbuf)
+            pl = g.PointingPlan(pre, xp_d, buf=buf, tmp_buf=tmp)
+            g.map2tod(out_tod_d, g.LocalMap(lp, map_d), xp_d, pl)
+            out_map_d.zero_()
+            g.tod2map(g.LocalMap(lp, out_map_d), tod_d, xp_d, pl)
+            tod_out_h.copy_(out_tod_d, non_blocking=True)
+            map_out_h.copy_(out_map_d, non_blocking=True)
+
+        for _ in range(min(args.warmup, 3)):
+            e2e_step()
+        torch.cuda.synchronize()
+        ke = max(1, min(args.steps, 5))
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(ke):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / ke)
+        assert np.allclose(tod_out_h[0, :64].numpy(), tod_out[0, :64].cpu().numpy(), rtol=1e-5, atol=1e-5)
+        hb = 4 * (xp.numel() + tod_in.numel() + 3 * npix)
+        db = 4 * (tod_in.numel() + 3 * npix)
+        e2e = {"value": round(world * nsamp / (e2e_ms * 1e-3) / 1e9, 4), "unit": "Gsamples/s",
+               "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db, "ms_per_step": round(e2e_ms, 3),
+               "includes": "H2D xpointing+tod+map, preplan+plan, map2tod, tod2map, D2H tod+map"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.ndet_rows)
+
+    if rank == 0:
+        value = world * nsamp / (ms_step * 1e-3) / 1e9
+        step_bytes = (m2t_bytes if do_m2t else 0) + (t2m_bytes if do_t2m else 0)
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Gsamples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": workload_config(args.ndet_rows, nsamp, len(cells), npix),
+            "pct_hbm_peak_step": round(100 * step_bytes / (ms_step * 1e-3) / 1e9 / peak, 2),
+            "roofline": {"bound": "hbm", "kernel": f"planned_{dom}", "achieved": round(achieved, 1),
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+                         "per_unit": "16 B/sample + 12 B/hit pixel (map2tod) or 24 B/hit pixel (tod2map)"},
+            "kernels_ms": {"planned_map2tod": round(m2t_ms, 4), "planned_tod2map": round(t2m_ms, 4),
+                           **unplanned, "plan_build": round(statistics.mean(plan_ms), 4),
+                           "first_plan_build_s": round(first_plan_s, 3)},
+            "plan": {"nmt": int(pp.plan_nmt), "overhead": round(pp.overhead, 4), "sort_digit_bits": pp.sort_digit_bits},
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "gpu_launches": args.steps * (int(do_m2t) + int(do_t2m)),
+        }
+        print(json.dumps(line), flush=True)
+
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,130 @@
+// Device building blocks shared by the gpu_mm_b200 kernels (sm_100a).
+//
+// The per-sample arithmetic restates the reference's pixel_locator / cell_enumerator
+// (kmsmith137/gpu_mm include/gpu_mm_internals.hpp:104-237); the rest is this implementation's own.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gmm {
+
+constexpr uint32_t kErrBadYpix = 0x1;
+constexpr uint32_t kErrBadXpix = 0x2;
+constexpr uint32_t kErrInconsistentNmt = 0x4;
+constexpr uint32_t kErrNotInPixelization = 0x8;
+constexpr unsigned kFullMask = 0xffffffffu;
+
+// mt word layout (PointingPlan.cu:75-80): bits 0-9 ixcell, 10-19 iycell, 20-45 cache line,
+// 46 mflag (line touches more than one cell), 47 zflag.
+constexpr int kCellBits = 20;
+constexpr uint64_t kCellMask = (1ull << 20) - 1;
+constexpr uint64_t kClMask = (1ull << 26) - 1;
+constexpr uint64_t kMflag = 1ull << 46;
+constexpr uint64_t kZflag = 1ull << 47;
+
+struct Located {
+    int iy0, iy1, ix0, ix1;
+    float dy, dx;
+};
+
+// pixel_locator<float>::locate (gpu_mm_internals.hpp:124-164): global pixel coordinates of the
+// four bilinear neighbours.  Bad coordinates set error bits but still give in-range indices.
+__device__ __forceinline__ uint32_t locate(float ypix, float xpix, int ny, int nx, bool periodic, Located &L)
+{
+    uint32_t err = 0;
+    int y0 = int(ypix);
+    y0 = max(y0, 0);
+    y0 = min(y0, ny - 2);
+    L.iy0 = y0;
+    L.iy1 = y0 + 1;
+    L.dy = ypix - float(y0);
+    bool yvalid = (ypix >= 0.0f) && (ypix <= float(ny - 1));
+    err |= yvalid ? 0u : kErrBadYpix;
+
+    if (periodic) {
+        bool xvalid = (xpix >= float(-nx)) && (xpix <= float(2 * nx));
+        err |= xvalid ? 0u : kErrBadXpix;
+        xpix = (xpix >= 0.0f) ? xpix : (xpix + float(nx));
+        xpix = (xpix <= float(nx)) ? xpix : (xpix - float(nx));
+        int x0 = int(xpix);
+        x0 = max(x0, 0);
+        L.dx = xpix - float(x0);
+        x0 = (x0 < nx) ? x0 : 0;
+        int x1 = x0 + 1;
+        L.ix0 = x0;
+        L.ix1 = (x1 < nx) ? x1 : 0;
+    } else {
+        bool xvalid = (xpix >= 0.0f) && (xpix <= float(nx - 2));
+        err |= xvalid ? 0u : kErrBadXpix;
+        int x0 = int(xpix);
+        x0 = max(x0, 0);
+        x0 = min(x0, nx - 2);
+        L.ix0 = x0;
+        L.ix1 = x0 + 1;
+        L.dx = xpix - float(x0);
+    }
+    return err;
+}
+
+// The six cell "slots" of a sample, restating cell_enumerator::enumerate
+// (gpu_mm_internals.hpp:194-236) as a function of cell value: y-slot = iycell parity; x-slot 0 =
+// even non-zero ixcell, 1 = odd, 2 = ixcell 0.  Slot k = 3*yslot + xslot is in the order
+// ca0..ca5 of PointingPlan.cu:173-178.  Empty slots hold -1; filled ones (iycell << 10) | ixcell.
+__device__ __forceinline__ void cell_slots(const Located &L, int slots[6])
+{
+    int iyc0 = L.iy0 >> 6, iyc1 = L.iy1 >> 6;
+    int ixc0 = L.ix0 >> 6, ixc1 = L.ix1 >> 6;
+    bool ysame = (iyc0 == iyc1);
+    bool xsame = (ixc0 == ixc1);
+    int yc[2], xc[3];
+    // y-cells are consecutive (iy1 = iy0+1), so the two have opposite parities.
+    yc[0] = (iyc0 & 1) ? (ysame ? -1 : iyc1) : iyc0;
+    yc[1] = (iyc0 & 1) ? iyc0 : (ysame ? -1 : iyc1);
+    int xs0 = (ixc0 == 0) ? 2 : (ixc0 & 1);
+    int xs1 = (ixc1 == 0) ? 2 : (ixc1 & 1);
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+        xc[b] = (xs0 == b) ? ixc0 : ((!xsame && (xs1 == b)) ? ixc1 : -1);
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+            slots[3 * a + b] = ((yc[a] >= 0) && (xc[b] >= 0)) ? ((yc[a] << 10) | xc[b]) : -1;
+}
+
+// Per-slot warp analysis of one 32-sample cache line (the role of cell_analysis,
+// PointingPlan.cu:19-37): amask[k] has one bit per distinct valid cell of slot k, at the lowest
+// lane holding it.
+__device__ __forceinline__ void line_slot_masks(const int slots[6], unsigned amask[6])
+{
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        unsigned peers = __match_any_sync(kFullMask, (unsigned) slots[k]);
+        bool lowest = (peers & lt) == 0;
+        amask[k] = __ballot_sync(kFullMask, lowest && (slots[k] >= 0));
+    }
+}
+
+__device__ __forceinline__ float ldcs(const float *p) { return __ldcs(p); }
+
+// OR-reduce an error word over the block and publish it with one atomicOr per block (only if
+// non-zero).  'scratch' needs blockDim.x/32 words; must be called by all threads of the block.
+__device__ __forceinline__ void block_publish_err(uint32_t err, uint32_t *scratch, uint32_t *errword)
+{
+    err = __reduce_or_sync(kFullMask, err);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    if (lane == 0)
+        scratch[warp] = err;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t e = (lane < nwarps) ? scratch[lane] : 0u;
+        e = __reduce_or_sync(kFullMask, e);
+        if ((lane == 0) && (e != 0))
+            atomicOr(errword, e);
+    }
+}
+
+}  // namespace gmm

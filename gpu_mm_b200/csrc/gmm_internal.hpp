@@ -1,0 +1,52 @@
+// Internal declarations shared by the gpu_mm_b200 translation units.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "gmm_common.cuh"
+#include "../../include/gpu_mm_b200.h"
+
+namespace gmm {
+
+// Number of SMs of the current device (cached per device).
+int device_sm_count();
+
+// ---- plan construction (plan_kernels.cu) ----
+int sort_passes(int nycells_max, int nxcells_max, int max_digit_bits, int *digit_bits);
+int64_t sort_scratch_nbytes(int digit_bits, int grid);
+int sort_grid_for(int64_t n);
+cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, int nxcells_max, int digit_bits,
+                          int npasses, uint32_t *hist, cudaStream_t stream);
+cudaError_t launch_preplan(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
+                           int nblocks, uint32_t *nmt, uint32_t *err, cudaStream_t stream);
+cudaError_t launch_plan_emit(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
+                             int nblocks, const uint32_t *nmt_cumsum, uint64_t *mt_out, uint64_t *owner_out,
+                             uint32_t *errflags, cudaStream_t stream);
+cudaError_t launch_expand_dynamic_map(uint32_t *global_ncells, int64_t *cell_offsets, int nycells, int nxcells,
+                                      const uint64_t *plan_mt, int64_t nmt, cudaStream_t stream);
+
+// ---- operators (operator_kernels.cu) ----
+struct OpArgs {
+    float *out;             // tod (map2tod) or local map (tod2map)
+    const float *in;        // local map (map2tod) or tod (tod2map)
+    const float *xp;        // xpointing [3][nsamp]
+    const float *response;  // [2][ndet] or nullptr
+    int64_t ndet, nperdet;
+    const int64_t *cell_offsets;
+    int64_t nsamp;
+    int ny, nx;
+    bool periodic;
+    int nycells, nxcells;
+    int64_t ystride, polstride;
+    bool partial, accum;
+    uint32_t *errword;
+};
+
+cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream);
+cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream);
+cudaError_t launch_unplanned_map2tod(const OpArgs &a, cudaStream_t stream);
+cudaError_t launch_unplanned_tod2map(const OpArgs &a, cudaStream_t stream);
+
+}  // namespace gmm

@@ -1,0 +1,519 @@
+// Pointing operators on sm_100a: planned and unplanned map2tod / tod2map (+ response variants).
+//
+// Semantics follow the reference CPU operators (kmsmith137/gpu_mm src_lib/map2tod_reference.cu:16-54,
+// tod2map_reference.cu:14-46) and the planned GPU ones (map2tod.cu, tod2map.cu, map2tod_response.cu,
+// tod2map_response.cu): bilinear T/Q/U interpolation with the cos 2a / sin 2a response, cells of
+// 64x64 pixels addressed through cell_offsets, and x-wraparound.
+//
+// Planned design (this implementation's own):
+//  * Every 32-sample cache line is processed exactly once, by the CTA that holds its "owner" cell
+//    (the lowest cell the line touches).  The plan carries that owner list sorted by cell, so a CTA
+//    walks a contiguous slice of it and reloads its tile only when the cell changes.
+//  * The tile is the owner cell plus a halo: rows [0, 64+HY) and columns [-HX, 64+HX) around the
+//    cell, in unwrapped x.  A line's whole bilinear footprint normally fits, so no cache line is
+//    read twice, no TOD word needs an atomic, and no pre-zeroing pass is needed.  Samples that do not
+//    fit take an exact fallback through global memory.
+//  * map2tod stages the tile (T, Q, U planes, padded row stride) from global memory; tod2map
+//    accumulates into it with shared-memory atomics and flushes each tile to the map once, skipping
+//    all-zero pixels.
+//  * xpointing and TOD are streamed with evict-first loads/stores so that the map and plan stay in
+//    L2; each warp keeps UNR cache lines in flight.
+#include <algorithm>
+
+#include "gmm_internal.hpp"
+
+namespace gmm {
+
+namespace {
+
+constexpr int HX = 32;                 // halo columns on each side
+constexpr int HY = 4;                  // halo rows below the cell
+constexpr int TY = 64 + HY;            // tile rows
+constexpr int TX = 64 + 2 * HX;        // tile columns (multiple of 32)
+constexpr int TS = TX + 1;             // padded row stride in shared memory
+constexpr int PS = TY * TS;            // one polarisation plane
+constexpr int NW = 16;                 // warps per CTA
+constexpr int NT = NW * 32;
+constexpr int CH = 512;                // owner entries staged per chunk
+constexpr int UNR = 4;                 // cache lines in flight per warp
+constexpr int NPRES = TY * TX / 32;    // presence bitmap words
+constexpr size_t kTileBytes = 3 * (size_t) PS * sizeof(float);
+
+static_assert(TX % 32 == 0, "presence bitmap rows must be whole words");
+static_assert((TY * TX) % NT == 0, "tile sweep must cover whole warps");
+
+struct Tile {
+    int gy0;   // global row of tile row 0
+    int gx0;   // unwrapped global column of tile column 0
+};
+
+__device__ __forceinline__ int64_t tile_pixel_offset(int r, int c, const Tile &T, const OpArgs &a)
+{
+    const int gy = T.gy0 + r;
+    int gx = T.gx0 + c;
+    if (a.periodic) {
+        gx %= a.nx;
+        gx += (gx < 0) ? a.nx : 0;
+    }
+    if ((gx < 0) || (gy >= 64 * a.nycells) || (gx >= 64 * a.nxcells))
+        return -1;
+    const int64_t off = __ldg(a.cell_offsets + (int64_t) (gy >> 6) * a.nxcells + (gx >> 6));
+    if (off < 0)
+        return -1;
+    return off + (int64_t) (gy & 63) * a.ystride + (gx & 63);
+}
+
+// Global-memory pixel offset (map_evaluator / map_accumulator addressing,
+// gpu_mm_internals.hpp:258-275), or -1 if the cell is absent.
+__device__ __forceinline__ int64_t global_pixel_offset(int iy, int ix, const OpArgs &a)
+{
+    const int iyc = iy >> 6, ixc = ix >> 6;
+    if ((iyc >= a.nycells) || (ixc >= a.nxcells))
+        return -1;
+    const int64_t off = __ldg(a.cell_offsets + (int64_t) iyc * a.nxcells + ixc);
+    if (off < 0)
+        return -1;
+    return off + (int64_t) (iy & 63) * a.ystride + (ix & 63);
+}
+
+__device__ __forceinline__ bool present_bit(const uint32_t *pres, int r, int c)
+{
+    return (pres[r * (TX / 32) + (c >> 5)] >> (c & 31)) & 1u;
+}
+
+// Per-sample response factors: (t_resp, p_resp) for the detector of sample s
+// (map2tod_response.cu:168-176).
+template<bool RESP>
+__device__ __forceinline__ void sample_response(const OpArgs &a, int64_t s, float &tr, float &pr)
+{
+    if constexpr (RESP) {
+        const int64_t det = s / a.nperdet;
+        tr = __ldg(a.response + det);
+        pr = __ldg(a.response + det + a.ndet);
+    } else {
+        tr = 1.0f;
+        pr = 1.0f;
+    }
+}
+
+// Fills (map2tod) or clears (tod2map) the tile for cell 'cell' and its presence bitmap.
+template<bool LOAD>
+__device__ void prepare_tile(float *tile, uint32_t *pres, int *s_absent, uint32_t cell, Tile &T, const OpArgs &a,
+                             const float *__restrict__ lmap)
+{
+    const int iyc = (int) (cell >> 10), ixc = (int) (cell & 1023u);
+    T.gy0 = iyc << 6;
+    T.gx0 = (ixc << 6) - HX;
+    const int lane = threadIdx.x & 31;
+    bool any_absent = false;
+    for (int idx = threadIdx.x; idx < TY * TX; idx += NT) {
+        const int r = idx / TX, c = idx % TX;
+        const int64_t off = tile_pixel_offset(r, c, T, a);
+        const bool p = off >= 0;
+        if constexpr (LOAD) {
+            const float t = p ? __ldg(lmap + off) : 0.0f;
+            const float q = p ? __ldg(lmap + off + a.polstride) : 0.0f;
+            const float u = p ? __ldg(lmap + off + 2 * a.polstride) : 0.0f;
+            float *dst = tile + r * TS + c;
+            dst[0] = t;
+            dst[PS] = q;
+            dst[2 * PS] = u;
+        }
+        const unsigned bal = __ballot_sync(kFullMask, p);
+        if (lane == 0)
+            pres[idx >> 5] = bal;
+        any_absent |= !p;
+    }
+    if (__any_sync(kFullMask, any_absent) && (lane == 0))
+        *s_absent = 1;
+}
+
+// Adds the tile into the map (one atomic per non-zero pixel and polarisation) and clears it.
+__device__ void flush_tile(float *tile, const Tile &T, const OpArgs &a, float *__restrict__ lmap)
+{
+    for (int idx = threadIdx.x; idx < TY * TX; idx += NT) {
+        const int r = idx / TX, c = idx % TX;
+        float *src = tile + r * TS + c;
+        const float t = src[0], q = src[PS], u = src[2 * PS];
+        if ((t != 0.0f) || (q != 0.0f) || (u != 0.0f)) {
+            const int64_t off = tile_pixel_offset(r, c, T, a);
+            if (off >= 0) {
+                atomicAdd(lmap + off, t);
+                atomicAdd(lmap + off + a.polstride, q);
+                atomicAdd(lmap + off + 2 * a.polstride, u);
+            }
+            src[0] = 0.0f;
+            src[PS] = 0.0f;
+            src[2 * PS] = 0.0f;
+        }
+    }
+}
+
+// Position of a located sample inside the tile; false if its footprint is not inside.
+__device__ __forceinline__ bool tile_position(const Located &L, const Tile &T, const OpArgs &a, int &ry, int &rx)
+{
+    ry = L.iy0 - T.gy0;
+    rx = L.ix0 - T.gx0;
+    if (a.periodic) {
+        rx += (rx < 0) ? a.nx : 0;
+        rx -= (rx > TX - 2) ? a.nx : 0;
+    }
+    return ((unsigned) ry <= (unsigned) (TY - 2)) && ((unsigned) rx <= (unsigned) (TX - 2));
+}
+
+__device__ __forceinline__ float global_eval(const OpArgs &a, const float *__restrict__ lmap, int iy, int ix,
+                                             float ct, float cq, float cu, uint32_t &err)
+{
+    const int64_t off = global_pixel_offset(iy, ix, a);
+    const bool valid = off >= 0;
+    const float t = valid ? __ldg(lmap + off) : 0.0f;
+    const float q = valid ? __ldg(lmap + off + a.polstride) : 0.0f;
+    const float u = valid ? __ldg(lmap + off + 2 * a.polstride) : 0.0f;
+    err |= (valid || a.partial) ? 0u : kErrNotInPixelization;
+    return ct * t + cq * q + cu * u;
+}
+
+__device__ __forceinline__ void global_accum(const OpArgs &a, float *__restrict__ lmap, int iy, int ix,
+                                             float t, float q, float u, float w, uint32_t &err)
+{
+    const int64_t off = global_pixel_offset(iy, ix, a);
+    const bool valid = off >= 0;
+    if (valid) {
+        atomicAdd(lmap + off, w * t);
+        atomicAdd(lmap + off + a.polstride, w * q);
+        atomicAdd(lmap + off + 2 * a.polstride, w * u);
+    }
+    err |= (valid || a.partial) ? 0u : kErrNotInPixelization;
+}
+
+// One sample of map2tod against the staged tile (or global memory if it does not fit).
+template<bool RESP>
+__device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, const uint32_t *pres, bool check,
+                                            const Tile &T, float y, float x, float al, int64_t s, uint32_t &err)
+{
+    Located L;
+    err |= locate(y, x, a.ny, a.nx, a.periodic, L);
+    float sn, cs;
+    sincosf(2.0f * al, &sn, &cs);
+    float ct = 1.0f, cq = cs, cu = sn;
+    if constexpr (RESP) {
+        float tr, pr;
+        sample_response<true>(a, s, tr, pr);
+        ct = tr;
+        cq = pr * cs;
+        cu = pr * sn;
+    }
+    int ry, rx;
+    float e00, e01, e10, e11;
+    if (tile_position(L, T, a, ry, rx)) {
+        const float *p = tile + ry * TS + rx;
+        if constexpr (RESP) {
+            e00 = ct * p[0] + cq * p[PS] + cu * p[2 * PS];
+            e01 = ct * p[1] + cq * p[PS + 1] + cu * p[2 * PS + 1];
+            e10 = ct * p[TS] + cq * p[PS + TS] + cu * p[2 * PS + TS];
+            e11 = ct * p[TS + 1] + cq * p[PS + TS + 1] + cu * p[2 * PS + TS + 1];
+        } else {
+            e00 = p[0] + cq * p[PS] + cu * p[2 * PS];
+            e01 = p[1] + cq * p[PS + 1] + cu * p[2 * PS + 1];
+            e10 = p[TS] + cq * p[PS + TS] + cu * p[2 * PS + TS];
+            e11 = p[TS + 1] + cq * p[PS + TS + 1] + cu * p[2 * PS + TS + 1];
+        }
+        if (check) {
+            const bool ok = present_bit(pres, ry, rx) && present_bit(pres, ry, rx + 1) &&
+                            present_bit(pres, ry + 1, rx) && present_bit(pres, ry + 1, rx + 1);
+            err |= ok ? 0u : kErrNotInPixelization;
+        }
+    } else {
+        e00 = global_eval(a, a.in, L.iy0, L.ix0, ct, cq, cu, err);
+        e01 = global_eval(a, a.in, L.iy0, L.ix1, ct, cq, cu, err);
+        e10 = global_eval(a, a.in, L.iy1, L.ix0, ct, cq, cu, err);
+        e11 = global_eval(a, a.in, L.iy1, L.ix1, ct, cq, cu, err);
+    }
+    const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
+    float r = (wy0 * wx0) * e00;
+    r += (wy0 * L.dx) * e01;
+    r += (L.dy * wx0) * e10;
+    r += (L.dy * L.dx) * e11;
+    return r;
+}
+
+template<bool RESP>
+__device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const uint32_t *pres, bool check,
+                                           const Tile &T, float y, float x, float al, float tv, int64_t s,
+                                           uint32_t &err)
+{
+    Located L;
+    err |= locate(y, x, a.ny, a.nx, a.periodic, L);
+    float sn, cs;
+    sincosf(2.0f * al, &sn, &cs);
+    float t, q, u;
+    if constexpr (RESP) {
+        float tr, pr;
+        sample_response<true>(a, s, tr, pr);
+        t = tr * tv;
+        q = pr * tv * cs;
+        u = pr * tv * sn;
+    } else {
+        t = tv;
+        q = tv * cs;
+        u = tv * sn;
+    }
+    const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
+    const float w00 = wy0 * wx0, w01 = wy0 * L.dx, w10 = L.dy * wx0, w11 = L.dy * L.dx;
+    int ry, rx;
+    if (tile_position(L, T, a, ry, rx)) {
+        float *p = tile + ry * TS + rx;
+        atomicAdd(p, w00 * t);
+        atomicAdd(p + PS, w00 * q);
+        atomicAdd(p + 2 * PS, w00 * u);
+        atomicAdd(p + 1, w01 * t);
+        atomicAdd(p + PS + 1, w01 * q);
+        atomicAdd(p + 2 * PS + 1, w01 * u);
+        atomicAdd(p + TS, w10 * t);
+        atomicAdd(p + PS + TS, w10 * q);
+        atomicAdd(p + 2 * PS + TS, w10 * u);
+        atomicAdd(p + TS + 1, w11 * t);
+        atomicAdd(p + PS + TS + 1, w11 * q);
+        atomicAdd(p + 2 * PS + TS + 1, w11 * u);
+        if (check) {
+            const bool ok = present_bit(pres, ry, rx) && present_bit(pres, ry, rx + 1) &&
+                            present_bit(pres, ry + 1, rx) && present_bit(pres, ry + 1, rx + 1);
+            err |= ok ? 0u : kErrNotInPixelization;
+        }
+    } else {
+        global_accum(a, a.out, L.iy0, L.ix0, t, q, u, w00, err);
+        global_accum(a, a.out, L.iy0, L.ix1, t, q, u, w01, err);
+        global_accum(a, a.out, L.iy1, L.ix0, t, q, u, w10, err);
+        global_accum(a, a.out, L.iy1, L.ix1, t, q, u, w11, err);
+    }
+}
+
+// Planned operator kernel.  TOD2MAP selects the direction; RESP the per-detector response.
+template<bool TOD2MAP, bool RESP>
+__global__ void __launch_bounds__(NT, 2)
+planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner)
+{
+    extern __shared__ float tile[];
+    __shared__ uint32_t pres[NPRES];
+    __shared__ uint64_t s_mt[CH];
+    __shared__ int s_absent;
+    __shared__ uint32_t s_err[NW];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t e0 = (nowner * (int64_t) blockIdx.x) / gridDim.x;
+    const int64_t e1 = (nowner * (int64_t) (blockIdx.x + 1)) / gridDim.x;
+    const int64_t nsamp = a.nsamp;
+    uint32_t err = 0;
+    uint32_t cur = 0xffffffffu;
+    Tile T{0, 0};
+
+    if constexpr (TOD2MAP) {
+        for (int i = threadIdx.x; i < 3 * PS; i += NT)
+            tile[i] = 0.0f;
+    }
+
+    for (int64_t c0 = e0; c0 < e1; c0 += CH) {
+        const int n = (int) ((e1 - c0 < (int64_t) CH) ? (e1 - c0) : (int64_t) CH);
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += NT)
+            s_mt[i] = __ldg(owner_mt + c0 + i);
+        __syncthreads();
+
+        int i = 0;
+        while (i < n) {
+            const uint32_t cell = (uint32_t) (s_mt[i] & kCellMask);
+            int lo = i + 1, hi = n;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if ((uint32_t) (s_mt[mid] & kCellMask) == cell) lo = mid + 1; else hi = mid;
+            }
+            const int j = lo;
+
+            if (cell != cur) {
+                __syncthreads();
+                if constexpr (TOD2MAP) {
+                    if (cur != 0xffffffffu)
+                        flush_tile(tile, T, a, a.out);
+                }
+                if (threadIdx.x == 0)
+                    s_absent = 0;
+                __syncthreads();
+                prepare_tile<!TOD2MAP>(tile, pres, &s_absent, cell, T, a, a.in);
+                __syncthreads();
+                cur = cell;
+            }
+            const bool check = (s_absent != 0) && !a.partial;
+
+            for (int base = i + warp * UNR; base < j; base += NW * UNR) {
+                float y[UNR], x[UNR], al[UNR], tv[UNR];
+                int64_t s[UNR];
+                bool ok[UNR];
+#pragma unroll
+                for (int u = 0; u < UNR; u++) {
+                    const int k = min(base + u, j - 1);
+                    int64_t line = (int64_t) ((s_mt[k] >> 20) & kClMask);
+                    // A plan word always names a line < nsamp/32; anything else means the plan does not
+                    // belong to this xpointing, so flag it and read line 0 instead of out of range.
+                    ok[u] = (32 * line < nsamp) && (base + u < j);
+                    err |= (32 * line < nsamp) ? 0u : kErrInconsistentNmt;
+                    line = (32 * line < nsamp) ? line : 0;
+                    s[u] = 32 * line + lane;
+                    y[u] = __ldcs(a.xp + s[u]);
+                    x[u] = __ldcs(a.xp + nsamp + s[u]);
+                    al[u] = __ldcs(a.xp + 2 * nsamp + s[u]);
+                    if constexpr (TOD2MAP)
+                        tv[u] = __ldcs(a.in + s[u]);
+                    else
+                        tv[u] = a.accum ? a.out[s[u]] : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < UNR; u++) {
+                    if (!ok[u])
+                        continue;
+                    if constexpr (TOD2MAP) {
+                        t2m_sample<RESP>(a, tile, pres, check, T, y[u], x[u], al[u], tv[u], s[u], err);
+                    } else {
+                        const float r = m2t_sample<RESP>(a, tile, pres, check, T, y[u], x[u], al[u], s[u], err);
+                        __stcs(a.out + s[u], a.accum ? (tv[u] + r) : r);
+                    }
+                }
+            }
+            i = j;
+        }
+    }
+
+    if constexpr (TOD2MAP) {
+        __syncthreads();
+        if (cur != 0xffffffffu)
+            flush_tile(tile, T, a, a.out);
+    }
+    block_publish_err(err, s_err, a.errword);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Unplanned operators (map2tod_unplanned.cu:17-71, tod2map_unplanned.cu:17-66): one pass over the
+// samples, map accesses straight to global memory.  Four consecutive samples per thread with
+// 16-byte loads when the arrays are aligned.
+
+template<bool TOD2MAP, int V>
+__global__ void __launch_bounds__(256)
+unplanned_kernel(OpArgs a)
+{
+    __shared__ uint32_t s_err[8];
+    uint32_t err = 0;
+    const int64_t nvec = a.nsamp / V;
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t v = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; v < nvec; v += stride) {
+        const int64_t s0 = v * V;
+        float y[V], x[V], al[V], tv[V], r[V];
+        if constexpr (V == 4) {
+            const float4 yy = __ldcs(reinterpret_cast<const float4 *>(a.xp + s0));
+            const float4 xx = __ldcs(reinterpret_cast<const float4 *>(a.xp + a.nsamp + s0));
+            const float4 aa = __ldcs(reinterpret_cast<const float4 *>(a.xp + 2 * a.nsamp + s0));
+            y[0] = yy.x; y[1] = yy.y; y[2] = yy.z; y[3] = yy.w;
+            x[0] = xx.x; x[1] = xx.y; x[2] = xx.z; x[3] = xx.w;
+            al[0] = aa.x; al[1] = aa.y; al[2] = aa.z; al[3] = aa.w;
+            if (TOD2MAP || a.accum) {
+                const float4 tt = TOD2MAP ? __ldcs(reinterpret_cast<const float4 *>(a.in + s0))
+                                          : *reinterpret_cast<const float4 *>(a.out + s0);
+                tv[0] = tt.x; tv[1] = tt.y; tv[2] = tt.z; tv[3] = tt.w;
+            } else {
+                tv[0] = tv[1] = tv[2] = tv[3] = 0.0f;
+            }
+        } else {
+            y[0] = __ldcs(a.xp + s0);
+            x[0] = __ldcs(a.xp + a.nsamp + s0);
+            al[0] = __ldcs(a.xp + 2 * a.nsamp + s0);
+            tv[0] = TOD2MAP ? __ldcs(a.in + s0) : (a.accum ? a.out[s0] : 0.0f);
+        }
+#pragma unroll
+        for (int k = 0; k < V; k++) {
+            Located L;
+            err |= locate(y[k], x[k], a.ny, a.nx, a.periodic, L);
+            float sn, cs;
+            sincosf(2.0f * al[k], &sn, &cs);
+            const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
+            if constexpr (TOD2MAP) {
+                const float t = tv[k], q = t * cs, u = t * sn;
+                global_accum(a, a.out, L.iy0, L.ix0, t, q, u, wy0 * wx0, err);
+                global_accum(a, a.out, L.iy0, L.ix1, t, q, u, wy0 * L.dx, err);
+                global_accum(a, a.out, L.iy1, L.ix0, t, q, u, L.dy * wx0, err);
+                global_accum(a, a.out, L.iy1, L.ix1, t, q, u, L.dy * L.dx, err);
+            } else {
+                float rr = (wy0 * wx0) * global_eval(a, a.in, L.iy0, L.ix0, 1.0f, cs, sn, err);
+                rr += (wy0 * L.dx) * global_eval(a, a.in, L.iy0, L.ix1, 1.0f, cs, sn, err);
+                rr += (L.dy * wx0) * global_eval(a, a.in, L.iy1, L.ix0, 1.0f, cs, sn, err);
+                rr += (L.dy * L.dx) * global_eval(a, a.in, L.iy1, L.ix1, 1.0f, cs, sn, err);
+                r[k] = a.accum ? (tv[k] + rr) : rr;
+            }
+        }
+        if constexpr (!TOD2MAP) {
+            if constexpr (V == 4)
+                __stcs(reinterpret_cast<float4 *>(a.out + s0), make_float4(r[0], r[1], r[2], r[3]));
+            else
+                __stcs(a.out + s0, r[0]);
+        }
+    }
+    block_publish_err(err, s_err, a.errword);
+}
+
+template<bool TOD2MAP, bool RESP>
+cudaError_t launch_planned_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream)
+{
+    if (nowner <= 0)
+        return cudaSuccess;
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaError_t e = cudaFuncSetAttribute(planned_kernel<TOD2MAP, RESP>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kTileBytes);
+        if (e != cudaSuccess)
+            return e;
+        attr_done = true;
+    }
+    // Two CTAs per SM; never more CTAs than ~64 cache lines each, so small plans reload few tiles.
+    int64_t g = 2 * (int64_t) device_sm_count();
+    g = std::max<int64_t>(1, std::min<int64_t>(g, (nowner + 63) / 64));
+    planned_kernel<TOD2MAP, RESP><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner);
+    return cudaGetLastError();
+}
+
+template<bool TOD2MAP>
+cudaError_t launch_unplanned_impl(const OpArgs &a, cudaStream_t stream)
+{
+    const bool aligned = ((((uintptr_t) a.xp) | ((uintptr_t) a.out) | ((uintptr_t) a.in)) & 15) == 0;
+    const bool vec = aligned && ((a.nsamp & 3) == 0);
+    const int64_t nvec = vec ? a.nsamp / 4 : a.nsamp;
+    int64_t g = 8 * (int64_t) device_sm_count();
+    g = std::max<int64_t>(1, std::min<int64_t>(g, (nvec + 255) / 256));
+    if (vec)
+        unplanned_kernel<TOD2MAP, 4><<<(unsigned) g, 256, 0, stream>>>(a);
+    else
+        unplanned_kernel<TOD2MAP, 1><<<(unsigned) g, 256, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream)
+{
+    return a.response ? launch_planned_impl<false, true>(a, owner_mt, nowner, stream)
+                      : launch_planned_impl<false, false>(a, owner_mt, nowner, stream);
+}
+
+cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream)
+{
+    return a.response ? launch_planned_impl<true, true>(a, owner_mt, nowner, stream)
+                      : launch_planned_impl<true, false>(a, owner_mt, nowner, stream);
+}
+
+cudaError_t launch_unplanned_map2tod(const OpArgs &a, cudaStream_t stream)
+{
+    return launch_unplanned_impl<false>(a, stream);
+}
+
+cudaError_t launch_unplanned_tod2map(const OpArgs &a, cudaStream_t stream)
+{
+    return launch_unplanned_impl<true>(a, stream);
+}
+
+}  // namespace gmm

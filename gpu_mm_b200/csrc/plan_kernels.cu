@@ -1,0 +1,582 @@
+// Plan construction on sm_100a: preplan counts, deterministic mt emission, hand-written LSD
+// radix sort, and dynamic-map cell discovery.
+//
+// Reference behaviour reproduced here (kmsmith137/gpu_mm):
+//   PointingPrePlan.cu:17-108    per-block count of (cell, cache line) pairs -> nmt_cumsum
+//   PointingPlan.cu:19-231       mt words, mflag and zflag (per-warp ring-buffer semantics)
+//   PointingPlan.cu:300-309      stable sort of the mt words by cell (CUB there, hand-written here)
+//   expand_dynamic_map.cu:18-102 cells of a sorted plan that are newly "targeted"
+//
+// Design: instead of the reference's racy chunk claims followed by a 20-bit sort (which leaves
+// the within-cell order nondeterministic), the emit kernel writes every planner block's words in
+// cache-line order, so the stable radix sort yields the canonical (cell, cache line) order and
+// the plan is bit-reproducible.  zflag is derived in closed form from per-line counts: the
+// reference's ring-buffer fill at the start of a line is the running count of that warp's
+// earlier lines mod 32.
+#include <algorithm>
+
+#include "gmm_internal.hpp"
+
+namespace gmm {
+
+// ------------------------------------------------------------------------------------------------
+// Preplan: per planner block, the number of distinct (cell, line) pairs.
+
+constexpr int kPlanWarps = 8;          // warps per planner CTA
+constexpr int kLinesPerWarp = 4;       // lines per warp per round
+constexpr int kRoundLines = kPlanWarps * kLinesPerWarp;   // 32: one scan per round
+
+static_assert(kRoundLines == 32, "round scan assumes one line per lane");
+
+struct LineSlots {
+    int slots[6];
+    unsigned amask[6];
+};
+
+__device__ __forceinline__ void analyse_line(float y, float x, int ny, int nx, bool periodic,
+                                             LineSlots &ls, uint32_t &err)
+{
+    Located L;
+    err |= locate(y, x, ny, nx, periodic, L);
+    cell_slots(L, ls.slots);
+    line_slot_masks(ls.slots, ls.amask);
+}
+
+__global__ void __launch_bounds__(kPlanWarps * 32)
+preplan_count_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bool periodic,
+                     int64_t nclpb, uint32_t *__restrict__ nmt_out, uint32_t *__restrict__ err_out)
+{
+    __shared__ uint32_t s_n[kPlanWarps];
+    __shared__ uint32_t s_e[kPlanWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t ncl = nsamp >> 5;
+    const int64_t l0 = blockIdx.x * nclpb;
+    const int64_t l1 = min(ncl, l0 + nclpb);
+    uint32_t n = 0, err = 0;
+
+    for (int64_t lb = l0 + warp * kLinesPerWarp; lb < l1; lb += kRoundLines) {
+        float y[kLinesPerWarp], x[kLinesPerWarp];
+#pragma unroll
+        for (int j = 0; j < kLinesPerWarp; j++) {
+            int64_t l = min(lb + j, l1 - 1);
+            y[j] = __ldcs(xp + 32 * l + lane);
+            x[j] = __ldcs(xp + nsamp + 32 * l + lane);
+        }
+#pragma unroll
+        for (int j = 0; j < kLinesPerWarp; j++) {
+            if (lb + j >= l1)
+                break;
+            LineSlots ls;
+            analyse_line(y[j], x[j], ny, nx, periodic, ls, err);
+#pragma unroll
+            for (int k = 0; k < 6; k++)
+                n += __popc(ls.amask[k]);
+        }
+    }
+
+    err = __reduce_or_sync(kFullMask, err);
+    if (lane == 0) {
+        s_n[warp] = n;   // warp-uniform
+        s_e[warp] = err;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t nn = (lane < kPlanWarps) ? s_n[lane] : 0u;
+        uint32_t ee = (lane < kPlanWarps) ? s_e[lane] : 0u;
+        nn = __reduce_add_sync(kFullMask, nn);
+        ee = __reduce_or_sync(kFullMask, ee);
+        if (lane == 0) {
+            nmt_out[blockIdx.x] = nn;
+            err_out[blockIdx.x] = ee;
+        }
+    }
+}
+
+// Turns per-block counts into the inclusive cumsum padded with the total (PointingPrePlan.cu:203-211)
+// and leaves {OR of error bits, total lo, total hi} in err[0..3) for one small readback.
+__global__ void __launch_bounds__(1024)
+preplan_finalize_kernel(uint32_t *__restrict__ nmt, uint32_t *__restrict__ err, int nblocks)
+{
+    __shared__ uint64_t s_w[32];
+    __shared__ uint32_t s_e[32];
+    __shared__ uint64_t s_total;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint64_t c = (t < nblocks) ? nmt[t] : 0;
+    uint32_t e = (t < nblocks) ? err[t] : 0;
+    uint64_t incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint64_t v = __shfl_up_sync(kFullMask, incl, d);
+        if (lane >= d) incl += v;
+    }
+    e = __reduce_or_sync(kFullMask, e);
+    if (lane == 31) s_w[warp] = incl;
+    if (lane == 0) s_e[warp] = e;
+    __syncthreads();
+    if (warp == 0) {
+        const uint64_t w = s_w[lane];
+        uint64_t wi = w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint64_t v = __shfl_up_sync(kFullMask, wi, d);
+            if (lane >= d) wi += v;
+        }
+        s_w[lane] = wi - w;
+        const uint32_t ee = __reduce_or_sync(kFullMask, s_e[lane]);
+        if (lane == 31) s_total = wi;
+        if (lane == 0) s_e[0] = ee;
+    }
+    __syncthreads();
+    incl += s_w[warp];
+    const uint64_t total = s_total;   // blocks >= nblocks contribute 0
+    nmt[t] = (uint32_t) ((t < nblocks) ? incl : total);
+    if (t == 0) {
+        err[0] = s_e[0];
+        err[1] = (uint32_t) (total & 0xffffffffu);
+        err[2] = (uint32_t) (total >> 32);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Plan emit: deterministic, cache-line-major mt words per planner block, plus one owner word per
+// cache line (the line's lowest cell), which the operators use to visit each line exactly once.
+
+__global__ void __launch_bounds__(kPlanWarps * 32)
+plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
+                 const uint32_t *__restrict__ nmt_cumsum, uint64_t *__restrict__ mt_out,
+                 uint64_t *__restrict__ owner_out, uint32_t *__restrict__ errflags)
+{
+    __shared__ int s_cnt[kRoundLines];
+    __shared__ int s_off[kRoundLines];
+    __shared__ int s_fill[kRoundLines];
+    __shared__ int s_ring[4];
+    __shared__ int64_t s_base;
+    __shared__ uint32_t s_err[kPlanWarps];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t ncl = nsamp >> 5;
+    const int64_t b = blockIdx.x;
+    const int64_t l0 = b * nclpb;
+    const int64_t l1 = min(ncl, l0 + nclpb);
+    const int64_t out0 = b ? (int64_t) nmt_cumsum[b - 1] : 0;
+    const int64_t nmax = (int64_t) nmt_cumsum[b] - out0;
+    uint64_t *out = mt_out + out0;
+
+    if (threadIdx.x < 4) s_ring[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+
+    uint32_t err = 0;
+
+    for (int64_t r0 = l0; r0 < l1; r0 += kRoundLines) {
+        // Phase 1: analyse this warp's lines of the round.
+        LineSlots ls[kLinesPerWarp];
+        float y[kLinesPerWarp], x[kLinesPerWarp];
+        const int64_t lw = r0 + warp * kLinesPerWarp;
+#pragma unroll
+        for (int j = 0; j < kLinesPerWarp; j++) {
+            int64_t l = min(lw + j, l1 - 1);
+            y[j] = __ldcs(xp + 32 * l + lane);
+            x[j] = __ldcs(xp + nsamp + 32 * l + lane);
+        }
+#pragma unroll
+        for (int j = 0; j < kLinesPerWarp; j++) {
+            int cnt = 0;
+            if (lw + j < l1) {
+                analyse_line(y[j], x[j], ny, nx, periodic, ls[j], err);
+#pragma unroll
+                for (int k = 0; k < 6; k++)
+                    cnt += __popc(ls[j].amask[k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    ls[j].amask[k] = 0;
+                    ls[j].slots[k] = -1;
+                }
+            }
+            if (lane == 0)
+                s_cnt[warp * kLinesPerWarp + j] = cnt;
+        }
+        __syncthreads();
+
+        // Phase 2: offsets within the round and the reference's ring-buffer fill per line.
+        // Line i of the round belongs to reference warp (i & 3) (PointingPlan.cu:167 with W=4;
+        // r0 - l0 is a multiple of 32).
+        if (warp == 0) {
+            int c = s_cnt[lane];
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                int v = __shfl_up_sync(kFullMask, incl, d);
+                if (lane >= d) incl += v;
+            }
+            int cls = c;
+#pragma unroll
+            for (int d = 4; d < 32; d <<= 1) {
+                int v = __shfl_up_sync(kFullMask, cls, d);
+                if (lane >= d) cls += v;
+            }
+            s_off[lane] = incl - c;
+            s_fill[lane] = (s_ring[lane & 3] + cls - c) & 31;
+            int class_total = __shfl_sync(kFullMask, cls, 28 + (lane & 3));
+            __syncwarp();
+            if (lane < 4)
+                s_ring[lane] = (s_ring[lane] + class_total) & 31;
+        }
+        __syncthreads();
+
+        // Phase 3: emit.  Entry order within a line: slot order, then lane order (the order in
+        // which the reference's ring buffer absorbs them, PointingPlan.cu:71-73, :182-187).
+#pragma unroll
+        for (int j = 0; j < kLinesPerWarp; j++) {
+            const int li = warp * kLinesPerWarp + j;
+            const int64_t l = r0 + li;
+            if (l >= l1)
+                break;
+            const int64_t base = s_base + s_off[li];
+            const int fill = s_fill[li];
+            const int cnt = s_cnt[li];
+            const bool mflag = (cnt > 1);
+            const uint64_t hi = ((uint64_t) l << 20) | (mflag ? kMflag : 0ull);
+            int pos = 0;
+            unsigned minc = 0xffffffffu;
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                const unsigned am = ls[j].amask[k];
+                if ((am >> lane) & 1u) {
+                    const int rank = __popc(am & lt);
+                    const int64_t p = base + pos + rank;
+                    const bool zflag = mflag && (rank == 0) && (fill + pos < 32);
+                    const uint64_t word = (uint64_t) (unsigned) ls[j].slots[k] | hi | (zflag ? kZflag : 0ull);
+                    if (p < nmax)
+                        out[p] = word;
+                    minc = min(minc, (unsigned) ls[j].slots[k]);
+                }
+                pos += __popc(am);
+            }
+            minc = __reduce_min_sync(kFullMask, minc);
+            if (lane == 0)
+                owner_out[l] = (uint64_t) minc | hi;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_base += s_off[kRoundLines - 1] + s_cnt[kRoundLines - 1];
+        __syncthreads();
+    }
+
+    if (s_base != nmax)
+        err |= kErrInconsistentNmt;
+    err = __reduce_or_sync(kFullMask, err);
+    if (lane == 0)
+        s_err[warp] = err;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t e = (lane < kPlanWarps) ? s_err[lane] : 0u;
+        e = __reduce_or_sync(kFullMask, e);
+        if (lane == 0)
+            errflags[b] = e;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Hand-written stable LSD radix sort of mt words by cell.
+//
+// Only the cell bits that can vary are sorted: the compound key is ix | (iy << xbits), an order-
+// preserving compression of the 20-bit cell field.  Each pass: upsweep (digit histogram per CTA
+// chunk), a one-CTA exclusive scan, and a downsweep that ranks keys stably (warp match + per-warp
+// running counts + a cross-warp scan per tile) and scatters them.
+
+struct DigitSpec {
+    int xbits;       // bits of the ixcell part
+    uint32_t xmask;  // (1 << xbits) - 1
+    uint32_t ymask;  // mask of the iycell part
+    int shift;       // first compound bit of this pass
+    int dbits;       // digit width of this pass
+};
+
+__device__ __forceinline__ uint32_t key_digit(uint64_t w, const DigitSpec &ds)
+{
+    uint32_t c = (uint32_t) w;
+    uint32_t ix = c & 0x3ffu, iy = (c >> 10) & 0x3ffu;
+    uint32_t comp = (ix & ds.xmask) | ((iy & ds.ymask) << ds.xbits);
+    return (comp >> ds.shift) & ((1u << ds.dbits) - 1u);
+}
+
+__global__ void __launch_bounds__(256)
+sort_upsweep_kernel(const uint64_t *__restrict__ keys, int64_t n, int64_t chunk, DigitSpec ds,
+                    uint32_t *__restrict__ hist)
+{
+    extern __shared__ uint32_t sh[];
+    const int nd = 1 << ds.dbits;
+    const int G = gridDim.x, g = blockIdx.x;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int d = threadIdx.x; d < nd; d += blockDim.x)
+        sh[d] = 0;
+    __syncthreads();
+    const int64_t c0 = g * chunk, c1 = min(n, c0 + chunk);
+    for (int64_t i0 = c0; i0 < c1; i0 += blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        const bool valid = i < c1;
+        const uint32_t d = valid ? key_digit(keys[i], ds) : 0xffffffffu;
+        const unsigned peers = __match_any_sync(kFullMask, d);
+        if (valid && ((peers & lt) == 0))
+            atomicAdd(&sh[d], (uint32_t) __popc(peers));
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < nd; d += blockDim.x)
+        hist[(int64_t) d * G + g] = sh[d];
+}
+
+// Exclusive scan of hist[0..m) in place, one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024)
+sort_scan_kernel(uint32_t *__restrict__ hist, int64_t m)
+{
+    __shared__ uint32_t s_w[32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int64_t seg = (m + 1023) / 1024;
+    const int64_t a = min(m, t * seg), z = min(m, a + seg);
+    uint32_t sum = 0;
+    for (int64_t i = a; i < z; i++)
+        sum += hist[i];
+    uint32_t incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t v = __shfl_up_sync(kFullMask, incl, d);
+        if (lane >= d) incl += v;
+    }
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = s_w[lane], wi = w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t v = __shfl_up_sync(kFullMask, wi, d);
+            if (lane >= d) wi += v;
+        }
+        s_w[lane] = wi - w;
+    }
+    __syncthreads();
+    uint32_t run = s_w[warp] + incl - sum;
+    for (int64_t i = a; i < z; i++) {
+        uint32_t v = hist[i];
+        hist[i] = run;
+        run += v;
+    }
+}
+
+constexpr int kSortWarps = 8;
+
+template<int K>
+__global__ void __launch_bounds__(kSortWarps * 32)
+sort_downsweep_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ out, int64_t n, int64_t chunk,
+                      DigitSpec ds, const uint32_t *__restrict__ offs)
+{
+    extern __shared__ uint32_t sh[];
+    const int nd = 1 << ds.dbits;
+    uint32_t *whist = sh;                        // [kSortWarps][nd]
+    uint32_t *run = sh + kSortWarps * nd;        // [nd]
+    const int G = gridDim.x, g = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+
+    for (int d = threadIdx.x; d < nd; d += blockDim.x)
+        run[d] = offs[(int64_t) d * G + g];
+    for (int i = threadIdx.x; i < kSortWarps * nd; i += blockDim.x)
+        whist[i] = 0;
+    __syncthreads();
+
+    const int64_t c0 = g * chunk, c1 = min(n, c0 + chunk);
+    constexpr int kTile = kSortWarps * 32 * K;
+    uint32_t *mine = whist + warp * nd;
+
+    for (int64_t t0 = c0; t0 < c1; t0 += kTile) {
+        uint64_t key[K];
+        uint32_t dig[K], rank[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int64_t i = t0 + (int64_t) warp * 32 * K + 32 * k + lane;
+            const bool valid = i < c1;
+            key[k] = valid ? in[i] : 0ull;
+            dig[k] = valid ? key_digit(key[k], ds) : 0xffffffffu;
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const bool valid = dig[k] != 0xffffffffu;
+            const unsigned peers = __match_any_sync(kFullMask, dig[k]);
+            const uint32_t prior = valid ? mine[dig[k]] : 0u;
+            __syncwarp();
+            if (valid && ((peers & lt) == 0))
+                mine[dig[k]] = prior + __popc(peers);
+            __syncwarp();
+            rank[k] = prior + __popc(peers & lt);
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < nd; d += blockDim.x) {
+            uint32_t s = run[d];
+#pragma unroll
+            for (int w = 0; w < kSortWarps; w++) {
+                uint32_t c = whist[w * nd + d];
+                whist[w * nd + d] = s;
+                s += c;
+            }
+            run[d] = s;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            if (dig[k] != 0xffffffffu)
+                out[mine[dig[k]] + rank[k]] = key[k];
+        __syncthreads();
+        for (int i = threadIdx.x; i < kSortWarps * nd; i += blockDim.x)
+            whist[i] = 0;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Dynamic-map cell discovery (expand_dynamic_map.cu:18-102): the last word of every cell run in
+// the sorted plan is a candidate; targeted cells (offset -1) get the next free cell index.
+
+__global__ void __launch_bounds__(256)
+expand_dynamic_map_kernel(uint32_t *__restrict__ global_ncells, int64_t *__restrict__ cell_offsets, int nycells,
+                          int nxcells, const uint64_t *__restrict__ plan_mt, int64_t nmt)
+{
+    __shared__ uint32_t s_cells[256];
+    __shared__ uint32_t s_n, s_base;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+    if (i < nmt) {
+        const uint32_t c = (uint32_t) (plan_mt[i] & kCellMask);
+        const uint32_t cn = (i + 1 < nmt) ? (uint32_t) (plan_mt[i + 1] & kCellMask) : 0xffffffffu;
+        const uint32_t ix = c & 0x3ffu, iy = c >> 10;
+        if ((c != cn) && (ix < (uint32_t) nxcells) && (iy < (uint32_t) nycells)) {
+            if (cell_offsets[(int64_t) iy * nxcells + ix] == -1) {
+                uint32_t k = atomicAdd(&s_n, 1u);
+                s_cells[k] = c;
+            }
+        }
+    }
+    __syncthreads();
+    const uint32_t nloc = s_n;
+    if (nloc == 0)
+        return;
+    if (threadIdx.x == 0)
+        s_base = atomicAdd(global_ncells, nloc);
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nloc; k += blockDim.x) {
+        const uint32_t c = s_cells[k];
+        const uint32_t ix = c & 0x3ffu, iy = c >> 10;
+        cell_offsets[(int64_t) iy * nxcells + ix] = (int64_t) (s_base + k) * (3 * 64 * 64);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Host launchers.
+
+static int bits_for(int64_t n)   // bits needed for values in [0, n)
+{
+    int b = 0;
+    while ((1ll << b) < n) b++;
+    return b;
+}
+
+int sort_passes(int nycells_max, int nxcells_max, int max_digit_bits, int *digit_bits)
+{
+    const int cb = bits_for(nxcells_max) + bits_for(nycells_max);
+    if (cb == 0) {
+        *digit_bits = 0;
+        return 0;
+    }
+    const int p = (cb + max_digit_bits - 1) / max_digit_bits;
+    *digit_bits = (cb + p - 1) / p;
+    return p;
+}
+
+int64_t sort_scratch_nbytes(int digit_bits, int grid)
+{
+    if (digit_bits <= 0) return 0;
+    return ((int64_t) (1 << digit_bits) * grid * 4 + 127) & ~127ll;
+}
+
+// Grid of the sort kernels: ~4096 keys per CTA, at most two CTAs per SM and never more than 320
+// (the histogram scratch is sized for 320 CTAs).
+static int sort_grid(int64_t n, int num_sms)
+{
+    int64_t g = (n + 4095) / 4096;
+    g = std::min<int64_t>(g, std::min<int64_t>(2 * (int64_t) num_sms, 320));
+    return (int) std::max<int64_t>(g, 1);
+}
+
+int sort_grid_for(int64_t n) { return sort_grid(n, device_sm_count()); }
+
+// Sorts 'n' mt words by cell.  The input is in 'a'; the result ends in 'a' if npasses is even and in
+// 'b' if it is odd (callers place the input accordingly).
+cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, int nxcells_max, int digit_bits,
+                          int npasses, uint32_t *hist, cudaStream_t stream)
+{
+    if ((n <= 0) || (npasses == 0))
+        return cudaSuccess;
+    const int xbits = bits_for(nxcells_max), ybits = bits_for(nycells_max);
+    const int G = sort_grid_for(n);
+    const int64_t chunk = (((n + G - 1) / G) + 255) / 256 * 256;
+    const int nd = 1 << digit_bits;
+    constexpr int K = 8;
+    const size_t up_smem = nd * sizeof(uint32_t);
+    const size_t down_smem = (size_t) (kSortWarps + 1) * nd * sizeof(uint32_t);
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaFuncSetAttribute(sort_downsweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(sort_upsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        attr_done = true;
+    }
+    uint64_t *src = a, *dst = b;
+    for (int p = 0; p < npasses; p++) {
+        DigitSpec ds;
+        ds.xbits = xbits;
+        ds.xmask = (1u << xbits) - 1u;
+        ds.ymask = (1u << ybits) - 1u;
+        ds.shift = p * digit_bits;
+        ds.dbits = min(digit_bits, xbits + ybits - p * digit_bits);
+        const int ndp = 1 << ds.dbits;
+        sort_upsweep_kernel<<<G, 256, ndp * sizeof(uint32_t), stream>>>(src, n, chunk, ds, hist);
+        sort_scan_kernel<<<1, 1024, 0, stream>>>(hist, (int64_t) ndp * G);
+        sort_downsweep_kernel<K><<<G, kSortWarps * 32, (kSortWarps + 1) * ndp * sizeof(uint32_t), stream>>>(
+            src, dst, n, chunk, ds, hist);
+        uint64_t *t = src; src = dst; dst = t;
+        (void) up_smem; (void) down_smem;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_preplan(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
+                           int nblocks, uint32_t *nmt, uint32_t *err, cudaStream_t stream)
+{
+    preplan_count_kernel<<<nblocks, kPlanWarps * 32, 0, stream>>>(xp, nsamp, ny, nx, periodic, nclpb, nmt, err);
+    preplan_finalize_kernel<<<1, 1024, 0, stream>>>(nmt, err, nblocks);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plan_emit(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
+                             int nblocks, const uint32_t *nmt_cumsum, uint64_t *mt_out, uint64_t *owner_out,
+                             uint32_t *errflags, cudaStream_t stream)
+{
+    plan_emit_kernel<<<nblocks, kPlanWarps * 32, 0, stream>>>(xp, nsamp, ny, nx, periodic, nclpb, nmt_cumsum,
+                                                               mt_out, owner_out, errflags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_expand_dynamic_map(uint32_t *global_ncells, int64_t *cell_offsets, int nycells, int nxcells,
+                                      const uint64_t *plan_mt, int64_t nmt, cudaStream_t stream)
+{
+    if (nmt <= 0)
+        return cudaSuccess;
+    const int64_t nb = (nmt + 255) / 256;
+    expand_dynamic_map_kernel<<<(unsigned) nb, 256, 0, stream>>>(global_ncells, cell_offsets, nycells, nxcells,
+                                                                  plan_mt, nmt);
+    return cudaGetLastError();
+}
+
+}  // namespace gmm

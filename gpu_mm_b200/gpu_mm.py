@@ -1,0 +1,413 @@
+"""
+Drop-in Python surface of gpu_mm's pointing operators, backed by hand-written sm_100a CUDA.
+
+This mirrors kmsmith137/gpu_mm ``gpu_mm/gpu_mm.py`` for the pointing-operator path:
+
+  map2tod(tod, local_map, xpointing, plan, partial_pixelization=False, response=None, debug=False, accum=False)
+  tod2map(local_map, tod, xpointing, plan, partial_pixelization=False, response=None, debug=False)
+  LocalPixelization, LocalMap, DynamicMap, PointingPrePlan, PointingPlan, read_xpointing_npzfile
+
+with the same argument names, meanings and exceptions (gpu_mm.py:262-385, :421-806, :1208-1329).
+Device arrays are torch CUDA tensors (any object with ``__cuda_array_interface__`` is accepted);
+host arrays are numpy.  The reference used cupy, which is not part of this stack.
+
+Data structures (see the reference's top-level docstring, gpu_mm.py:1-150):
+
+* TOD: float32 ``tod[nsamp]`` or ``tod[ndet][nt]``; nsamp a multiple of 32 and <= 2^31.
+* xpointing: float32 ``xpointing[3][nsamp]`` or ``[3][ndet][nt]``, rows {y, x, alpha}; a detector
+  measures ``T + cos(2 alpha) Q + sin(2 alpha) U``.
+* Local map: 64x64-pixel cells, element (pol, iy, ix) of cell (iycell, ixcell) at
+  ``cell_offsets[iycell, ixcell] + pol*polstride + iy*ystride + ix``; negative offsets are absent cells.
+
+The ``plan`` argument selects the operator: a PointingPlan (planned, fastest), None (unplanned), or
+'reference' (the library's slow single-threaded CPU operator, for testing).  No path falls back
+to the CPU silently; the package refuses to import without its native extension.
+"""
+
+import numpy as np
+import torch
+
+from . import gpu_mm_pybind11
+
+mm_dtype = np.float64 if (gpu_mm_pybind11._get_tsize() == 8) else np.float32
+
+_UNPLANNED_ERRFLAG_WORDS = 2048   # gpu_mm.py:306 ("max_blocks = 2048  # ad hoc")
+
+
+def _device_zeros(n, dtype):
+    return torch.zeros(n, dtype=dtype, device="cuda")
+
+
+def map2tod(tod, local_map, xpointing, plan, partial_pixelization=False, response=None, debug=False, accum=False):
+    """
+    Arguments (gpu_mm.py:262-312):
+
+      - tod: output array, shape (nsamp,) or (ndet, nt).  Overwritten unless accum=True.
+      - local_map: input LocalMap.
+      - xpointing: shape (3, nsamp) or (3, ndet, nt) array.
+      - plan: a PointingPlan, None (plan-free GPU code), or 'reference' (CPU reference code).
+      - partial_pixelization: if True, xpointing outside the local map reads zeros; if False, that
+        raises an exception.
+      - response: optional (2, ndet) per-detector (T, P) response; needs a PointingPlan.
+      - accum: if True the result is added to 'tod'.
+    """
+    assert isinstance(local_map, LocalMap)
+    lpix = local_map.pixelization
+    larr = local_map.arr
+
+    if isinstance(plan, PointingPlan):
+        if response is None:
+            gpu_mm_pybind11.planned_map2tod(tod, larr, xpointing, lpix, plan, partial_pixelization, debug, accum)
+        else:
+            gpu_mm_pybind11.response_map2tod(tod, larr, xpointing, response, lpix, plan, partial_pixelization, debug, accum)
+    elif plan is None:
+        errflag = _device_zeros(_UNPLANNED_ERRFLAG_WORDS, torch.int32)
+        gpu_mm_pybind11.unplanned_map2tod(tod, larr, xpointing, lpix, errflag, partial_pixelization, accum)
+    elif isinstance(plan, str) and plan == 'reference':
+        gpu_mm_pybind11.reference_map2tod(tod, larr, xpointing, lpix, partial_pixelization, accum)
+    else:
+        raise RuntimeError(f"Bad 'plan' argument to map2tod(): {plan}")
+
+
+def tod2map(local_map, tod, xpointing, plan, partial_pixelization=False, response=None, debug=False):
+    """
+    Arguments (gpu_mm.py:314-385):
+
+      - local_map: output LocalMap or DynamicMap; tod2map() accumulates into it.
+      - tod: input array, shape (nsamp,) or (ndet, nt).
+      - xpointing: shape (3, nsamp) or (3, ndet, nt) array.
+      - plan: a PointingPlan, None (plan-free GPU code), or 'reference' (CPU reference code).
+      - partial_pixelization: as in map2tod().
+      - response: optional (2, ndet) per-detector (T, P) response; needs a PointingPlan.
+    """
+    if isinstance(local_map, DynamicMap):
+        if not isinstance(plan, PointingPlan):
+            raise RuntimeError("tod2map(): if output is a DynamicMap, then the 'plan' argument"
+                               + f" must be a PointingPlan (got: {plan})'")
+        if partial_pixelization != local_map.have_cell_mask:
+            raise RuntimeError(f"tod2map(): {partial_pixelization=} was specified,"
+                               + f" but DynamicMap.have_cell_mask={local_map.have_cell_mask}"
+                               + " (expected these to be equal)")
+        local_map.expand(plan)
+        if response is None:
+            gpu_mm_pybind11.planned_tod2map(local_map._unstable_arr, tod, xpointing,
+                                            local_map._unstable_pixelization, plan, partial_pixelization, debug)
+        else:
+            gpu_mm_pybind11.response_tod2map(local_map._unstable_arr, tod, xpointing, response,
+                                             local_map._unstable_pixelization, plan, partial_pixelization, debug)
+        return
+
+    if not isinstance(local_map, LocalMap):
+        raise RuntimeError(f"tod2map(): Bad 'local_map' argument to tod2map(): expected LocalMap or DynamicMap, got: {local_map}")
+
+    lpix = local_map.pixelization
+    larr = local_map.arr
+
+    if isinstance(plan, PointingPlan):
+        if response is None:
+            gpu_mm_pybind11.planned_tod2map(larr, tod, xpointing, lpix, plan, partial_pixelization, debug)
+        else:
+            gpu_mm_pybind11.response_tod2map(larr, tod, xpointing, response, lpix, plan, partial_pixelization, debug)
+    elif plan is None:
+        errflag = _device_zeros(_UNPLANNED_ERRFLAG_WORDS, torch.int32)
+        gpu_mm_pybind11.unplanned_tod2map(larr, tod, xpointing, lpix, errflag, partial_pixelization)
+    elif isinstance(plan, str) and plan == 'reference':
+        gpu_mm_pybind11.reference_tod2map(larr, tod, xpointing, lpix, partial_pixelization)
+    else:
+        raise RuntimeError(f"Bad 'plan' argument to tod2map(): {plan}")
+
+
+####################################################################################################
+
+
+def _to_numpy_int64(a):
+    if isinstance(a, torch.Tensor):
+        a = a.detach().cpu().numpy()
+    return np.ascontiguousarray(np.asarray(a), dtype=np.int64)
+
+
+class LocalPixelization(gpu_mm_pybind11.LocalPixelization):
+    """
+    Global pixelization (nypix_global, nxpix_global, periodic_xcoord) plus a set of 64x64 cells and
+    their memory layout (cell_offsets, ystride, polstride); see gpu_mm.py:421-526.
+
+    Members: nypix_global, nxpix_global, periodic_xcoord, cell_offsets_cpu (numpy),
+    cell_offsets_gpu (torch), ystride, polstride, nycells, nxcells, npix.
+    """
+
+    def __init__(self, nypix_global, nxpix_global, cell_offsets, ystride, polstride, periodic_xcoord=True):
+        self.cell_offsets_cpu = _to_numpy_int64(cell_offsets)
+        self.cell_offsets_gpu = torch.as_tensor(self.cell_offsets_cpu).to("cuda")
+        gpu_mm_pybind11.LocalPixelization.__init__(self, nypix_global, nxpix_global, self.cell_offsets_cpu,
+                                                   self.cell_offsets_gpu, ystride, polstride, periodic_xcoord)
+
+    def is_simple_rectangle(self):
+        """True if the layout is a contiguous (3, 64*nycells, 64*nxcells) array (gpu_mm.py:450-458)."""
+        rect_offsets = self._make_rectangular_cell_offsets(self.nycells, self.nxcells)
+        return np.array_equal(self.cell_offsets_cpu, rect_offsets)
+
+    def __eq__(self, x):
+        assert isinstance(x, LocalPixelization)
+        if self is x:
+            return True
+        if (self.nypix_global, self.nxpix_global) != (x.nypix_global, x.nxpix_global):
+            return False
+        if (self.periodic_xcoord, self.ystride, self.polstride) != (x.periodic_xcoord, x.ystride, x.polstride):
+            return False
+        if (self.nycells, self.nxcells, self.npix) != (x.nycells, x.nxcells, x.npix):
+            return False
+        return bool(np.all(np.maximum(self.cell_offsets_cpu, -1) == np.maximum(x.cell_offsets_cpu, -1)))
+
+    __hash__ = None
+
+    @classmethod
+    def _make_rectangular_cell_offsets(cls, nycells, nxcells):
+        cell_offsets = np.empty((nycells, nxcells), dtype=np.int64)
+        cell_offsets[:, :] = 64 * np.arange(nxcells).reshape((1, -1))
+        cell_offsets[:, :] += 64 * 64 * nxcells * np.arange(nycells).reshape((-1, 1))
+        return cell_offsets
+
+    @classmethod
+    def make_rectangle(cls, nypix_global, nxpix_global, periodic_xcoord=True):
+        """A LocalPixelization covering the whole global map as a contiguous
+        (3, nypix_padded, nxpix_padded) array (gpu_mm.py:478-511)."""
+        assert nypix_global > 0
+        assert nxpix_global > 0
+        nycells = (nypix_global + 63) // 64
+        nxcells = (nxpix_global + 63) // 64
+        return LocalPixelization(nypix_global, nxpix_global,
+                                 cell_offsets=cls._make_rectangular_cell_offsets(nycells, nxcells),
+                                 ystride=64 * nxcells, polstride=64 * 64 * nycells * nxcells,
+                                 periodic_xcoord=periodic_xcoord)
+
+    @classmethod
+    def make_cells(cls, nypix_global, nxpix_global, cells, periodic_xcoord=True):
+        """A LocalPixelization holding only the given cells (an iterable of (iycell, ixcell)), in
+        cell-major layout float32[ncells][3][64][64] (ystride=64, polstride=64*64), in the given order."""
+        nycells = (nypix_global + 63) // 64
+        nxcells = (nxpix_global + 63) // 64
+        offs = np.full((nycells, nxcells), -1, dtype=np.int64)
+        for i, (iy, ix) in enumerate(cells):
+            offs[iy, ix] = 3 * 64 * 64 * i
+        return LocalPixelization(nypix_global, nxpix_global, offs, 64, 64 * 64, periodic_xcoord)
+
+
+class LocalMap:
+    """A LocalPixelization plus the map array 'arr' (torch CUDA tensor or numpy host array),
+    float32 and contiguous (gpu_mm.py:529-580)."""
+
+    def __init__(self, pixelization, arr):
+        assert isinstance(pixelization, LocalPixelization)
+        on_gpu = isinstance(arr, torch.Tensor) and arr.is_cuda
+        assert on_gpu or isinstance(arr, np.ndarray), "LocalMap: 'arr' must be a torch CUDA tensor or a numpy array"
+        if on_gpu:
+            assert arr.dtype == torch.float32
+            assert arr.is_contiguous()
+        else:
+            assert arr.dtype == np.float32
+            assert arr.flags['C_CONTIGUOUS']
+        self.pixelization = pixelization
+        self.nypix_global = pixelization.nypix_global
+        self.nxpix_global = pixelization.nxpix_global
+        self.periodic_xcoord = pixelization.periodic_xcoord
+        self.on_gpu = on_gpu
+        self.npix = pixelization.npix
+        self.dtype = np.float32
+        self.arr = arr
+
+    def to_global(self):
+        """The map as a numpy array of shape (3, nypix_global, nxpix_global); pixels outside the
+        local map are zero (gpu_mm.py:565-580)."""
+        src = self.arr.detach().cpu().numpy() if isinstance(self.arr, torch.Tensor) else self.arr
+        src = np.ascontiguousarray(src.reshape(-1))
+        dst = np.zeros((3, self.nypix_global, self.nxpix_global), dtype=np.float32)
+        gpu_mm_pybind11.local_map_to_global(self.pixelization, dst, src)
+        return dst
+
+
+####################################################################################################
+
+
+class DynamicMap:
+    """
+    A LocalMap that starts with zero cells and grows as tod2map() touches new cells; call finalize()
+    to obtain a LocalMap (gpu_mm.py:586-806).  Layout: float32 local_map[ncells][3][64][64].
+    'cell_mask' (bool, (nycells, nxcells)) restricts growth to a target region.
+    """
+
+    def __init__(self, nypix_global, nxpix_global, dtype, cell_mask=None, periodic_xcoord=True, initial_ncells=1024):
+        assert 0 < nxpix_global <= 64 * 1024
+        assert 0 < nypix_global <= 64 * 1024
+        assert np.dtype(dtype) == np.float32 or dtype == torch.float32
+        assert initial_ncells > 0
+
+        self.nypix_global = nypix_global
+        self.nxpix_global = nxpix_global
+        self.periodic_xcoord = periodic_xcoord
+        self.have_cell_mask = (cell_mask is not None)
+        self.ncells_allocated = initial_ncells
+        self.reallocation_factor = 1.5
+        self.dtype = np.float32
+
+        # cell_offsets: -1 for "targeted" cells, -2 for "untargeted" ones (expand_dynamic_map.cu:67-68).
+        if cell_mask is None:
+            nycells = (nypix_global + 63) // 64
+            nxcells = (nxpix_global + 63) // 64
+            cell_offsets = np.full((nycells, nxcells), -1, dtype=np.int64)
+        else:
+            cell_mask = np.asarray(cell_mask)
+            assert cell_mask.ndim == 2
+            assert cell_mask.dtype == bool
+            cell_offsets = np.where(cell_mask, -1, -2).astype(np.int64)
+
+        self._unstable_pixelization = LocalPixelization(nypix_global, nxpix_global, cell_offsets,
+                                                        ystride=64, polstride=64 * 64, periodic_xcoord=periodic_xcoord)
+        self._padded_arr = torch.zeros(self.ncells_allocated * 3 * 64 * 64, dtype=torch.float32, device="cuda")
+        self._unstable_arr = self._padded_arr[:0]
+        self.global_ncells = torch.zeros(32, dtype=torch.int32, device="cuda")[:1]
+        self.ncells_curr = 0
+        self.pixelization_is_finalized = False
+        self.map_is_finalized = False
+
+    def expand(self, plan):
+        """Adds the cells a PointingPlan touches, zero-initialised (gpu_mm.py:674-702)."""
+        if self.pixelization_is_finalized:
+            raise RuntimeError("Can't currently call tod2map() [or DynamicMap.expand()]"
+                               + " after MpiPixelization.__init__() [or DynamicMap.permute()].")
+        assert isinstance(plan, PointingPlan)
+        assert plan.nypix_global == self.nypix_global
+        assert plan.nxpix_global == self.nxpix_global
+        assert plan.periodic_xcoord == self.periodic_xcoord
+
+        self.ncells_curr = gpu_mm_pybind11.expand_dynamic_map2(self.global_ncells, self._unstable_pixelization, plan)
+
+        if self.ncells_curr > self.ncells_allocated:
+            self.ncells_allocated = int(self.reallocation_factor * self.ncells_allocated)
+            self.ncells_allocated = max(self.ncells_allocated, self.ncells_curr)
+            new = torch.zeros(self.ncells_allocated * 3 * 64 * 64, dtype=torch.float32, device="cuda")
+            new[:len(self._unstable_arr)] = self._unstable_arr[:]
+            self._padded_arr = new
+
+        self._unstable_pixelization.npix = self.ncells_curr * (64 * 64)
+        self._unstable_arr = self._padded_arr[:(self.ncells_curr * 3 * 64 * 64)]
+
+    def permute(self, iycells, ixcells):
+        """Reorders the cells to the given (iycells, ixcells) order and finalizes the pixelization
+        (gpu_mm.py:705-757).  The data move is one gather on the device."""
+        if self.pixelization_is_finalized:
+            raise RuntimeError("Can't currently call MpiPixelization.__init__() [or DynamicMap.permute()]"
+                               + " after DynamicMap.finalize() [or MpiPixelization.__init__(), DynamicMap.permute()]")
+        self._unstable_pixelization.copy_gpu_offsets_to_cpu()
+        assert self._unstable_pixelization.npix == (self.ncells_curr * 64 * 64)
+        new_offsets = self._unstable_pixelization.cell_offsets_cpu
+        old_offsets = np.copy(new_offsets)
+
+        assert isinstance(iycells, np.ndarray) and isinstance(ixcells, np.ndarray)
+        assert iycells.shape == ixcells.shape == (self.ncells_curr,)
+        assert 0 <= np.min(iycells) <= np.max(iycells) < old_offsets.shape[0]
+        assert 0 <= np.min(ixcells) <= np.max(ixcells) < old_offsets.shape[1]
+
+        new_offsets[iycells, ixcells] = np.arange(self.ncells_curr) * (3 * 64 * 64)
+        if not np.all((old_offsets >= 0) == (new_offsets >= 0)):
+            raise RuntimeError('DynamicMap.permute(): specified (iycells,ixcells) do not match footprint of current pixelization')
+
+        self.pixelization_is_finalized = True
+        self._unstable_pixelization.copy_cpu_offsets_to_gpu()
+        assert self._unstable_pixelization.npix == (self.ncells_curr * 64 * 64)
+
+        src_cells = torch.as_tensor(old_offsets[iycells, ixcells] // (3 * 64 * 64), device="cuda")
+        old = self._unstable_arr.view(-1, 3 * 64 * 64)
+        self._padded_arr = self._unstable_arr = old.index_select(0, src_cells).reshape(-1).contiguous()
+        self.ncells_allocated = self.ncells_curr
+
+    def finalize(self):
+        """Called at the end of the TOD loop; returns a LocalMap (gpu_mm.py:760-779)."""
+        if self.map_is_finalized:
+            raise RuntimeError('Double call to DynamicMap.finalize() [not currently allowed]')
+        if not self.pixelization_is_finalized:
+            self._unstable_pixelization.copy_gpu_offsets_to_cpu()
+            self.pixelization_is_finalized = True
+        if self.ncells_allocated > self.ncells_curr:
+            self._unstable_arr = self._unstable_arr.clone()
+        ret = LocalMap(self._unstable_pixelization, self._unstable_arr)
+        assert self._unstable_pixelization.npix == (self.ncells_curr * 64 * 64)
+        self._padded_arr = self._unstable_arr = None
+        self.map_is_finalized = True
+        return ret
+
+    def randomly_permute(self):
+        """Only called during testing."""
+        self._unstable_pixelization.copy_gpu_offsets_to_cpu()
+        iycells, ixcells = np.where(self._unstable_pixelization.cell_offsets_cpu >= 0)
+        perm = np.random.permutation(self.ncells_curr)
+        self.permute(iycells[perm], ixcells[perm])
+
+
+####################################################################################################
+
+
+class PointingPrePlan(gpu_mm_pybind11.PointingPrePlan):
+    """
+    First step of plan construction (gpu_mm.py:1208-1259): counts (cell, cache line) pairs per
+    planner block and sizes the PointingPlan buffers.  Small (a few KB); keep one per TOD.
+
+    Constructor: PointingPrePlan(xpointing_gpu, nypix_global, nxpix_global, buf=None, tmp_buf=None,
+    periodic_xcoord=True, debug=False).  'buf' and 'tmp_buf' are 1-d 32-bit device arrays of length
+    PointingPrePlan.preplan_size; the preplan keeps 'buf' (it holds nmt_cumsum), 'tmp_buf' may be shared.
+
+    Members (from C++): nsamp, nypix_global, nxpix_global, periodic_xcoord, plan_nbytes,
+    plan_constructor_tmp_nbytes, overhead, ncl_per_threadblock, planner_nblocks,
+    nmt_per_threadblock, pointing_nblocks, plan_nmt, cub_nbytes, get_nmt_cumsum().
+    """
+
+    preplan_size = gpu_mm_pybind11.PointingPrePlan._get_preplan_size()
+
+    def __init__(self, xpointing_gpu, nypix_global, nxpix_global, buf=None, tmp_buf=None, periodic_xcoord=True, debug=False):
+        if buf is None:
+            buf = torch.empty(self.preplan_size, dtype=torch.int32, device="cuda")
+        if tmp_buf is None:
+            tmp_buf = torch.empty(self.preplan_size, dtype=torch.int32, device="cuda")
+        self._buf = buf
+        gpu_mm_pybind11.PointingPrePlan.__init__(self, xpointing_gpu, nypix_global, nxpix_global, buf, tmp_buf,
+                                                 periodic_xcoord, debug)
+
+
+class PointingPlan(gpu_mm_pybind11.PointingPlan):
+    """
+    The plan argument of map2tod()/tod2map() (gpu_mm.py:1262-1299): mt words sorted by
+    (cell, cache line) -- the reference's plan_mt, reproduced bit for bit in canonical order -- plus
+    one owner word per cache line, which the operators use to visit every line once.
+
+    Constructor: PointingPlan(preplan, xpointing_gpu, buf=None, tmp_buf=None, debug=False).  'buf'
+    (uint8, >= preplan.plan_nbytes) is kept by the plan; 'tmp_buf' (uint8, >=
+    preplan.plan_constructor_tmp_nbytes) is only used during construction and may be shared.
+    """
+
+    def __init__(self, preplan, xpointing_gpu, buf=None, tmp_buf=None, debug=False):
+        if buf is None:
+            buf = torch.empty(preplan.plan_nbytes, dtype=torch.uint8, device="cuda")
+        if tmp_buf is None:
+            tmp_buf = torch.empty(preplan.plan_constructor_tmp_nbytes, dtype=torch.uint8, device="cuda")
+        self._buf = buf
+        self.preplan = preplan
+        gpu_mm_pybind11.PointingPlan.__init__(self, preplan, xpointing_gpu, buf, tmp_buf, debug)
+
+
+####################################################################################################
+
+
+def read_xpointing_npzfile(filename):
+    """Reads a (3, ndet, nt) xpointing array from the reference's ad hoc .npz format
+    (gpu_mm.py:1305-1329): rows stored as (x, y, alpha), nt padded to a multiple of 32."""
+    f = np.load(filename)
+    xp = f['xpointing']
+    assert (xp.ndim == 3) and (xp.shape[0] == 3)
+    ndet = xp.shape[1]
+    ntu = xp.shape[2]
+    ntp = 32 * ((ntu + 31) // 32)
+    xpointing_cpu = np.zeros((3, ndet, ntp), dtype=xp.dtype)
+    xpointing_cpu[0, :, :ntu] = xp[1, :, :]
+    xpointing_cpu[1, :, :ntu] = xp[0, :, :]
+    xpointing_cpu[2, :, :ntu] = xp[2, :, :]
+    xpointing_cpu[:, :, ntu:] = xpointing_cpu[:, :, ntu - 1].reshape((3, -1, 1))
+    return xpointing_cpu

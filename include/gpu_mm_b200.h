@@ -1,0 +1,168 @@
+/*
+ * gpu_mm_b200: C ABI of the B200-native pointing-operator hot path.
+ *
+ * This is the drop-in boundary.  Every entry point replaces one piece of the reference's C++
+ * interface (kmsmith137/gpu_mm, include/gpu_mm.hpp); the comment above each one names it.  The
+ * signatures use plain pointers, 64-bit sizes and a cudaStream_t, and no C++ or torch types.  The
+ * C++ API (include/gpu_mm_b200/gpu_mm.hpp) and the pybind11 module gpu_mm_pybind11 sit on top.
+ *
+ * Conventions
+ *  - Device arrays are raw device pointers, float32 (the reference's pybind layer wraps float32
+ *    only, gpu_mm_pybind11.cu:17-19).  TODs are flat [nsamp]; xpointing is [3][nsamp] with rows
+ *    {y, x, alpha} (gpu_mm.py:59-85).
+ *  - Every function returns an int status.  0 means success.  Values 1, 2, 4 and 8 are the reference's
+ *    device error bits (gpu_mm_internals.hpp:26-29); GMM_ERR_* >= 0x100 are API errors.  The last
+ *    error message of the calling thread is available from gmm_last_error().
+ *  - The device error bits of an operator call are OR-reduced on the device into one 32-bit word.
+ *    If 'errword_gpu' is NULL, the call reads that word back on 'stream' and returns its bits, which
+ *    is synchronous like the reference (check_arguments.cu:69-74).  Otherwise the word is left on
+ *    the device for a deferred check with gmm_errword_read(), and the call does not block.
+ *  - No function allocates device memory.  Callers own every buffer, as with the reference's Python
+ *    constructors (gpu_mm.py:1253-1259, :1293-1299).
+ */
+#ifndef GPU_MM_B200_H
+#define GPU_MM_B200_H
+
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GMM_ERR_BAD_YPIX 0x1
+#define GMM_ERR_BAD_XPIX 0x2
+#define GMM_ERR_INCONSISTENT_NMT 0x4
+#define GMM_ERR_NOT_IN_PIXELIZATION 0x8
+#define GMM_ERR_INVALID_ARGUMENT 0x100
+#define GMM_ERR_CUDA 0x200
+#define GMM_ERR_BUFFER_TOO_SMALL 0x400
+
+/* Size of the nmt/err buffers owned by a preplan (gpu_mm.hpp:63, PointingPrePlan::preplan_size). */
+#define GMM_PREPLAN_SIZE 1024
+
+/* Local pixelization as seen by the device: LocalPixelization (gpu_mm.hpp:17-58). */
+typedef struct gmm_lpix {
+    int32_t nypix_global;
+    int32_t nxpix_global;
+    int32_t periodic_xcoord;
+    int32_t nycells;              /* cell_offsets.shape[0], <= 1024 */
+    int32_t nxcells;              /* cell_offsets.shape[1], <= 1024 */
+    int32_t reserved;
+    int64_t ystride;
+    int64_t polstride;
+    int64_t npix;                 /* local pixels (map size is 3*npix) */
+    const int64_t *cell_offsets;  /* device pointer, [nycells][nxcells], negative = absent */
+} gmm_lpix;
+
+/* Scalars of a PointingPrePlan (gpu_mm.hpp:79-101, PointingPrePlan.cu:159-250).  The launch
+ * geometry fields (ncl_per_threadblock .. pointing_nblocks, plan_nmt) equal the reference's;
+ * plan_nbytes / plan_constructor_tmp_nbytes are this implementation's buffer sizes. */
+typedef struct gmm_preplan_info {
+    int64_t nsamp;
+    int32_t nypix_global;
+    int32_t nxpix_global;
+    int32_t periodic_xcoord;
+    int32_t sort_digit_bits;      /* radix digit width chosen for the plan sort */
+    int64_t plan_nbytes;
+    int64_t plan_constructor_tmp_nbytes;
+    double overhead;
+    int64_t ncl_per_threadblock;
+    int64_t planner_nblocks;
+    int64_t nmt_per_threadblock;
+    int64_t pointing_nblocks;
+    int64_t plan_nmt;
+    int64_t sort_nbytes;          /* replaces PointingPrePlan::cub_nbytes: scratch of the radix sort */
+} gmm_preplan_info;
+
+/* Byte offsets of the arrays inside a plan buffer (the reference's 'buf' holds plan_mt and err,
+ * PointingPlan.cu:251-260; this layout appends the owner-line list). */
+typedef struct gmm_plan_layout {
+    int64_t mt_offset;        /* uint64 plan_mt[plan_nmt], sorted by (cell, cache line) */
+    int64_t err_offset;       /* uint32 err[max(planner_nblocks, pointing_nblocks)] */
+    int64_t owner_offset;     /* uint64 owner_mt[nsamp/32]: one word per cache line, sorted */
+    int64_t total_nbytes;
+} gmm_plan_layout;
+
+/* Thread-local message of the last failing call on this thread ("" if none). */
+const char *gmm_last_error(void);
+
+/* Library version string. */
+const char *gmm_version(void);
+
+/* Maximum radix digit width (4..11 bits) of the plan sort, used by later gmm_preplan calls.  The
+ * reference's sort is CUB's (PointingPlan.cu:300-309), whose digit width is not a parameter; here
+ * it is a tuning knob set by the autotuner (gpu_mm_b200/tuning.py).  Default 8. */
+int gmm_set_sort_digit_bits(int32_t bits);
+int gmm_get_sort_digit_bits(void);
+
+/* Replaces the PointingPrePlan constructor (PointingPrePlan.cu:129-251 / gpu_mm.hpp:74-77).
+ * Counts mt words per planner block on the device, writes the inclusive cumsum (padded with the
+ * total) to nmt_gpu[GMM_PREPLAN_SIZE], uses err_gpu[GMM_PREPLAN_SIZE] as scratch, and fills *info.
+ * Synchronises with 'stream' once (to learn nmt), like the reference constructor. */
+int gmm_preplan(const float *xpointing_gpu, int64_t nsamp, int32_t nypix_global, int32_t nxpix_global,
+                int32_t periodic_xcoord, uint32_t *nmt_gpu, uint32_t *err_gpu, int32_t debug,
+                cudaStream_t stream, gmm_preplan_info *info);
+
+/* Computes the host-side PointingPrePlan scalars from nsamp and nmt (no device work). */
+int gmm_preplan_info_init(int64_t nsamp, int32_t nypix_global, int32_t nxpix_global, int32_t periodic_xcoord,
+                          int64_t nmt, gmm_preplan_info *info);
+
+/* Layout of a plan buffer for a given preplan. */
+int gmm_plan_layout_get(const gmm_preplan_info *info, gmm_plan_layout *layout);
+
+/* Replaces the PointingPlan constructor (PointingPlan.cu:237-312 / gpu_mm.hpp:132-137): emits the
+ * mt words, sorts them with the hand-written radix sort and builds the owner-line list.
+ * 'buf' needs info->plan_nbytes bytes and 'tmp' info->plan_constructor_tmp_nbytes bytes, both
+ * 128-byte aligned device memory.  Synchronises once to check the error flags (PointingPlan.cu:311). */
+int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum_gpu, const float *xpointing_gpu,
+                   void *buf, int64_t buf_nbytes, void *tmp, int64_t tmp_nbytes, int32_t debug,
+                   cudaStream_t stream);
+
+/* Replaces launch_planned_map2tod<float> (gpu_mm.hpp:155-165, map2tod.cu:194-272). */
+int gmm_planned_map2tod(float *tod, const float *local_map, const float *xpointing, const gmm_lpix *lpix,
+                        const gmm_preplan_info *info, const void *plan_buf, int32_t partial_pixelization,
+                        int32_t accum, uint32_t *errword_gpu, cudaStream_t stream);
+
+/* Replaces launch_planned_tod2map<float> (gpu_mm.hpp:168-177, tod2map.cu:157-226).  Accumulates. */
+int gmm_planned_tod2map(float *local_map, const float *tod, const float *xpointing, const gmm_lpix *lpix,
+                        const gmm_preplan_info *info, const void *plan_buf, int32_t partial_pixelization,
+                        uint32_t *errword_gpu, cudaStream_t stream);
+
+/* Replaces launch_response_map2tod<float> / launch_response_tod2map<float> (gpu_mm.hpp:179-202,
+ * map2tod_response.cu:205-290, tod2map_response.cu).  response is [2][ndet] (T, P), ndet divides nsamp. */
+int gmm_response_map2tod(float *tod, const float *local_map, const float *xpointing, const float *response,
+                         int64_t ndet, const gmm_lpix *lpix, const gmm_preplan_info *info, const void *plan_buf,
+                         int32_t partial_pixelization, int32_t accum, uint32_t *errword_gpu, cudaStream_t stream);
+int gmm_response_tod2map(float *local_map, const float *tod, const float *xpointing, const float *response,
+                         int64_t ndet, const gmm_lpix *lpix, const gmm_preplan_info *info, const void *plan_buf,
+                         int32_t partial_pixelization, uint32_t *errword_gpu, cudaStream_t stream);
+
+/* Replaces launch_unplanned_map2tod<float> (gpu_mm.hpp:204-213, map2tod_unplanned.cu:74-127).
+ * errflags_gpu has errflags_len >= 1 words (the reference's per-block array); word 0 receives the
+ * OR of all device error bits. */
+int gmm_unplanned_map2tod(float *tod, const float *local_map, const float *xpointing, int64_t nsamp,
+                          const gmm_lpix *lpix, uint32_t *errflags_gpu, int64_t errflags_len,
+                          int32_t partial_pixelization, int32_t accum, int32_t sync_check, cudaStream_t stream);
+
+/* Replaces launch_unplanned_tod2map<float> (gpu_mm.hpp:216-224, tod2map_unplanned.cu:68-121). */
+int gmm_unplanned_tod2map(float *local_map, const float *tod, const float *xpointing, int64_t nsamp,
+                          const gmm_lpix *lpix, uint32_t *errflags_gpu, int64_t errflags_len,
+                          int32_t partial_pixelization, int32_t sync_check, cudaStream_t stream);
+
+/* Deferred error check: reads the device error word (after 'stream' completes), masks the bits in
+ * 'ignore' and returns the rest (check_gpu_errflags, check_arguments.cu:69-74). */
+int gmm_errword_read(const uint32_t *errword_gpu, uint32_t ignore, cudaStream_t stream);
+
+/* Replaces expand_dynamic_map (gpu_mm.hpp:268-272, expand_dynamic_map.cu:106-141): cells of the
+ * sorted plan whose offset is -1 ("targeted") get offsets (global_ncells + i) * 3*64*64.
+ * Returns the updated cell count in *ncells_out (synchronous). */
+int gmm_expand_dynamic_map(uint32_t *global_ncells_gpu, int64_t *cell_offsets_gpu, int32_t nycells,
+                           int32_t nxcells, const uint64_t *plan_mt_gpu, int64_t nmt, uint32_t *ncells_out,
+                           cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPU_MM_B200_H */

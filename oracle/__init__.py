@@ -1,0 +1,280 @@
+"""CPU oracle for the gpu_mm pointing-operator hot path -- TEST INFRASTRUCTURE ONLY.
+
+This package is the checker for the CUDA product path.  Only ``tests/``, ``__graft_entry__.smoke()``
+and ``bench.py``'s CPU-baseline / reference legs may import it, and only to check or to time the CPU
+baseline; the product (``gpu_mm_b200``) never imports it and has no CPU fallback.
+
+Two native libraries sit behind it:
+
+* ``liboracle.so`` -- the C restatement in ``oracle.c`` (every function cites the reference file:line
+  it follows: ``map2tod_reference.cu``, ``tod2map_reference.cu``, ``gpu_mm_internals.hpp``,
+  ``PointingPrePlan.cu``, ``PointingPlan.cu``, ``PointingPlanTester.cu``).
+* ``_ref/libgpu_mm_ref.so`` (optional) -- the reference's own ``include/gpu_mm_internals.hpp``
+  templates compiled from the reference source tree by ``oracle/Makefile``.  It pins the C
+  restatement and serves as the "reference" CPU baseline.  It is built only where the reference
+  tree exists; the committed golden vectors under ``tests/golden/`` carry its outputs elsewhere.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+ERR_BAD_YPIX = 0x1
+ERR_BAD_XPIX = 0x2
+ERR_INCONSISTENT_NMT = 0x4
+ERR_NOT_IN_PIXELIZATION = 0x8
+
+
+class LpixStruct(ctypes.Structure):
+    _fields_ = [
+        ("nypix_global", ctypes.c_int32),
+        ("nxpix_global", ctypes.c_int32),
+        ("periodic_xcoord", ctypes.c_int32),
+        ("nycells", ctypes.c_int32),
+        ("nxcells", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+        ("ystride", ctypes.c_int64),
+        ("polstride", ctypes.c_int64),
+        ("cell_offsets", ctypes.POINTER(ctypes.c_int64)),
+    ]
+
+
+class Lpix:
+    """Plain description of a local pixelization (gpu_mm.hpp:17-58) for the oracle."""
+
+    def __init__(self, nypix_global, nxpix_global, cell_offsets, ystride, polstride, periodic_xcoord=True):
+        self.cell_offsets = np.ascontiguousarray(cell_offsets, dtype=np.int64)
+        assert self.cell_offsets.ndim == 2
+        self.nypix_global = int(nypix_global)
+        self.nxpix_global = int(nxpix_global)
+        self.ystride = int(ystride)
+        self.polstride = int(polstride)
+        self.periodic_xcoord = bool(periodic_xcoord)
+        self.nycells, self.nxcells = self.cell_offsets.shape
+        self.npix = 64 * 64 * int(np.count_nonzero(self.cell_offsets >= 0))
+        self.struct = LpixStruct(
+            self.nypix_global, self.nxpix_global, int(self.periodic_xcoord), self.nycells, self.nxcells, 0,
+            self.ystride, self.polstride, self.cell_offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+
+    @classmethod
+    def rectangle(cls, nypix_global, nxpix_global, periodic_xcoord=True):
+        """Same layout as LocalPixelization.make_rectangle (gpu_mm.py:478-483)."""
+        nyc = (nypix_global + 63) // 64
+        nxc = (nxpix_global + 63) // 64
+        offs = 64 * np.arange(nxc)[None, :] + 64 * 64 * nxc * np.arange(nyc)[:, None]
+        return cls(nypix_global, nxpix_global, offs, 64 * nxc, 64 * 64 * nyc * nxc, periodic_xcoord)
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle: {path} is missing; run 'make -C oracle liboracle.so'")
+        L = ctypes.CDLL(path)
+        u32, i64, i32 = ctypes.c_uint32, ctypes.c_int64, ctypes.c_int32
+        fp, dp = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
+        LP = ctypes.POINTER(LpixStruct)
+        L.oracle_locate_f32.argtypes = [ctypes.c_float, ctypes.c_float, i32, i32, i32,
+                                        ctypes.POINTER(i32), fp]
+        L.oracle_locate_f32.restype = u32
+        for name, T in (("f32", fp), ("f64", dp)):
+            f = getattr(L, f"oracle_map2tod_{name}")
+            f.argtypes = [T, T, T, i64, LP, i32, i32]
+            f.restype = u32
+            f = getattr(L, f"oracle_tod2map_{name}")
+            f.argtypes = [T, T, T, i64, LP, i32]
+            f.restype = u32
+        L.oracle_response_map2tod_f32.argtypes = [fp, fp, fp, fp, i64, i64, LP, i32, i32]
+        L.oracle_response_map2tod_f32.restype = u32
+        L.oracle_response_tod2map_f32.argtypes = [fp, fp, fp, fp, i64, i64, LP, i32]
+        L.oracle_response_tod2map_f32.restype = u32
+        L.oracle_map2tod_f32_mt.argtypes = [fp, fp, fp, i64, LP, i32, i32, i32]
+        L.oracle_map2tod_f32_mt.restype = u32
+        L.oracle_tod2map_f32_mt.argtypes = [fp, fp, fp, i64, i64, LP, i32, i32]
+        L.oracle_tod2map_f32_mt.restype = u32
+        L.oracle_preplan.argtypes = [fp, i64, i32, i32, i32, ctypes.POINTER(u32), ctypes.POINTER(i64),
+                                     ctypes.POINTER(u32)]
+        L.oracle_preplan.restype = i64
+        L.oracle_plan.argtypes = [fp, i64, i32, i32, i32, i64, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(u32)]
+        L.oracle_plan.restype = u32
+        L.oracle_sample_slots.argtypes = [fp, i64, i32, i32, i32, ctypes.POINTER(i32)]
+        L.oracle_line_counts.argtypes = [fp, i64, i32, i32, i32, ctypes.POINTER(ctypes.c_uint8)]
+        _LIB = L
+    return _LIB
+
+
+def ref_path():
+    return os.path.join(_HERE, "_ref", "libgpu_mm_ref.so")
+
+
+def ref_available():
+    return os.path.exists(ref_path())
+
+
+def ref():
+    """The reference-header build (oracle/_ref).  Raises if it was not built."""
+    global _REF
+    if _REF is None:
+        if not ref_available():
+            raise RuntimeError("oracle/_ref was not built (it needs the reference source tree)")
+        R = ctypes.CDLL(ref_path())
+        u32, i64, i32 = ctypes.c_uint32, ctypes.c_int64, ctypes.c_int32
+        fp, dp = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
+        LP = ctypes.POINTER(LpixStruct)
+        R.ref_locate_f32.argtypes = [ctypes.c_float, ctypes.c_float, i32, i32, i32, ctypes.POINTER(i32), fp]
+        R.ref_locate_f32.restype = u32
+        for name, T in (("f32", fp), ("f64", dp)):
+            f = getattr(R, f"ref_map2tod_{name}")
+            f.argtypes = [T, T, T, i64, LP, i32, i32]
+            f.restype = u32
+            f = getattr(R, f"ref_tod2map_{name}")
+            f.argtypes = [T, T, T, i64, LP, i32]
+            f.restype = u32
+        R.ref_map2tod_f32_mt.argtypes = [fp, fp, fp, i64, LP, i32, i32, i32]
+        R.ref_map2tod_f32_mt.restype = u32
+        R.ref_tod2map_f32_mt.argtypes = [fp, fp, fp, i64, i64, LP, i32, i32]
+        R.ref_tod2map_f32_mt.restype = u32
+        R.ref_enumerate_gpu.argtypes = [ctypes.c_void_p, i64, i32, i32, i32, ctypes.c_void_p, ctypes.c_void_p]
+        R.ref_enumerate_gpu.restype = i32
+        _REF = R
+    return _REF
+
+
+# ------------------------------------------------------------------------------------------------
+
+
+def _nsamp(xpointing):
+    xp = np.asarray(xpointing)
+    assert xp.shape[0] == 3
+    return xp.size // 3
+
+
+def _ftype(dtype):
+    return (ctypes.c_float, "f32") if np.dtype(dtype) == np.float32 else (ctypes.c_double, "f64")
+
+
+def map2tod(tod, lmap, xpointing, lpix, partial_pixelization=False, accum=False, use_ref=False):
+    """reference_map2tod semantics (map2tod_reference.cu:16-54).  Updates 'tod' in place and
+    returns the error bits (bit 8 not masked)."""
+    assert tod.flags["C_CONTIGUOUS"] and lmap.flags["C_CONTIGUOUS"] and xpointing.flags["C_CONTIGUOUS"]
+    assert tod.dtype == lmap.dtype == xpointing.dtype
+    ct, name = _ftype(tod.dtype)
+    L = ref() if use_ref else lib()
+    f = getattr(L, ("ref_map2tod_" if use_ref else "oracle_map2tod_") + name)
+    return f(_ptr(tod, ct), _ptr(lmap, ct), _ptr(xpointing, ct), _nsamp(xpointing),
+             ctypes.byref(lpix.struct), int(partial_pixelization), int(accum))
+
+
+def tod2map(lmap, tod, xpointing, lpix, partial_pixelization=False, use_ref=False):
+    """reference_tod2map semantics (tod2map_reference.cu:14-46): accumulates into 'lmap'."""
+    assert tod.flags["C_CONTIGUOUS"] and lmap.flags["C_CONTIGUOUS"] and xpointing.flags["C_CONTIGUOUS"]
+    assert tod.dtype == lmap.dtype == xpointing.dtype
+    ct, name = _ftype(tod.dtype)
+    L = ref() if use_ref else lib()
+    f = getattr(L, ("ref_tod2map_" if use_ref else "oracle_tod2map_") + name)
+    return f(_ptr(lmap, ct), _ptr(tod, ct), _ptr(xpointing, ct), _nsamp(xpointing),
+             ctypes.byref(lpix.struct), int(partial_pixelization))
+
+
+def map2tod_mt(tod, lmap, xpointing, lpix, nthreads, partial_pixelization=False, accum=False, use_ref=False):
+    ct = ctypes.c_float
+    f = ref().ref_map2tod_f32_mt if use_ref else lib().oracle_map2tod_f32_mt
+    return f(_ptr(tod, ct), _ptr(lmap, ct), _ptr(xpointing, ct), _nsamp(xpointing), ctypes.byref(lpix.struct),
+             int(partial_pixelization), int(accum), int(nthreads))
+
+
+def tod2map_mt(lmap, tod, xpointing, lpix, nthreads, partial_pixelization=False, use_ref=False):
+    ct = ctypes.c_float
+    f = ref().ref_tod2map_f32_mt if use_ref else lib().oracle_tod2map_f32_mt
+    return f(_ptr(lmap, ct), _ptr(tod, ct), _ptr(xpointing, ct), _nsamp(xpointing), lmap.size,
+             ctypes.byref(lpix.struct), int(partial_pixelization), int(nthreads))
+
+
+def response_map2tod(tod, lmap, xpointing, response, lpix, partial_pixelization=False, accum=False):
+    ndet = response.shape[1]
+    nsamp = _nsamp(xpointing)
+    ct = ctypes.c_float
+    return lib().oracle_response_map2tod_f32(
+        _ptr(tod, ct), _ptr(lmap, ct), _ptr(xpointing, ct), _ptr(np.ascontiguousarray(response), ct),
+        ndet, nsamp // ndet, ctypes.byref(lpix.struct), int(partial_pixelization), int(accum))
+
+
+def response_tod2map(lmap, tod, xpointing, response, lpix, partial_pixelization=False):
+    ndet = response.shape[1]
+    nsamp = _nsamp(xpointing)
+    ct = ctypes.c_float
+    return lib().oracle_response_tod2map_f32(
+        _ptr(lmap, ct), _ptr(tod, ct), _ptr(xpointing, ct), _ptr(np.ascontiguousarray(response), ct),
+        ndet, nsamp // ndet, ctypes.byref(lpix.struct), int(partial_pixelization))
+
+
+def locate(y, x, ny, nx, periodic, use_ref=False):
+    idx = (ctypes.c_int32 * 4)()
+    d = (ctypes.c_float * 2)()
+    f = ref().ref_locate_f32 if use_ref else lib().oracle_locate_f32
+    err = f(float(y), float(x), int(ny), int(nx), int(periodic), idx, d)
+    return tuple(idx), (np.float32(d[0]), np.float32(d[1])), err
+
+
+def preplan(xpointing, nypix_global, nxpix_global, periodic_xcoord=True):
+    """Returns dict(nmt, nmt_cumsum[1024], ncl_per_threadblock, planner_nblocks,
+    nmt_per_threadblock, pointing_nblocks, err)  (PointingPrePlan.cu:129-251)."""
+    xp = np.ascontiguousarray(xpointing, dtype=np.float32)
+    cum = np.zeros(1024, dtype=np.uint32)
+    geom = np.zeros(4, dtype=np.int64)
+    err = np.zeros(1, dtype=np.uint32)
+    nmt = lib().oracle_preplan(_ptr(xp, ctypes.c_float), _nsamp(xp), int(nypix_global), int(nxpix_global),
+                               int(periodic_xcoord), _ptr(cum, ctypes.c_uint32), _ptr(geom, ctypes.c_int64),
+                               _ptr(err, ctypes.c_uint32))
+    return dict(nmt=int(nmt), nmt_cumsum=cum, ncl_per_threadblock=int(geom[0]), planner_nblocks=int(geom[1]),
+                nmt_per_threadblock=int(geom[2]), pointing_nblocks=int(geom[3]), err=int(err[0]))
+
+
+def plan(xpointing, nypix_global, nxpix_global, periodic_xcoord=True, nmt=None):
+    """Canonical plan: (plan_mt uint64[nmt] sorted by (cell, cache line) with exact mflag/zflag,
+    owner_bits uint32[ceil(nmt/32)], err)."""
+    xp = np.ascontiguousarray(xpointing, dtype=np.float32)
+    if nmt is None:
+        nmt = preplan(xp, nypix_global, nxpix_global, periodic_xcoord)["nmt"]
+    mt = np.zeros(max(nmt, 1), dtype=np.uint64)
+    owner = np.zeros(max((nmt + 31) // 32, 1), dtype=np.uint32)
+    err = lib().oracle_plan(_ptr(xp, ctypes.c_float), _nsamp(xp), int(nypix_global), int(nxpix_global),
+                            int(periodic_xcoord), int(nmt), _ptr(mt, ctypes.c_uint64), _ptr(owner, ctypes.c_uint32))
+    return mt[:nmt], owner[:(nmt + 31) // 32], int(err)
+
+
+def sample_slots(xpointing, nypix_global, nxpix_global, periodic_xcoord=True):
+    xp = np.ascontiguousarray(xpointing, dtype=np.float32)
+    n = _nsamp(xp)
+    out = np.zeros(6 * n, dtype=np.int32)
+    lib().oracle_sample_slots(_ptr(xp, ctypes.c_float), n, int(nypix_global), int(nxpix_global),
+                              int(periodic_xcoord), _ptr(out, ctypes.c_int32))
+    return out.reshape(n, 6)
+
+
+def line_counts(xpointing, nypix_global, nxpix_global, periodic_xcoord=True):
+    xp = np.ascontiguousarray(xpointing, dtype=np.float32)
+    n = _nsamp(xp)
+    out = np.zeros(n // 32, dtype=np.uint8)
+    lib().oracle_line_counts(_ptr(xp, ctypes.c_float), n, int(nypix_global), int(nxpix_global),
+                             int(periodic_xcoord), _ptr(out, ctypes.c_uint8))
+    return out
+
+
+def rel_l1(a, b):
+    """The reference's comparison metric, sum|a-b| / (sum|a| + sum|b|)  (tests.py:220-224)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = np.abs(a).sum() + np.abs(b).sum()
+    assert den > 0
+    return float(np.abs(a - b).sum() / den)

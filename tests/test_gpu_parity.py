@@ -1,0 +1,412 @@
+"""GPU parity tests: the sm_100a path (through the drop-in Python API and through the C ABI) against
+the oracle, on the reference's own golden vectors and on seeded synthetic scans.
+
+Tolerances (float32 operators): rel-L1 = sum|a-b| / (sum|a|+sum|b|) < 1e-6, the reference's metric
+(tests.py:220-224, :277, :326), and max|a-b| / max|b| < 1e-5.  Plans are compared bit for bit.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from tests._common import random_raster, rel_stats
+
+pytestmark = pytest.mark.gpu
+
+RL1_TOL = 1e-6
+MAX_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def g():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import gpu_mm_b200
+    return gpu_mm_b200
+
+
+def cuda(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+def build_plan(g, xp_gpu, ny, nx, periodic):
+    pp = g.PointingPrePlan(xp_gpu, ny, nx, periodic_xcoord=periodic)
+    return pp, g.PointingPlan(pp, xp_gpu)
+
+
+def check_plan(g, xp, ny, nx, periodic, pp, plan):
+    ref = oracle.preplan(xp, ny, nx, periodic)
+    assert pp.plan_nmt == ref["nmt"]
+    for k in ("ncl_per_threadblock", "planner_nblocks", "nmt_per_threadblock", "pointing_nblocks"):
+        assert getattr(pp, k) == ref[k], k
+    np.testing.assert_array_equal(pp.get_nmt_cumsum(), ref["nmt_cumsum"][:pp.planner_nblocks])
+    mt_ref, owner_ref, err = oracle.plan(xp, ny, nx, periodic, nmt=ref["nmt"])
+    assert err == 0
+    mt = plan.get_plan_mt()
+    np.testing.assert_array_equal(mt, mt_ref)   # all 64 bits, canonical order
+    bits = np.unpackbits(owner_ref.view(np.uint8), bitorder="little")[:len(mt_ref)].astype(bool)
+    owner = plan._get_owner_mt()
+    np.testing.assert_array_equal(owner & np.uint64((1 << 46) - 1), mt_ref[bits] & np.uint64((1 << 46) - 1))
+
+
+def lpix_from(g, ny, nx, offs, ys, ps, periodic):
+    return g.LocalPixelization(ny, nx, offs, ys, ps, periodic)
+
+
+GOLDEN = ("wrap_rect", "flat_cells_accum", "partial_missing", "scattered")
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_golden_vectors(g, golden_ops, name):
+    """Planned and unplanned operators reproduce the reference header's outputs (golden vectors)."""
+    p = golden_ops[f"{name}__params"]
+    ny, nx, periodic, ys, ps, partial, accum = (int(p[0]), int(p[1]), bool(p[2]), int(p[3]), int(p[4]),
+                                                bool(p[5]), bool(p[6]))
+    xp = golden_ops[f"{name}__xpointing"]
+    lp = lpix_from(g, ny, nx, golden_ops[f"{name}__cell_offsets"], ys, ps, periodic)
+    xg = cuda(xp)
+    pp, plan = build_plan(g, xg, ny, nx, periodic)
+    check_plan(g, xp, ny, nx, periodic, pp, plan)
+    lmap = g.LocalMap(lp, cuda(golden_ops[f"{name}__map"].astype(np.float32)))
+    want = golden_ops[f"{name}__m2t_out"]
+    for pl in (plan, None):
+        tod = cuda(golden_ops[f"{name}__tod_init"].astype(np.float32))
+        g.map2tod(tod, lmap, xg, pl, partial_pixelization=partial, accum=accum)
+        rl1, mx = rel_stats(host(tod), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, (pl is None, rl1, mx)
+    want = golden_ops[f"{name}__t2m_out"]
+    for pl in (plan, None):
+        out = g.LocalMap(lp, cuda(np.zeros(3 * lp.npix, np.float32)))
+        g.tod2map(out, cuda(golden_ops[f"{name}__tod_in"].astype(np.float32)), xg, pl, partial_pixelization=partial)
+        rl1, mx = rel_stats(host(out.arr), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, (pl is None, rl1, mx)
+
+
+def test_golden_errors(g, golden_ops):
+    """Out-of-range y/x raise the reference's messages (check_arguments.cu:48-51), in the preplan
+    and in the unplanned operators."""
+    name = "errors"
+    p = golden_ops[f"{name}__params"]
+    ny, nx = int(p[0]), int(p[1])
+    xg = cuda(golden_ops[f"{name}__xpointing"])
+    with pytest.raises(RuntimeError, match="y-value is outside range"):
+        g.PointingPrePlan(xg, ny, nx, periodic_xcoord=False)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, False)
+    lmap = g.LocalMap(lp, cuda(golden_ops[f"{name}__map"].astype(np.float32)))
+    tod = cuda(np.zeros(golden_ops[f"{name}__tod_in"].shape, np.float32))
+    with pytest.raises(RuntimeError, match="y-value is outside range"):
+        g.map2tod(tod, lmap, xg, None)
+
+
+SYNTH = [
+    # (ny, nx, periodic, ndet, nt, speed, seed)
+    (300, 500, True, 8, 4096, 0.7, 0),
+    (300, 500, False, 8, 4096, 0.9, 1),
+    (130, 1000, True, 16, 2048, 1.0, 2),     # fast scan: lines span up to 33 px
+    (64, 64, True, 4, 1024, 0.3, 3),         # one cell, wrap inside it
+    (200, 90, True, 4, 1024, 2.5, 4),        # narrow map: x wraps every ~36 samples
+]
+
+
+@pytest.mark.parametrize("case", SYNTH)
+def test_synthetic_scans(g, case):
+    ny, nx, periodic, ndet, nt, speed, seed = case
+    rng = np.random.default_rng(1000 + seed)
+    xp = random_raster(rng, ndet, nt, ny, nx, periodic, speed=speed)
+    xg = cuda(xp)
+    pp, plan = build_plan(g, xg, ny, nx, periodic)
+    check_plan(g, xp, ny, nx, periodic, pp, plan)
+    lp_o = oracle.Lpix.rectangle(ny, nx, periodic)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, periodic)
+    m = rng.standard_normal(3 * lp.npix).astype(np.float32)
+    lmap = g.LocalMap(lp, cuda(m))
+    for accum in (False, True):
+        t0 = rng.standard_normal(xp.shape[1:]).astype(np.float32)
+        want = t0.copy()
+        oracle.map2tod(want, m, xp, lp_o, False, accum)
+        for pl in (plan, None):
+            tod = cuda(t0)
+            g.map2tod(tod, lmap, xg, pl, accum=accum)
+            rl1, mx = rel_stats(host(tod), want)
+            assert rl1 < RL1_TOL and mx < MAX_TOL, (accum, pl is None, rl1, mx)
+    t = rng.standard_normal(xp.shape[1:]).astype(np.float32)
+    m0 = rng.standard_normal(3 * lp.npix).astype(np.float32)
+    want = m0.copy()
+    oracle.tod2map(want, t, xp, lp_o)
+    for pl in (plan, None):
+        out = g.LocalMap(lp, cuda(m0))
+        g.tod2map(out, cuda(t), xg, pl)
+        rl1, mx = rel_stats(host(out.arr), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, (pl is None, rl1, mx)
+
+
+def test_partial_pixelization_and_missing_cells(g):
+    """Cells absent from the local map read as zero with partial_pixelization, and raise without it
+    (map2tod.cu:127-129, gpu_mm_internals.hpp:280)."""
+    rng = np.random.default_rng(77)
+    ny, nx = 256, 320
+    xp = random_raster(rng, 8, 2048, ny, nx, True, speed=0.8)
+    xg = cuda(xp)
+    pp, plan = build_plan(g, xg, ny, nx, True)
+    nyc, nxc = 4, 5
+    present = np.ones((nyc, nxc), bool)
+    present[1, 2] = present[2, 0] = present[0, 4] = False
+    offs = np.full((nyc, nxc), -1, np.int64)
+    k = 0
+    for iy in range(nyc):
+        for ix in range(nxc):
+            if present[iy, ix]:
+                offs[iy, ix] = 3 * 4096 * k
+                k += 1
+    lp = g.LocalPixelization(ny, nx, offs, 64, 4096, True)
+    lp_o = oracle.Lpix(ny, nx, offs, 64, 4096, True)
+    m = rng.standard_normal(3 * lp.npix).astype(np.float32)
+    lmap = g.LocalMap(lp, cuda(m))
+    want = np.zeros(xp.shape[1:], np.float32)
+    err = oracle.map2tod(want, m, xp, lp_o, False, False)   # same values as partial=True, plus the error bit
+    assert err & oracle.ERR_NOT_IN_PIXELIZATION   # the scan does touch a missing cell
+    for pl in (plan, None):
+        tod = cuda(np.zeros(xp.shape[1:], np.float32))
+        g.map2tod(tod, lmap, xg, pl, partial_pixelization=True)
+        rl1, mx = rel_stats(host(tod), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL
+        with pytest.raises(RuntimeError, match="not in LocalPixelization"):
+            g.map2tod(tod, lmap, xg, pl, partial_pixelization=False)
+    t = rng.standard_normal(xp.shape[1:]).astype(np.float32)
+    want = np.zeros(3 * lp.npix, np.float32)
+    oracle.tod2map(want, t, xp, lp_o, True)
+    for pl in (plan, None):
+        out = g.LocalMap(lp, cuda(np.zeros(3 * lp.npix, np.float32)))
+        g.tod2map(out, cuda(t), xg, pl, partial_pixelization=True)
+        rl1, mx = rel_stats(host(out.arr), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL
+        with pytest.raises(RuntimeError, match="not in LocalPixelization"):
+            g.tod2map(out, cuda(t), xg, pl, partial_pixelization=False)
+
+
+def test_response_variants(g):
+    """Per-detector (T, P) response (map2tod_response.cu, tod2map_response.cu), as in tests.py:295-354."""
+    rng = np.random.default_rng(31)
+    ny, nx = 200, 400
+    ndet, nt = 8, 2048
+    xp = random_raster(rng, ndet, nt, ny, nx, True)
+    xg = cuda(xp)
+    pp, plan = build_plan(g, xg, ny, nx, True)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, True)
+    lp_o = oracle.Lpix.rectangle(ny, nx, True)
+    resp = rng.uniform(0.5, 2.0, (2, ndet)).astype(np.float32)
+    m = rng.standard_normal(3 * lp.npix).astype(np.float32)
+    for accum in (False, True):
+        t0 = rng.standard_normal((ndet, nt)).astype(np.float32)
+        want = t0.copy()
+        oracle.response_map2tod(want, m, xp, resp, lp_o, False, accum)
+        tod = cuda(t0)
+        g.map2tod(tod, g.LocalMap(lp, cuda(m)), xg, plan, response=cuda(resp), accum=accum)
+        rl1, mx = rel_stats(host(tod), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL
+    t = rng.standard_normal((ndet, nt)).astype(np.float32)
+    want = np.zeros(3 * lp.npix, np.float32)
+    oracle.response_tod2map(want, t, xp, resp, lp_o)
+    out = g.LocalMap(lp, cuda(np.zeros(3 * lp.npix, np.float32)))
+    g.tod2map(out, cuda(t), xg, plan, response=cuda(resp))
+    rl1, mx = rel_stats(host(out.arr), want)
+    assert rl1 < RL1_TOL and mx < MAX_TOL
+
+
+def test_config1_full_size(g):
+    """The small benchmark configuration (2^22 samples, 3x1024x2048 map) end to end against the oracle."""
+    from gpu_mm_b200 import synthetic
+    c = synthetic.config1(device="cpu")
+    xp = c["xpointing"].numpy()
+    ny, nx = c["nypix"], c["nxpix"]
+    xg = cuda(xp)
+    pp, plan = build_plan(g, xg, ny, nx, True)
+    check_plan(g, xp, ny, nx, True, pp, plan)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, True)
+    lp_o = oracle.Lpix.rectangle(ny, nx, True)
+    m = c["map"].numpy().reshape(-1)
+    want = np.zeros(xp.shape[1:], np.float32)
+    oracle.map2tod(want, m, xp, lp_o)
+    lmap = g.LocalMap(lp, cuda(m))
+    for pl in (plan, None):
+        tod = cuda(np.zeros(xp.shape[1:], np.float32))
+        g.map2tod(tod, lmap, xg, pl)
+        rl1, mx = rel_stats(host(tod), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, (pl is None, rl1, mx)
+    t = c["tod"].numpy()
+    want = np.zeros(3 * lp.npix, np.float32)
+    oracle.tod2map(want, t, xp, lp_o)
+    for pl in (plan, None):
+        out = g.LocalMap(lp, cuda(np.zeros(3 * lp.npix, np.float32)))
+        g.tod2map(out, cuda(t), xg, pl)
+        rl1, mx = rel_stats(host(out.arr), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, (pl is None, rl1, mx)
+
+
+def test_plan_reuse_and_buffers(g):
+    """Caller-supplied buffers (gpu_mm.py:1253-1299): one shared tmp_buf for several plans; a plan is
+    reusable across calls and gives identical results."""
+    import torch
+    rng = np.random.default_rng(8)
+    ny, nx = 256, 256
+    xps = [random_raster(rng, 4, 1024, ny, nx, True) for _ in range(3)]
+    tmp_pp = torch.empty(1024, dtype=torch.int32, device="cuda")
+    plans = []
+    tmp = None
+    for xp in xps:
+        xg = cuda(xp)
+        pp = g.PointingPrePlan(xg, ny, nx, buf=torch.empty(1024, dtype=torch.int32, device="cuda"), tmp_buf=tmp_pp)
+        if tmp is None or tmp.numel() < pp.plan_constructor_tmp_nbytes:
+            tmp = torch.empty(2 * pp.plan_constructor_tmp_nbytes, dtype=torch.uint8, device="cuda")
+        plan = g.PointingPlan(pp, xg, buf=torch.empty(pp.plan_nbytes, dtype=torch.uint8, device="cuda"), tmp_buf=tmp)
+        plans.append((xp, xg, pp, plan))
+    for xp, xg, pp, plan in plans:
+        check_plan(g, xp, ny, nx, True, pp, plan)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, True)
+    lmap = g.LocalMap(lp, cuda(rng.standard_normal(3 * lp.npix).astype(np.float32)))
+    xp, xg, pp, plan = plans[0]
+    outs = []
+    for _ in range(3):
+        tod = cuda(np.zeros(xp.shape[1:], np.float32))
+        g.map2tod(tod, lmap, xg, plan)
+        outs.append(host(tod))
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+def test_dynamic_map(g):
+    """DynamicMap grown chunk by chunk, randomly permuted and finalized equals the reference
+    tod2map on a global map (tests.py:356-411)."""
+    rng = np.random.default_rng(12)
+    ny, nx = 300, 700
+    xp = random_raster(rng, 4, 4096, ny, nx, True, speed=0.6)
+    t = rng.standard_normal((4, 4096)).astype(np.float32)
+    lp_o = oracle.Lpix.rectangle(ny, nx, True)
+    ref = np.zeros(3 * lp_o.npix, np.float32)
+    oracle.tod2map(ref, t, xp, lp_o)
+    nyc, nxc = lp_o.nycells, lp_o.nxcells
+    ref_global = ref.reshape(3, 64 * nyc, 64 * nxc)[:, :ny, :nx]
+    dmap = g.DynamicMap(ny, nx, np.float32, initial_ncells=1)
+    for a, b in ((0, 1024), (1024, 1056), (1056, 4096)):
+        xc = cuda(np.ascontiguousarray(xp[:, :, a:b]))
+        pp = g.PointingPrePlan(xc, ny, nx)
+        plan = g.PointingPlan(pp, xc)
+        g.tod2map(dmap, cuda(np.ascontiguousarray(t[:, a:b])), xc, plan)
+    dmap.randomly_permute()
+    lmap = dmap.finalize()
+    got = lmap.to_global()
+    rl1, mx = rel_stats(got, ref_global)
+    assert rl1 < RL1_TOL and mx < MAX_TOL
+
+
+def test_reference_cpu_operators(g):
+    """plan='reference' runs the library's CPU operator and agrees with the oracle."""
+    rng = np.random.default_rng(4)
+    ny, nx = 100, 200
+    xp = random_raster(rng, 2, 512, ny, nx, True)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, True)
+    lp_o = oracle.Lpix.rectangle(ny, nx, True)
+    m = rng.standard_normal(3 * lp.npix).astype(np.float32)
+    tod = np.zeros(xp.shape[1:], np.float32)
+    g.map2tod(tod, g.LocalMap(lp, m), xp, 'reference')
+    want = np.zeros_like(tod)
+    oracle.map2tod(want, m, xp, lp_o)
+    np.testing.assert_allclose(tod, want, rtol=1e-6, atol=1e-6)
+
+
+def test_reference_enumerator_on_gpu(g):
+    """The oracle's cell slots equal the reference's own device-only cell_enumerator, run on the GPU
+    from oracle/_ref (skipped where that library was not built)."""
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built")
+    import torch
+    rng = np.random.default_rng(21)
+    for (ny, nx, periodic) in ((300, 400, True), (300, 400, False), (70, 64, True)):
+        n = 8192
+        xp = np.zeros((3, n), np.float32)
+        xp[0] = rng.uniform(0, ny - 1, n)
+        lo, hi = ((-nx, 2 * nx) if periodic else (0, nx - 2))
+        xp[1] = rng.uniform(lo, hi, n)
+        xp[1, :64] = np.clip(np.arange(64) * 64.0 - 1.0, lo, hi)
+        xg = cuda(xp)
+        slots = torch.zeros(6 * n, dtype=torch.int32, device="cuda")
+        errs = torch.zeros(n, dtype=torch.int32, device="cuda")
+        rc = oracle.ref().ref_enumerate_gpu(xg.data_ptr(), n, ny, nx, int(periodic), slots.data_ptr(), errs.data_ptr())
+        assert rc == 0
+        np.testing.assert_array_equal(host(slots).reshape(n, 6), oracle.sample_slots(xp, ny, nx, periodic))
+
+
+def test_c_abi_direct(g):
+    """Calls libgpu_mm_b200.so through ctypes with device pointers (the boundary a cgo/JNI/ctypes user
+    binds), including the deferred error word."""
+    import torch
+    L = ctypes.CDLL(g.library_path())
+    L.gmm_last_error.restype = ctypes.c_char_p
+
+    class Info(ctypes.Structure):
+        _fields_ = [("nsamp", ctypes.c_int64), ("nypix_global", ctypes.c_int32), ("nxpix_global", ctypes.c_int32),
+                    ("periodic_xcoord", ctypes.c_int32), ("sort_digit_bits", ctypes.c_int32),
+                    ("plan_nbytes", ctypes.c_int64), ("plan_constructor_tmp_nbytes", ctypes.c_int64),
+                    ("overhead", ctypes.c_double), ("ncl_per_threadblock", ctypes.c_int64),
+                    ("planner_nblocks", ctypes.c_int64), ("nmt_per_threadblock", ctypes.c_int64),
+                    ("pointing_nblocks", ctypes.c_int64), ("plan_nmt", ctypes.c_int64), ("sort_nbytes", ctypes.c_int64)]
+
+    class Lpix(ctypes.Structure):
+        _fields_ = [("nypix_global", ctypes.c_int32), ("nxpix_global", ctypes.c_int32),
+                    ("periodic_xcoord", ctypes.c_int32), ("nycells", ctypes.c_int32), ("nxcells", ctypes.c_int32),
+                    ("reserved", ctypes.c_int32), ("ystride", ctypes.c_int64), ("polstride", ctypes.c_int64),
+                    ("npix", ctypes.c_int64), ("cell_offsets", ctypes.c_void_p)]
+
+    rng = np.random.default_rng(2)
+    ny, nx = 256, 512
+    xp = random_raster(rng, 4, 2048, ny, nx, True)
+    nsamp = xp.size // 3
+    xg = cuda(xp)
+    nmt = torch.zeros(1024, dtype=torch.int32, device="cuda")
+    err = torch.zeros(1024, dtype=torch.int32, device="cuda")
+    info = Info()
+    rc = L.gmm_preplan(ctypes.c_void_p(xg.data_ptr()), ctypes.c_int64(nsamp), ny, nx, 1, ctypes.c_void_p(nmt.data_ptr()),
+                       ctypes.c_void_p(err.data_ptr()), 0, None, ctypes.byref(info))
+    assert rc == 0, L.gmm_last_error()
+    buf = torch.empty(info.plan_nbytes, dtype=torch.uint8, device="cuda")
+    tmp = torch.empty(info.plan_constructor_tmp_nbytes, dtype=torch.uint8, device="cuda")
+    rc = L.gmm_plan_build(ctypes.byref(info), ctypes.c_void_p(nmt.data_ptr()), ctypes.c_void_p(xg.data_ptr()),
+                          ctypes.c_void_p(buf.data_ptr()), ctypes.c_int64(buf.numel()), ctypes.c_void_p(tmp.data_ptr()),
+                          ctypes.c_int64(tmp.numel()), 0, None)
+    assert rc == 0, L.gmm_last_error()
+    mt_ref, _, _ = oracle.plan(xp, ny, nx, True)
+    np.testing.assert_array_equal(host(buf[:8 * info.plan_nmt].view(torch.int64)).view(np.uint64), mt_ref)
+
+    lp_o = oracle.Lpix.rectangle(ny, nx, True)
+    offs = cuda(lp_o.cell_offsets)
+    lp = Lpix(ny, nx, 1, lp_o.nycells, lp_o.nxcells, 0, lp_o.ystride, lp_o.polstride, lp_o.npix, offs.data_ptr())
+    m = rng.standard_normal(3 * lp_o.npix).astype(np.float32)
+    mg = cuda(m)
+    tod = torch.zeros(nsamp, dtype=torch.float32, device="cuda")
+    word = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = L.gmm_planned_map2tod(ctypes.c_void_p(tod.data_ptr()), ctypes.c_void_p(mg.data_ptr()),
+                               ctypes.c_void_p(xg.data_ptr()), ctypes.byref(lp), ctypes.byref(info),
+                               ctypes.c_void_p(buf.data_ptr()), 0, 0, ctypes.c_void_p(word.data_ptr()), None)
+    assert rc == 0
+    assert L.gmm_errword_read(ctypes.c_void_p(word.data_ptr()), 0, None) == 0
+    want = np.zeros(nsamp, np.float32)
+    oracle.map2tod(want, m, xp, lp_o)
+    rl1, mx = rel_stats(host(tod), want)
+    assert rl1 < RL1_TOL and mx < MAX_TOL
+    # Missing cells raise bit 8 through the deferred word.
+    offs2 = np.full_like(lp_o.cell_offsets, -1)
+    og = cuda(offs2)
+    lp.cell_offsets = og.data_ptr()
+    rc = L.gmm_planned_map2tod(ctypes.c_void_p(tod.data_ptr()), ctypes.c_void_p(mg.data_ptr()),
+                               ctypes.c_void_p(xg.data_ptr()), ctypes.byref(lp), ctypes.byref(info),
+                               ctypes.c_void_p(buf.data_ptr()), 0, 0, ctypes.c_void_p(word.data_ptr()), None)
+    assert rc == 0
+    assert L.gmm_errword_read(ctypes.c_void_p(word.data_ptr()), 0, None) == 8
+    assert L.gmm_errword_read(ctypes.c_void_p(word.data_ptr()), 8, None) == 0
