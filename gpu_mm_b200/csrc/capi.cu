@@ -41,6 +41,7 @@ thread_local std::string g_last_error;
 int g_sort_max_digit_bits = 8;
 
 constexpr int kSortGridMax = 320;
+constexpr int64_t kCellmapBytes = (1 << 20) / 8;   // one bit per possible cell
 
 int fail(int code, const std::string &msg)
 {
@@ -150,6 +151,9 @@ OpArgs make_args(const gmm_lpix *lp, const float *xp, int64_t nsamp, bool partia
     a.response = nullptr;
     a.ndet = 1;
     a.nperdet = nsamp;
+    a.det_m = 0;
+    a.det_sh1 = 0;
+    a.det_sh2 = 0;
     a.cell_offsets = lp->cell_offsets;
     a.nsamp = nsamp;
     a.ny = lp->nypix_global;
@@ -163,6 +167,17 @@ OpArgs make_args(const gmm_lpix *lp, const float *xp, int64_t nsamp, bool partia
     a.accum = accum;
     a.errword = errword;
     return a;
+}
+
+// Magic numbers for unsigned 32-bit division by d (Granlund & Montgomery 1994, round-up variant):
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1, q = (t + ((n - t) >> min(l,1))) >> max(l-1,0).
+void set_divisor(OpArgs &a, uint32_t d)
+{
+    int l = 0;
+    while ((1ull << l) < d) l++;
+    a.det_m = (uint32_t) (((1ull << 32) * ((1ull << l) - d)) / d + 1);
+    a.det_sh1 = std::min(l, 1);
+    a.det_sh2 = std::max(l - 1, 0);
 }
 
 int check_plan_vs_lpix(const gmm_lpix *lp, const gmm_preplan_info *info, const char *where)
@@ -231,7 +246,7 @@ int gmm_preplan_info_init(int64_t nsamp, int32_t ny, int32_t nx, int32_t periodi
 
     const int64_t ncl = nsamp / 32;
     const int64_t max_nblocks = std::max(info->planner_nblocks, info->pointing_nblocks);
-    info->plan_nbytes = align128(8 * nmt) + align128(4 * max_nblocks) + align128(8 * ncl);
+    info->plan_nbytes = align128(8 * nmt) + align128(4 * max_nblocks) + align128(8 * ncl) + kCellmapBytes;
     info->plan_constructor_tmp_nbytes = align128(8 * nmt) + align128(8 * ncl) + info->sort_nbytes;
     return 0;
 }
@@ -244,7 +259,8 @@ int gmm_plan_layout_get(const gmm_preplan_info *info, gmm_plan_layout *layout)
     layout->mt_offset = 0;
     layout->err_offset = align128(8 * info->plan_nmt);
     layout->owner_offset = layout->err_offset + align128(4 * max_nblocks);
-    layout->total_nbytes = layout->owner_offset + align128(8 * (info->nsamp / 32));
+    layout->cellmap_offset = layout->owner_offset + align128(8 * (info->nsamp / 32));
+    layout->total_nbytes = layout->cellmap_offset + kCellmapBytes;
     return 0;
 }
 
@@ -302,6 +318,7 @@ int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum, con
     uint64_t *plan_mt = (uint64_t *) (b + lay.mt_offset);
     uint32_t *errflags = (uint32_t *) (b + lay.err_offset);
     uint64_t *owner = (uint64_t *) (b + lay.owner_offset);
+    uint32_t *cellmap = (uint32_t *) (b + lay.cellmap_offset);
     const int64_t nmt = info->plan_nmt, ncl = info->nsamp / 32;
     char *t = (char *) tmp;
     uint64_t *mt_alt = (uint64_t *) t;
@@ -325,6 +342,10 @@ int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum, con
         e = radix_sort_mt(even ? plan_mt : mt_alt, even ? mt_alt : plan_mt, nmt, nyc, nxc, dbits, passes, hist, stream);
     if (e == cudaSuccess)
         e = radix_sort_mt(even ? owner : owner_alt, even ? owner_alt : owner, ncl, nyc, nxc, dbits, passes, hist, stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(cellmap, 0, kCellmapBytes, stream);
+    if (e == cudaSuccess)
+        e = launch_plan_cellmap(plan_mt, nmt, cellmap, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, where);
 
@@ -360,6 +381,7 @@ static int planned_op(bool tod2map, float *out, const float *in, const float *xp
     gmm_plan_layout_get(info, &lay);
     const char *b = (const char *) plan_buf;
     const uint64_t *owner = (const uint64_t *) (b + lay.owner_offset);
+    const uint32_t *cellmap = (const uint32_t *) (b + lay.cellmap_offset);
     uint32_t *word = errword ? errword : (uint32_t *) (b + lay.err_offset);
 
     OpArgs a = make_args(lp, xp, info->nsamp, partial != 0, accum != 0, word);
@@ -369,11 +391,12 @@ static int planned_op(bool tod2map, float *out, const float *in, const float *xp
         a.response = response;
         a.ndet = ndet;
         a.nperdet = info->nsamp / ndet;
+        set_divisor(a, (uint32_t) a.nperdet);
     }
     cudaError_t e = cudaMemsetAsync(word, 0, sizeof(uint32_t), stream);
     if (e == cudaSuccess)
-        e = tod2map ? launch_planned_tod2map(a, owner, info->nsamp / 32, stream)
-                    : launch_planned_map2tod(a, owner, info->nsamp / 32, stream);
+        e = tod2map ? launch_planned_tod2map(a, owner, info->nsamp / 32, cellmap, stream)
+                    : launch_planned_map2tod(a, owner, info->nsamp / 32, cellmap, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, where);
     if (errword)

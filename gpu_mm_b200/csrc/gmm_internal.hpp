@@ -24,6 +24,7 @@ cudaError_t launch_preplan(const float *xp, int64_t nsamp, int ny, int nx, bool 
 cudaError_t launch_plan_emit(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
                              int nblocks, const uint32_t *nmt_cumsum, uint64_t *mt_out, uint64_t *owner_out,
                              uint32_t *errflags, cudaStream_t stream);
+cudaError_t launch_plan_cellmap(const uint64_t *plan_mt, int64_t nmt, uint32_t *cellmap, cudaStream_t stream);
 cudaError_t launch_expand_dynamic_map(uint32_t *global_ncells, int64_t *cell_offsets, int nycells, int nxcells,
                                       const uint64_t *plan_mt, int64_t nmt, cudaStream_t stream);
 
@@ -34,6 +35,10 @@ struct OpArgs {
     const float *xp;        // xpointing [3][nsamp]
     const float *response;  // [2][ndet] or nullptr
     int64_t ndet, nperdet;
+    // sample -> detector index as a multiply-high (Granlund & Montgomery, "Division by invariant
+    // integers using multiplication", PLDI 1994): det = (t + ((s - t) >> sh1)) >> sh2, t = umulhi(m, s).
+    uint32_t det_m;
+    int det_sh1, det_sh2;
     const int64_t *cell_offsets;
     int64_t nsamp;
     int ny, nx;
@@ -44,8 +49,10 @@ struct OpArgs {
     uint32_t *errword;
 };
 
-cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream);
-cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream);
+cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                   cudaStream_t stream);
+cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                   cudaStream_t stream);
 cudaError_t launch_unplanned_map2tod(const OpArgs &a, cudaStream_t stream);
 cudaError_t launch_unplanned_tod2map(const OpArgs &a, cudaStream_t stream);
 

@@ -7,15 +7,19 @@
 //
 // Planned design (this implementation's own):
 //  * Every 32-sample cache line is processed exactly once, by the CTA that holds its "owner" cell
-//    (the lowest cell the line touches).  The plan carries that owner list sorted by cell, so a CTA
-//    walks a contiguous slice of it and reloads its tile only when the cell changes.
+//    (the lowest cell the line touches).  The plan carries that owner list sorted by cell; a CTA
+//    walks a contiguous slice of it.  Its warps walk the slice independently and meet at a barrier
+//    only when the cell changes, which is when the tile is reloaded (map2tod) or flushed (tod2map).
 //  * The tile is the owner cell plus a halo: rows [0, 64+HY) and columns [-HX, 64+HX) around the
 //    cell, in unwrapped x.  A line's whole bilinear footprint normally fits, so no cache line is
-//    read twice, no TOD word needs an atomic, and no pre-zeroing pass is needed.  Samples that do not
-//    fit take an exact fallback through global memory.
-//  * map2tod stages the tile (T, Q, U planes, padded row stride) from global memory; tod2map
-//    accumulates into it with shared-memory atomics and flushes each tile to the map once, skipping
-//    all-zero pixels.
+//    read twice, no TOD word needs an atomic, and no pre-zeroing pass is needed.  Samples that do
+//    not fit take an exact path through global memory.
+//  * Absent cells read as zero.  The not-in-pixelization error is decided per plan cell (the plan
+//    carries a bitmap of its cells), exactly the reference's condition, so the sample loop does no
+//    presence test.
+//  * tod2map accumulates into the tile with shared-memory atomics.  Adjacent samples usually hit
+//    the same pixel, so lane i adds T, Q and U in an order rotated by i mod 3: in one atomic
+//    instruction, neighbouring lanes then target different words.
 //  * xpointing and TOD are streamed with evict-first loads/stores so that the map and plan stay in
 //    L2; each warp keeps UNR cache lines in flight.
 #include <algorithm>
@@ -29,18 +33,14 @@ namespace {
 constexpr int HX = 32;                 // halo columns on each side
 constexpr int HY = 4;                  // halo rows below the cell
 constexpr int TY = 64 + HY;            // tile rows
-constexpr int TX = 64 + 2 * HX;        // tile columns (multiple of 32)
+constexpr int TX = 64 + 2 * HX;        // tile columns
 constexpr int TS = TX + 1;             // padded row stride in shared memory
 constexpr int PS = TY * TS;            // one polarisation plane
 constexpr int NW = 16;                 // warps per CTA
 constexpr int NT = NW * 32;
-constexpr int CH = 512;                // owner entries staged per chunk
 constexpr int UNR = 4;                 // cache lines in flight per warp
-constexpr int NPRES = TY * TX / 32;    // presence bitmap words
 constexpr size_t kTileBytes = 3 * (size_t) PS * sizeof(float);
-
-static_assert(TX % 32 == 0, "presence bitmap rows must be whole words");
-static_assert((TY * TX) % NT == 0, "tile sweep must cover whole warps");
+constexpr int kCellmapWords = (1 << 20) / 32;
 
 struct Tile {
     int gy0;   // global row of tile row 0
@@ -76,56 +76,33 @@ __device__ __forceinline__ int64_t global_pixel_offset(int iy, int ix, const OpA
     return off + (int64_t) (iy & 63) * a.ystride + (ix & 63);
 }
 
-__device__ __forceinline__ bool present_bit(const uint32_t *pres, int r, int c)
+__device__ __forceinline__ uint32_t detector_of(const OpArgs &a, uint32_t s)
 {
-    return (pres[r * (TX / 32) + (c >> 5)] >> (c & 31)) & 1u;
+    const uint32_t t = __umulhi(a.det_m, s);
+    return (t + ((s - t) >> a.det_sh1)) >> a.det_sh2;
 }
 
-// Per-sample response factors: (t_resp, p_resp) for the detector of sample s
+// Per-sample response factors (t_resp, p_resp) = (response[det], response[det+ndet])
 // (map2tod_response.cu:168-176).
-template<bool RESP>
-__device__ __forceinline__ void sample_response(const OpArgs &a, int64_t s, float &tr, float &pr)
+__device__ __forceinline__ void sample_response(const OpArgs &a, uint32_t s, float &tr, float &pr)
 {
-    if constexpr (RESP) {
-        const int64_t det = s / a.nperdet;
-        tr = __ldg(a.response + det);
-        pr = __ldg(a.response + det + a.ndet);
-    } else {
-        tr = 1.0f;
-        pr = 1.0f;
-    }
+    const uint32_t det = detector_of(a, s);
+    tr = __ldg(a.response + det);
+    pr = __ldg(a.response + det + a.ndet);
 }
 
-// Fills (map2tod) or clears (tod2map) the tile for cell 'cell' and its presence bitmap.
-template<bool LOAD>
-__device__ void prepare_tile(float *tile, uint32_t *pres, int *s_absent, uint32_t cell, Tile &T, const OpArgs &a,
-                             const float *__restrict__ lmap)
+// Loads the tile of 'cell' from the local map (absent pixels read as zero).
+__device__ void load_tile(float *tile, const Tile &T, const OpArgs &a, const float *__restrict__ lmap)
 {
-    const int iyc = (int) (cell >> 10), ixc = (int) (cell & 1023u);
-    T.gy0 = iyc << 6;
-    T.gx0 = (ixc << 6) - HX;
-    const int lane = threadIdx.x & 31;
-    bool any_absent = false;
     for (int idx = threadIdx.x; idx < TY * TX; idx += NT) {
         const int r = idx / TX, c = idx % TX;
         const int64_t off = tile_pixel_offset(r, c, T, a);
         const bool p = off >= 0;
-        if constexpr (LOAD) {
-            const float t = p ? __ldg(lmap + off) : 0.0f;
-            const float q = p ? __ldg(lmap + off + a.polstride) : 0.0f;
-            const float u = p ? __ldg(lmap + off + 2 * a.polstride) : 0.0f;
-            float *dst = tile + r * TS + c;
-            dst[0] = t;
-            dst[PS] = q;
-            dst[2 * PS] = u;
-        }
-        const unsigned bal = __ballot_sync(kFullMask, p);
-        if (lane == 0)
-            pres[idx >> 5] = bal;
-        any_absent |= !p;
+        float *dst = tile + r * TS + c;
+        dst[0] = p ? __ldg(lmap + off) : 0.0f;
+        dst[PS] = p ? __ldg(lmap + off + a.polstride) : 0.0f;
+        dst[2 * PS] = p ? __ldg(lmap + off + 2 * a.polstride) : 0.0f;
     }
-    if (__any_sync(kFullMask, any_absent) && (lane == 0))
-        *s_absent = 1;
 }
 
 // Adds the tile into the map (one atomic per non-zero pixel and polarisation) and clears it.
@@ -188,8 +165,8 @@ __device__ __forceinline__ void global_accum(const OpArgs &a, float *__restrict_
 
 // One sample of map2tod against the staged tile (or global memory if it does not fit).
 template<bool RESP>
-__device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, const uint32_t *pres, bool check,
-                                            const Tile &T, float y, float x, float al, int64_t s, uint32_t &err)
+__device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, const Tile &T, float y, float x,
+                                            float al, uint32_t s, uint32_t &err)
 {
     Located L;
     err |= locate(y, x, a.ny, a.nx, a.periodic, L);
@@ -198,7 +175,7 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
     float ct = 1.0f, cq = cs, cu = sn;
     if constexpr (RESP) {
         float tr, pr;
-        sample_response<true>(a, s, tr, pr);
+        sample_response(a, s, tr, pr);
         ct = tr;
         cq = pr * cs;
         cu = pr * sn;
@@ -218,16 +195,13 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
             e10 = p[TS] + cq * p[PS + TS] + cu * p[2 * PS + TS];
             e11 = p[TS + 1] + cq * p[PS + TS + 1] + cu * p[2 * PS + TS + 1];
         }
-        if (check) {
-            const bool ok = present_bit(pres, ry, rx) && present_bit(pres, ry, rx + 1) &&
-                            present_bit(pres, ry + 1, rx) && present_bit(pres, ry + 1, rx + 1);
-            err |= ok ? 0u : kErrNotInPixelization;
-        }
     } else {
-        e00 = global_eval(a, a.in, L.iy0, L.ix0, ct, cq, cu, err);
-        e01 = global_eval(a, a.in, L.iy0, L.ix1, ct, cq, cu, err);
-        e10 = global_eval(a, a.in, L.iy1, L.ix0, ct, cq, cu, err);
-        e11 = global_eval(a, a.in, L.iy1, L.ix1, ct, cq, cu, err);
+        // Absent cells are already reported through the plan's cell bitmap.
+        uint32_t unused = 0;
+        e00 = global_eval(a, a.in, L.iy0, L.ix0, ct, cq, cu, unused);
+        e01 = global_eval(a, a.in, L.iy0, L.ix1, ct, cq, cu, unused);
+        e10 = global_eval(a, a.in, L.iy1, L.ix0, ct, cq, cu, unused);
+        e11 = global_eval(a, a.in, L.iy1, L.ix1, ct, cq, cu, unused);
     }
     const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
     float r = (wy0 * wx0) * e00;
@@ -237,10 +211,11 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
     return r;
 }
 
+// One sample of tod2map.  o0..o2 are this lane's polarisation plane offsets in rotated order and
+// 'rot' selects the matching rotation of (t, q, u).
 template<bool RESP>
-__device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const uint32_t *pres, bool check,
-                                           const Tile &T, float y, float x, float al, float tv, int64_t s,
-                                           uint32_t &err)
+__device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const Tile &T, float y, float x, float al,
+                                           float tv, uint32_t s, int rot, int o0, int o1, int o2, uint32_t &err)
 {
     Located L;
     err |= locate(y, x, a.ny, a.nx, a.periodic, L);
@@ -249,7 +224,7 @@ __device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const u
     float t, q, u;
     if constexpr (RESP) {
         float tr, pr;
-        sample_response<true>(a, s, tr, pr);
+        sample_response(a, s, tr, pr);
         t = tr * tv;
         q = pr * tv * cs;
         u = pr * tv * sn;
@@ -262,130 +237,150 @@ __device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const u
     const float w00 = wy0 * wx0, w01 = wy0 * L.dx, w10 = L.dy * wx0, w11 = L.dy * L.dx;
     int ry, rx;
     if (tile_position(L, T, a, ry, rx)) {
-        float *p = tile + ry * TS + rx;
-        atomicAdd(p, w00 * t);
-        atomicAdd(p + PS, w00 * q);
-        atomicAdd(p + 2 * PS, w00 * u);
-        atomicAdd(p + 1, w01 * t);
-        atomicAdd(p + PS + 1, w01 * q);
-        atomicAdd(p + 2 * PS + 1, w01 * u);
-        atomicAdd(p + TS, w10 * t);
-        atomicAdd(p + PS + TS, w10 * q);
-        atomicAdd(p + 2 * PS + TS, w10 * u);
-        atomicAdd(p + TS + 1, w11 * t);
-        atomicAdd(p + PS + TS + 1, w11 * q);
-        atomicAdd(p + 2 * PS + TS + 1, w11 * u);
-        if (check) {
-            const bool ok = present_bit(pres, ry, rx) && present_bit(pres, ry, rx + 1) &&
-                            present_bit(pres, ry + 1, rx) && present_bit(pres, ry + 1, rx + 1);
+        const float v0 = (rot == 0) ? t : ((rot == 1) ? q : u);
+        const float v1 = (rot == 0) ? q : ((rot == 1) ? u : t);
+        const float v2 = (rot == 0) ? u : ((rot == 1) ? t : q);
+        const int p = ry * TS + rx;
+        float *p0 = tile + p + o0, *p1 = tile + p + o1, *p2 = tile + p + o2;
+        atomicAdd(p0, w00 * v0);
+        atomicAdd(p1, w00 * v1);
+        atomicAdd(p2, w00 * v2);
+        atomicAdd(p0 + 1, w01 * v0);
+        atomicAdd(p1 + 1, w01 * v1);
+        atomicAdd(p2 + 1, w01 * v2);
+        atomicAdd(p0 + TS, w10 * v0);
+        atomicAdd(p1 + TS, w10 * v1);
+        atomicAdd(p2 + TS, w10 * v2);
+        atomicAdd(p0 + TS + 1, w11 * v0);
+        atomicAdd(p1 + TS + 1, w11 * v1);
+        atomicAdd(p2 + TS + 1, w11 * v2);
+    } else {
+        uint32_t unused = 0;
+        global_accum(a, a.out, L.iy0, L.ix0, t, q, u, w00, unused);
+        global_accum(a, a.out, L.iy0, L.ix1, t, q, u, w01, unused);
+        global_accum(a, a.out, L.iy1, L.ix0, t, q, u, w10, unused);
+        global_accum(a, a.out, L.iy1, L.ix1, t, q, u, w11, unused);
+    }
+}
+
+// Not-in-pixelization check of the plan's cells (this CTA's share of the bitmap).
+__device__ uint32_t check_plan_cells(const uint32_t *__restrict__ cellmap, const OpArgs &a)
+{
+    uint32_t err = 0;
+    for (int w = blockIdx.x * NT + threadIdx.x; w < kCellmapWords; w += gridDim.x * NT) {
+        uint32_t bits = __ldg(cellmap + w);
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const int c = 32 * w + b;
+            const int iy = c >> 10, ix = c & 1023;
+            const bool ok = (iy < a.nycells) && (ix < a.nxcells) &&
+                            (__ldg(a.cell_offsets + (int64_t) iy * a.nxcells + ix) >= 0);
             err |= ok ? 0u : kErrNotInPixelization;
         }
-    } else {
-        global_accum(a, a.out, L.iy0, L.ix0, t, q, u, w00, err);
-        global_accum(a, a.out, L.iy0, L.ix1, t, q, u, w01, err);
-        global_accum(a, a.out, L.iy1, L.ix0, t, q, u, w10, err);
-        global_accum(a, a.out, L.iy1, L.ix1, t, q, u, w11, err);
     }
+    return err;
 }
 
 // Planned operator kernel.  TOD2MAP selects the direction; RESP the per-detector response.
 template<bool TOD2MAP, bool RESP>
 __global__ void __launch_bounds__(NT, 2)
-planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner)
+planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, const uint32_t *__restrict__ cellmap)
 {
     extern __shared__ float tile[];
-    __shared__ uint32_t pres[NPRES];
-    __shared__ uint64_t s_mt[CH];
-    __shared__ int s_absent;
+    __shared__ int s_run[2];
     __shared__ uint32_t s_err[NW];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t e0 = (nowner * (int64_t) blockIdx.x) / gridDim.x;
     const int64_t e1 = (nowner * (int64_t) (blockIdx.x + 1)) / gridDim.x;
-    const int64_t nsamp = a.nsamp;
-    uint32_t err = 0;
-    uint32_t cur = 0xffffffffu;
-    Tile T{0, 0};
+    const uint32_t nsamp = (uint32_t) a.nsamp;
+    uint32_t err = a.partial ? 0u : check_plan_cells(cellmap, a);
+
+    const int rot = lane % 3;
+    const int o0 = rot * PS, o1 = ((rot + 1) % 3) * PS, o2 = ((rot + 2) % 3) * PS;
 
     if constexpr (TOD2MAP) {
         for (int i = threadIdx.x; i < 3 * PS; i += NT)
             tile[i] = 0.0f;
     }
 
-    for (int64_t c0 = e0; c0 < e1; c0 += CH) {
-        const int n = (int) ((e1 - c0 < (int64_t) CH) ? (e1 - c0) : (int64_t) CH);
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += NT)
-            s_mt[i] = __ldg(owner_mt + c0 + i);
+    int64_t start = e0;
+    int parity = 0;
+    while (start < e1) {
+        const uint32_t cell = (uint32_t) (__ldg(owner_mt + start) & kCellMask);
+        Tile T;
+        T.gy0 = (int) (cell >> 10) << 6;
+        T.gx0 = ((int) (cell & 1023u) << 6) - HX;
+        if (threadIdx.x == 0)
+            s_run[parity] = (int) (e1 - start);
+        if constexpr (!TOD2MAP)
+            load_tile(tile, T, a, a.in);
         __syncthreads();
 
-        int i = 0;
-        while (i < n) {
-            const uint32_t cell = (uint32_t) (s_mt[i] & kCellMask);
-            int lo = i + 1, hi = n;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if ((uint32_t) (s_mt[mid] & kCellMask) == cell) lo = mid + 1; else hi = mid;
+        // Owner words are fetched one iteration ahead (lane u < UNR holds word k+u), so the owner
+        // load is not on the critical path of the pointing loads that depend on it.
+        int64_t k = start + warp * UNR;
+        uint64_t wnext = ((lane < UNR) && (k + lane < e1)) ? __ldg(owner_mt + k + lane) : 0ull;
+        for (; k < e1; k += NW * UNR) {
+            const uint64_t wcur = wnext;
+            const int64_t kn = k + NW * UNR;
+            wnext = ((lane < UNR) && (kn + lane < e1)) ? __ldg(owner_mt + kn + lane) : 0ull;
+            // The owner list is sorted by cell: the first entry of another cell ends this run for
+            // the whole CTA, and every later entry of this warp is past it as well.
+            bool ok[UNR];
+            bool foreign = false;
+            uint32_t s[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; u++) {
+                const int64_t idx = k + u;
+                const bool in = idx < e1;
+                const uint64_t w = __shfl_sync(kFullMask, wcur, u);
+                const bool same = in && ((uint32_t) (w & kCellMask) == cell);
+                if (in && !same && !foreign && (lane == 0))
+                    atomicMin(&s_run[parity], (int) (idx - start));
+                foreign = foreign || (in && !same);
+                // A plan word always names a line < nsamp/32; anything else means the plan does
+                // not belong to this xpointing, so flag it and read line 0 instead.
+                uint32_t line = (uint32_t) ((w >> 20) & kClMask);
+                const bool line_ok = line < (nsamp >> 5);
+                err |= (same && !line_ok) ? kErrInconsistentNmt : 0u;
+                ok[u] = same && !foreign && line_ok;
+                line = line_ok ? line : 0u;
+                s[u] = 32u * line + (uint32_t) lane;
             }
-            const int j = lo;
-
-            if (cell != cur) {
-                __syncthreads();
+            float y[UNR], x[UNR], al[UNR], tv[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; u++) {
+                y[u] = __ldcs(a.xp + s[u]);
+                x[u] = __ldcs(a.xp + nsamp + s[u]);
+                al[u] = __ldcs(a.xp + 2 * (size_t) nsamp + s[u]);
+                if constexpr (TOD2MAP)
+                    tv[u] = __ldcs(a.in + s[u]);
+                else
+                    tv[u] = (a.accum && ok[u]) ? a.out[s[u]] : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < UNR; u++) {
+                if (!ok[u])
+                    continue;
                 if constexpr (TOD2MAP) {
-                    if (cur != 0xffffffffu)
-                        flush_tile(tile, T, a, a.out);
-                }
-                if (threadIdx.x == 0)
-                    s_absent = 0;
-                __syncthreads();
-                prepare_tile<!TOD2MAP>(tile, pres, &s_absent, cell, T, a, a.in);
-                __syncthreads();
-                cur = cell;
-            }
-            const bool check = (s_absent != 0) && !a.partial;
-
-            for (int base = i + warp * UNR; base < j; base += NW * UNR) {
-                float y[UNR], x[UNR], al[UNR], tv[UNR];
-                int64_t s[UNR];
-                bool ok[UNR];
-#pragma unroll
-                for (int u = 0; u < UNR; u++) {
-                    const int k = min(base + u, j - 1);
-                    int64_t line = (int64_t) ((s_mt[k] >> 20) & kClMask);
-                    // A plan word always names a line < nsamp/32; anything else means the plan does not
-                    // belong to this xpointing, so flag it and read line 0 instead of out of range.
-                    ok[u] = (32 * line < nsamp) && (base + u < j);
-                    err |= (32 * line < nsamp) ? 0u : kErrInconsistentNmt;
-                    line = (32 * line < nsamp) ? line : 0;
-                    s[u] = 32 * line + lane;
-                    y[u] = __ldcs(a.xp + s[u]);
-                    x[u] = __ldcs(a.xp + nsamp + s[u]);
-                    al[u] = __ldcs(a.xp + 2 * nsamp + s[u]);
-                    if constexpr (TOD2MAP)
-                        tv[u] = __ldcs(a.in + s[u]);
-                    else
-                        tv[u] = a.accum ? a.out[s[u]] : 0.0f;
-                }
-#pragma unroll
-                for (int u = 0; u < UNR; u++) {
-                    if (!ok[u])
-                        continue;
-                    if constexpr (TOD2MAP) {
-                        t2m_sample<RESP>(a, tile, pres, check, T, y[u], x[u], al[u], tv[u], s[u], err);
-                    } else {
-                        const float r = m2t_sample<RESP>(a, tile, pres, check, T, y[u], x[u], al[u], s[u], err);
-                        __stcs(a.out + s[u], a.accum ? (tv[u] + r) : r);
-                    }
+                    t2m_sample<RESP>(a, tile, T, y[u], x[u], al[u], tv[u], s[u], rot, o0, o1, o2, err);
+                } else {
+                    const float r = m2t_sample<RESP>(a, tile, T, y[u], x[u], al[u], s[u], err);
+                    __stcs(a.out + s[u], a.accum ? (tv[u] + r) : r);
                 }
             }
-            i = j;
+            if (foreign)
+                break;
         }
-    }
-
-    if constexpr (TOD2MAP) {
         __syncthreads();
-        if (cur != 0xffffffffu)
+        const int64_t next = start + s_run[parity];
+        if constexpr (TOD2MAP)
             flush_tile(tile, T, a, a.out);
+        parity ^= 1;
+        __syncthreads();
+        start = next;
     }
     block_publish_err(err, s_err, a.errword);
 }
@@ -458,7 +453,8 @@ unplanned_kernel(OpArgs a)
 }
 
 template<bool TOD2MAP, bool RESP>
-cudaError_t launch_planned_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream)
+cudaError_t launch_planned_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                cudaStream_t stream)
 {
     if (nowner <= 0)
         return cudaSuccess;
@@ -470,10 +466,10 @@ cudaError_t launch_planned_impl(const OpArgs &a, const uint64_t *owner_mt, int64
             return e;
         attr_done = true;
     }
-    // Two CTAs per SM; never more CTAs than ~64 cache lines each, so small plans reload few tiles.
+    // Two CTAs per SM; never fewer than ~64 cache lines per CTA, so small plans reload few tiles.
     int64_t g = 2 * (int64_t) device_sm_count();
     g = std::max<int64_t>(1, std::min<int64_t>(g, (nowner + 63) / 64));
-    planned_kernel<TOD2MAP, RESP><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner);
+    planned_kernel<TOD2MAP, RESP><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner, cellmap);
     return cudaGetLastError();
 }
 
@@ -494,16 +490,18 @@ cudaError_t launch_unplanned_impl(const OpArgs &a, cudaStream_t stream)
 
 }  // namespace
 
-cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream)
+cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                   cudaStream_t stream)
 {
-    return a.response ? launch_planned_impl<false, true>(a, owner_mt, nowner, stream)
-                      : launch_planned_impl<false, false>(a, owner_mt, nowner, stream);
+    return a.response ? launch_planned_impl<false, true>(a, owner_mt, nowner, cellmap, stream)
+                      : launch_planned_impl<false, false>(a, owner_mt, nowner, cellmap, stream);
 }
 
-cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, cudaStream_t stream)
+cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                   cudaStream_t stream)
 {
-    return a.response ? launch_planned_impl<true, true>(a, owner_mt, nowner, stream)
-                      : launch_planned_impl<true, false>(a, owner_mt, nowner, stream);
+    return a.response ? launch_planned_impl<true, true>(a, owner_mt, nowner, cellmap, stream)
+                      : launch_planned_impl<true, false>(a, owner_mt, nowner, cellmap, stream);
 }
 
 cudaError_t launch_unplanned_map2tod(const OpArgs &a, cudaStream_t stream)

@@ -436,6 +436,23 @@ sort_downsweep_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ ou
 }
 
 // ------------------------------------------------------------------------------------------------
+// Cell bitmap of a sorted plan: one bit per cell that occurs in plan_mt.  The operators check it
+// against the local pixelization, which gives the reference's not-in-pixelization semantics (an
+// error iff the plan touches an absent cell, map2tod.cu:127-129) without any per-sample test.
+
+__global__ void __launch_bounds__(256)
+plan_cellmap_kernel(const uint64_t *__restrict__ plan_mt, int64_t nmt, uint32_t *__restrict__ cellmap)
+{
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nmt; i += stride) {
+        const uint32_t c = (uint32_t) (plan_mt[i] & kCellMask);
+        const uint32_t prev = (i > 0) ? (uint32_t) (plan_mt[i - 1] & kCellMask) : 0xffffffffu;
+        if (c != prev)
+            atomicOr(cellmap + (c >> 5), 1u << (c & 31));
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
 // Dynamic-map cell discovery (expand_dynamic_map.cu:18-102): the last word of every cell run in
 // the sorted plan is a candidate; targeted cells (offset -1) get the next free cell index.
 
@@ -565,6 +582,15 @@ cudaError_t launch_plan_emit(const float *xp, int64_t nsamp, int ny, int nx, boo
 {
     plan_emit_kernel<<<nblocks, kPlanWarps * 32, 0, stream>>>(xp, nsamp, ny, nx, periodic, nclpb, nmt_cumsum,
                                                                mt_out, owner_out, errflags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plan_cellmap(const uint64_t *plan_mt, int64_t nmt, uint32_t *cellmap, cudaStream_t stream)
+{
+    if (nmt <= 0)
+        return cudaSuccess;
+    const int64_t g = std::min<int64_t>((nmt + 255) / 256, 8 * (int64_t) device_sm_count());
+    plan_cellmap_kernel<<<(unsigned) g, 256, 0, stream>>>(plan_mt, nmt, cellmap);
     return cudaGetLastError();
 }
 

@@ -43,16 +43,18 @@ def raster_xpointing(ndet_y, ndet_x, nt, spacing, speed, nxpix, y0, ydrift, xlo=
         ys = y0 + ydrift * t
     else:
         ys = y0 + triangle(yspeed * t, float(yspan))
+    # One detector row at a time keeps the float64 temporaries at (ndet_x, nt).
+    j = torch.arange(ndet_x, dtype=torch.float64, device=device)[:, None]
     for i in range(ndet_y):
-        for j in range(ndet_x):
-            d = ndet_x * i + j
-            x = xs + spacing * j
-            if wrap_x:
-                x = torch.remainder(x, float(nxpix))
-            out[0, d] = (ys + spacing * i).to(dtype)
-            out[1, d] = x.to(dtype)
-            frac = torch.remainder(t / alpha_period + d / float(ndet), 1.0)
-            out[2, d] = (2.0 * math.pi * frac).to(dtype)
+        d = ndet_x * i + j
+        x = xs[None, :] + spacing * j
+        if wrap_x:
+            x = torch.remainder(x, float(nxpix))
+        rows = slice(ndet_x * i, ndet_x * (i + 1))
+        out[0, rows] = (ys[None, :] + spacing * i).to(dtype)
+        out[1, rows] = x.to(dtype)
+        frac = torch.remainder(t[None, :] / alpha_period + d / float(ndet), 1.0)
+        out[2, rows] = (2.0 * math.pi * frac).to(dtype)
     return out
 
 

@@ -81,6 +81,7 @@ typedef struct gmm_plan_layout {
     int64_t mt_offset;        /* uint64 plan_mt[plan_nmt], sorted by (cell, cache line) */
     int64_t err_offset;       /* uint32 err[max(planner_nblocks, pointing_nblocks)] */
     int64_t owner_offset;     /* uint64 owner_mt[nsamp/32]: one word per cache line, sorted */
+    int64_t cellmap_offset;   /* uint32 cellmap[2^20/32]: bit c set iff cell c occurs in plan_mt */
     int64_t total_nbytes;
 } gmm_plan_layout;
 

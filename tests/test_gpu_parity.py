@@ -192,11 +192,12 @@ def test_partial_pixelization_and_missing_cells(g):
             g.tod2map(out, cuda(t), xg, pl, partial_pixelization=False)
 
 
-def test_response_variants(g):
-    """Per-detector (T, P) response (map2tod_response.cu, tod2map_response.cu), as in tests.py:295-354."""
-    rng = np.random.default_rng(31)
+@pytest.mark.parametrize("ndet,nt", [(8, 2048), (6, 1056), (96, 24)])
+def test_response_variants(g, ndet, nt):
+    """Per-detector (T, P) response (map2tod_response.cu, tod2map_response.cu), as in tests.py:295-354;
+    detector lengths that are a power of two, not a power of two, and shorter than a cache line."""
+    rng = np.random.default_rng(31 + ndet)
     ny, nx = 200, 400
-    ndet, nt = 8, 2048
     xp = random_raster(rng, ndet, nt, ny, nx, True)
     xg = cuda(xp)
     pp, plan = build_plan(g, xg, ny, nx, True)
