@@ -201,6 +201,9 @@ extern "C" {
 
 const char *gmm_last_error(void) { return g_last_error.c_str(); }
 
+// Records 'msg' as this thread's last error and returns 'code' (for the library's other files).
+int gmm_fail_message(int code, const char *msg) { return fail(code, msg); }
+
 const char *gmm_version(void) { return "gpu_mm_b200 0.1.0 (sm_100a)"; }
 
 int gmm_set_sort_digit_bits(int32_t bits)

@@ -8,6 +8,8 @@
 #include "gmm_common.cuh"
 #include "../../include/gpu_mm_b200.h"
 
+extern "C" int gmm_fail_message(int code, const char *msg);
+
 namespace gmm {
 
 // Number of SMs of the current device (cached per device).

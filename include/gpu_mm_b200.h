@@ -120,6 +120,28 @@ int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum_gpu,
                    void *buf, int64_t buf_nbytes, void *tmp, int64_t tmp_nbytes, int32_t debug,
                    cudaStream_t stream);
 
+/* Plan construction for callers that cannot allocate device memory.  This entry point has no
+ * counterpart in the reference.  It is gmm_plan_build without the 'tmp' argument: its temporary
+ * storage (the unsorted mt words, the second owner-list buffer and the radix-sort histograms) lives
+ * in a static device array of GMM_NOALLOC_SCRATCH_BYTES (32 MiB) inside this library.  It is meant
+ * for hosts that must not call cudaMalloc -- real-time acquisition loops, code that hands out device
+ * memory from its own fixed pool, foreign-language runtimes without a device allocator -- and that
+ * still need to build plans.  The caller passes the inputs (preplan, nmt_cumsum, xpointing) and the
+ * output 'buf' as usual.
+ *  - Plans whose info->plan_constructor_tmp_nbytes exceeds GMM_NOALLOC_SCRATCH_BYTES are rejected
+ *    with GMM_ERR_BUFFER_TOO_SMALL; that covers up to roughly 2^24 samples at typical overheads.
+ *  - The array is reserved on every device where this library's module holding it has been loaded
+ *    and is kept until the process exits.
+ *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress); make
+ *    that first call before any stream capture.
+ *  - All calls share the one array.  Calls that overlap on the GPU (other streams, other host
+ *    threads) race on it and must be serialised by the caller.  Nothing in the array needs to
+ *    start at zero: every call overwrites what it reads.
+ * Allocates nothing. */
+#define GMM_NOALLOC_SCRATCH_BYTES (32ll << 20)
+int gmm_plan_build_noalloc(const gmm_preplan_info *info, const uint32_t *nmt_cumsum_gpu, const float *xpointing_gpu,
+                           void *buf, int64_t buf_nbytes, int32_t debug, cudaStream_t stream);
+
 /* Replaces launch_planned_map2tod<float> (gpu_mm.hpp:155-165, map2tod.cu:194-272). */
 int gmm_planned_map2tod(float *tod, const float *local_map, const float *xpointing, const gmm_lpix *lpix,
                         const gmm_preplan_info *info, const void *plan_buf, int32_t partial_pixelization,
