@@ -108,7 +108,24 @@ __device__ __forceinline__ void line_slot_masks(const int slots[6], unsigned ama
     }
 }
 
-__device__ __forceinline__ float ldcs(const float *p) { return __ldcs(p); }
+// sin(2a) and cos(2a) for the detector response.  2a is reduced to [-pi, pi] by a two-term
+// Cody-Waite split of 2*pi (W. J. Cody and W. Waite, "Software Manual for the Elementary
+// Functions", 1980): head 6.28125 (exact in 8 bits, so j*head is exact for |j| < 2^16) plus the
+// float tail 2*pi - 6.28125; then the hardware approximations __sinf/__cosf.  Absolute error
+// about 5e-7 against CUDA's sincosf for |2a| <= 1024 (the hardware approximations' own error
+// dominates; the tail term adds at most 163 * 2^-34 there); larger arguments use sincosf.
+__device__ __forceinline__ void sincos2a(float alpha, float *s, float *c)
+{
+    const float th = 2.0f * alpha;
+    if (fabsf(th) <= 1024.0f) {
+        const float j = rintf(th * 0.15915494309189535f);
+        float r = fmaf(j, -6.28125f, th);
+        r = fmaf(j, -1.9353071795864769e-3f, r);
+        __sincosf(r, s, c);
+    } else {
+        sincosf(th, s, c);
+    }
+}
 
 // OR-reduce an error word over the block and publish it with one atomicOr per block (only if
 // non-zero).  'scratch' needs blockDim.x/32 words; must be called by all threads of the block.

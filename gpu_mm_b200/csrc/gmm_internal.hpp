@@ -1,6 +1,7 @@
 // Internal declarations shared by the gpu_mm_b200 translation units.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <cuda_runtime.h>
@@ -50,6 +51,24 @@ struct OpArgs {
     bool partial, accum;
     uint32_t *errword;
 };
+
+// Raises a kernel's dynamic shared-memory limit, once per device: 'done' holds one bit per device
+// ordinal (ordinals >= 64 set it on every call).
+template<typename Kernel>
+cudaError_t set_smem_limit(Kernel k, size_t nbytes, std::atomic<uint64_t> &done)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return e;
+    const uint64_t bit = (dev < 64) ? (1ull << dev) : 0ull;
+    if (done.load(std::memory_order_acquire) & bit)
+        return cudaSuccess;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) nbytes);
+    if (e == cudaSuccess)
+        done.fetch_or(bit, std::memory_order_release);
+    return e;
+}
 
 cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                    cudaStream_t stream);

@@ -39,6 +39,7 @@ constexpr int PS = TY * TS;            // one polarisation plane
 constexpr int NW = 16;                 // warps per CTA
 constexpr int NT = NW * 32;
 constexpr int UNR = 4;                 // cache lines in flight per warp
+constexpr int CH = 4;                  // owner entries a warp decodes at once (a multiple of UNR)
 constexpr size_t kTileBytes = 3 * (size_t) PS * sizeof(float);
 constexpr int kCellmapWords = (1 << 20) / 32;
 
@@ -127,11 +128,12 @@ __device__ void flush_tile(float *tile, const Tile &T, const OpArgs &a, float *_
 }
 
 // Position of a located sample inside the tile; false if its footprint is not inside.
+template<bool PERIODIC>
 __device__ __forceinline__ bool tile_position(const Located &L, const Tile &T, const OpArgs &a, int &ry, int &rx)
 {
     ry = L.iy0 - T.gy0;
     rx = L.ix0 - T.gx0;
-    if (a.periodic) {
+    if constexpr (PERIODIC) {
         rx += (rx < 0) ? a.nx : 0;
         rx -= (rx > TX - 2) ? a.nx : 0;
     }
@@ -164,14 +166,14 @@ __device__ __forceinline__ void global_accum(const OpArgs &a, float *__restrict_
 }
 
 // One sample of map2tod against the staged tile (or global memory if it does not fit).
-template<bool RESP>
+template<bool RESP, bool PERIODIC>
 __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, const Tile &T, float y, float x,
                                             float al, uint32_t s, uint32_t &err)
 {
     Located L;
-    err |= locate(y, x, a.ny, a.nx, a.periodic, L);
+    err |= locate(y, x, a.ny, a.nx, PERIODIC, L);
     float sn, cs;
-    sincosf(2.0f * al, &sn, &cs);
+    sincos2a(al, &sn, &cs);
     float ct = 1.0f, cq = cs, cu = sn;
     if constexpr (RESP) {
         float tr, pr;
@@ -182,7 +184,7 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
     }
     int ry, rx;
     float e00, e01, e10, e11;
-    if (tile_position(L, T, a, ry, rx)) {
+    if (tile_position<PERIODIC>(L, T, a, ry, rx)) {
         const float *p = tile + ry * TS + rx;
         if constexpr (RESP) {
             e00 = ct * p[0] + cq * p[PS] + cu * p[2 * PS];
@@ -213,14 +215,14 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
 
 // One sample of tod2map.  o0..o2 are this lane's polarisation plane offsets in rotated order and
 // 'rot' selects the matching rotation of (t, q, u).
-template<bool RESP>
+template<bool RESP, bool PERIODIC>
 __device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const Tile &T, float y, float x, float al,
                                            float tv, uint32_t s, int rot, int o0, int o1, int o2, uint32_t &err)
 {
     Located L;
-    err |= locate(y, x, a.ny, a.nx, a.periodic, L);
+    err |= locate(y, x, a.ny, a.nx, PERIODIC, L);
     float sn, cs;
-    sincosf(2.0f * al, &sn, &cs);
+    sincos2a(al, &sn, &cs);
     float t, q, u;
     if constexpr (RESP) {
         float tr, pr;
@@ -236,7 +238,7 @@ __device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const T
     const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
     const float w00 = wy0 * wx0, w01 = wy0 * L.dx, w10 = L.dy * wx0, w11 = L.dy * L.dx;
     int ry, rx;
-    if (tile_position(L, T, a, ry, rx)) {
+    if (tile_position<PERIODIC>(L, T, a, ry, rx)) {
         const float v0 = (rot == 0) ? t : ((rot == 1) ? q : u);
         const float v1 = (rot == 0) ? q : ((rot == 1) ? u : t);
         const float v2 = (rot == 0) ? u : ((rot == 1) ? t : q);
@@ -282,8 +284,14 @@ __device__ uint32_t check_plan_cells(const uint32_t *__restrict__ cellmap, const
     return err;
 }
 
-// Planned operator kernel.  TOD2MAP selects the direction; RESP the per-detector response.
-template<bool TOD2MAP, bool RESP>
+// Planned operator kernel.  TOD2MAP selects the direction, RESP the per-detector response and
+// PERIODIC the x-wraparound.
+//
+// A warp takes CH consecutive owner entries at a time; lane i < CH decodes entry i, and two ballots
+// give the chunk's usable lines and the first entry of another cell (which ends the CTA's run).
+// The lines are then processed UNR at a time with one sample per lane, so the per-line decoding
+// costs a shuffle per sample.
+template<bool TOD2MAP, bool RESP, bool PERIODIC>
 __global__ void __launch_bounds__(NT, 2)
 planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, const uint32_t *__restrict__ cellmap)
 {
@@ -295,6 +303,10 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
     const int64_t e0 = (nowner * (int64_t) blockIdx.x) / gridDim.x;
     const int64_t e1 = (nowner * (int64_t) (blockIdx.x + 1)) / gridDim.x;
     const uint32_t nsamp = (uint32_t) a.nsamp;
+    const uint32_t nlines = nsamp >> 5;
+    const float *__restrict__ yrow = a.xp;
+    const float *__restrict__ xrow = a.xp + nsamp;
+    const float *__restrict__ arow = a.xp + 2 * (size_t) nsamp;
     uint32_t err = a.partial ? 0u : check_plan_cells(cellmap, a);
 
     const int rot = lane % 3;
@@ -318,60 +330,162 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
             load_tile(tile, T, a, a.in);
         __syncthreads();
 
-        // Owner words are fetched one iteration ahead (lane u < UNR holds word k+u), so the owner
-        // load is not on the critical path of the pointing loads that depend on it.
-        int64_t k = start + warp * UNR;
-        uint64_t wnext = ((lane < UNR) && (k + lane < e1)) ? __ldg(owner_mt + k + lane) : 0ull;
-        for (; k < e1; k += NW * UNR) {
-            const uint64_t wcur = wnext;
-            const int64_t kn = k + NW * UNR;
-            wnext = ((lane < UNR) && (kn + lane < e1)) ? __ldg(owner_mt + kn + lane) : 0ull;
+        // The next chunk's owner word is fetched while this chunk is processed.
+        int64_t c = start + warp * CH;
+        uint64_t wnext = ((lane < CH) && (c + lane < e1)) ? __ldg(owner_mt + c + lane) : 0ull;
+        for (; c < e1; c += NW * CH) {
+            const bool in = (lane < CH) && (c + lane < e1);
+            const uint64_t w = wnext;
+            const int64_t cn = c + NW * CH;
+            wnext = ((lane < CH) && (cn + lane < e1)) ? __ldg(owner_mt + cn + lane) : 0ull;
             // The owner list is sorted by cell: the first entry of another cell ends this run for
-            // the whole CTA, and every later entry of this warp is past it as well.
-            bool ok[UNR];
-            bool foreign = false;
-            uint32_t s[UNR];
+            // the whole CTA, and every later entry is past it as well.
+            const bool same = in && ((uint32_t) (w & kCellMask) == cell);
+            // A plan word always names a line < nsamp/32; anything else means the plan does not
+            // belong to this xpointing, so flag it and skip the line.
+            const uint32_t line = (uint32_t) ((w >> 20) & kClMask);
+            const bool line_ok = line < nlines;
+            err |= (same && !line_ok) ? kErrInconsistentNmt : 0u;
+            const unsigned okmask = __ballot_sync(kFullMask, same && line_ok);
+            const unsigned fmask = __ballot_sync(kFullMask, in && !same);
+            if ((fmask != 0) && (lane == 0))
+                atomicMin(&s_run[parity], (int) (c - start) + __ffs(fmask) - 1);
+
+            for (int g = 0; (g < CH) && ((okmask >> g) != 0u); g += UNR) {
+                bool ok[UNR];
+                uint32_t s[UNR];
 #pragma unroll
-            for (int u = 0; u < UNR; u++) {
-                const int64_t idx = k + u;
-                const bool in = idx < e1;
-                const uint64_t w = __shfl_sync(kFullMask, wcur, u);
-                const bool same = in && ((uint32_t) (w & kCellMask) == cell);
-                if (in && !same && !foreign && (lane == 0))
-                    atomicMin(&s_run[parity], (int) (idx - start));
-                foreign = foreign || (in && !same);
-                // A plan word always names a line < nsamp/32; anything else means the plan does
-                // not belong to this xpointing, so flag it and read line 0 instead.
-                uint32_t line = (uint32_t) ((w >> 20) & kClMask);
-                const bool line_ok = line < (nsamp >> 5);
-                err |= (same && !line_ok) ? kErrInconsistentNmt : 0u;
-                ok[u] = same && !foreign && line_ok;
-                line = line_ok ? line : 0u;
-                s[u] = 32u * line + (uint32_t) lane;
-            }
-            float y[UNR], x[UNR], al[UNR], tv[UNR];
+                for (int u = 0; u < UNR; u++) {
+                    ok[u] = (okmask >> (g + u)) & 1u;
+                    s[u] = (__shfl_sync(kFullMask, line, g + u) << 5) + (uint32_t) lane;
+                }
+                float y[UNR], x[UNR], al[UNR], tv[UNR];
 #pragma unroll
-            for (int u = 0; u < UNR; u++) {
-                y[u] = __ldcs(a.xp + s[u]);
-                x[u] = __ldcs(a.xp + nsamp + s[u]);
-                al[u] = __ldcs(a.xp + 2 * (size_t) nsamp + s[u]);
-                if constexpr (TOD2MAP)
-                    tv[u] = __ldcs(a.in + s[u]);
-                else
-                    tv[u] = (a.accum && ok[u]) ? a.out[s[u]] : 0.0f;
-            }
+                for (int u = 0; u < UNR; u++) {
+                    y[u] = ok[u] ? __ldcs(yrow + s[u]) : 0.0f;
+                    x[u] = ok[u] ? __ldcs(xrow + s[u]) : 0.0f;
+                    al[u] = ok[u] ? __ldcs(arow + s[u]) : 0.0f;
+                    if constexpr (TOD2MAP)
+                        tv[u] = ok[u] ? __ldcs(a.in + s[u]) : 0.0f;
+                    else
+                        tv[u] = (a.accum && ok[u]) ? a.out[s[u]] : 0.0f;
+                }
 #pragma unroll
-            for (int u = 0; u < UNR; u++) {
-                if (!ok[u])
-                    continue;
-                if constexpr (TOD2MAP) {
-                    t2m_sample<RESP>(a, tile, T, y[u], x[u], al[u], tv[u], s[u], rot, o0, o1, o2, err);
-                } else {
-                    const float r = m2t_sample<RESP>(a, tile, T, y[u], x[u], al[u], s[u], err);
-                    __stcs(a.out + s[u], a.accum ? (tv[u] + r) : r);
+                for (int u = 0; u < UNR; u++) {
+                    if (!ok[u])
+                        continue;
+                    if constexpr (TOD2MAP) {
+                        t2m_sample<RESP, PERIODIC>(a, tile, T, y[u], x[u], al[u], tv[u], s[u], rot, o0, o1, o2, err);
+                    } else {
+                        const float r = m2t_sample<RESP, PERIODIC>(a, tile, T, y[u], x[u], al[u], s[u], err);
+                        __stcs(a.out + s[u], a.accum ? (tv[u] + r) : r);
+                    }
                 }
             }
-            if (foreign)
+            if (fmask != 0u)
+                break;
+        }
+        __syncthreads();
+        const int64_t next = start + s_run[parity];
+        if constexpr (TOD2MAP)
+            flush_tile(tile, T, a, a.out);
+        parity ^= 1;
+        __syncthreads();
+        start = next;
+    }
+    block_publish_err(err, s_err, a.errword);
+}
+
+// Planned operator kernel, 16-byte form (xpointing and TOD 16-byte aligned).  A warp takes four
+// owner entries at a time: lane group g = lane/8 handles entry g's cache line, each lane four
+// consecutive samples of it, so xpointing and TOD move with one float4 load (or store) per lane
+// and row, and the owner word needs no shuffle.
+template<bool TOD2MAP, bool RESP, bool PERIODIC>
+__global__ void __launch_bounds__(NT, 2)
+planned_kernel_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner,
+                  const uint32_t *__restrict__ cellmap)
+{
+    extern __shared__ float tile[];
+    __shared__ int s_run[2];
+    __shared__ uint32_t s_err[NW];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane >> 3, sub = lane & 7;
+    const int64_t e0 = (nowner * (int64_t) blockIdx.x) / gridDim.x;
+    const int64_t e1 = (nowner * (int64_t) (blockIdx.x + 1)) / gridDim.x;
+    const uint32_t nsamp = (uint32_t) a.nsamp;
+    const uint32_t nlines = nsamp >> 5;
+    const float *__restrict__ yrow = a.xp;
+    const float *__restrict__ xrow = a.xp + nsamp;
+    const float *__restrict__ arow = a.xp + 2 * (size_t) nsamp;
+    uint32_t err = a.partial ? 0u : check_plan_cells(cellmap, a);
+
+    const int rot = lane % 3;
+    const int o0 = rot * PS, o1 = ((rot + 1) % 3) * PS, o2 = ((rot + 2) % 3) * PS;
+
+    if constexpr (TOD2MAP) {
+        for (int i = threadIdx.x; i < 3 * PS; i += NT)
+            tile[i] = 0.0f;
+    }
+
+    int64_t start = e0;
+    int parity = 0;
+    while (start < e1) {
+        const uint32_t cell = (uint32_t) (__ldg(owner_mt + start) & kCellMask);
+        Tile T;
+        T.gy0 = (int) (cell >> 10) << 6;
+        T.gx0 = ((int) (cell & 1023u) << 6) - HX;
+        if (threadIdx.x == 0)
+            s_run[parity] = (int) (e1 - start);
+        if constexpr (!TOD2MAP)
+            load_tile(tile, T, a, a.in);
+        __syncthreads();
+
+        int64_t c = start + 4 * warp;
+        uint64_t wnext = (c + grp < e1) ? __ldg(owner_mt + c + grp) : 0ull;
+        for (; c < e1; c += 4 * NW) {
+            const bool in = c + grp < e1;
+            const uint64_t w = wnext;
+            const int64_t cn = c + 4 * NW;
+            wnext = (cn + grp < e1) ? __ldg(owner_mt + cn + grp) : 0ull;
+            // The owner list is sorted by cell: the first entry of another cell ends this run.
+            const bool same = in && ((uint32_t) (w & kCellMask) == cell);
+            const uint32_t line = (uint32_t) ((w >> 20) & kClMask);
+            const bool line_ok = line < nlines;
+            err |= (same && !line_ok) ? kErrInconsistentNmt : 0u;
+            const bool ok = same && line_ok;
+            const unsigned fmask = __ballot_sync(kFullMask, in && !same) & 0x01010101u;
+            if ((fmask != 0u) && (lane == 0))
+                atomicMin(&s_run[parity], (int) (c - start) + ((__ffs(fmask) - 1) >> 3));
+
+            if (ok) {
+                const uint32_t s0 = (line << 5) + 4u * (uint32_t) sub;
+                const float4 y4 = __ldcs(reinterpret_cast<const float4 *>(yrow + s0));
+                const float4 x4 = __ldcs(reinterpret_cast<const float4 *>(xrow + s0));
+                const float4 a4 = __ldcs(reinterpret_cast<const float4 *>(arow + s0));
+                float4 t4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if constexpr (TOD2MAP)
+                    t4 = __ldcs(reinterpret_cast<const float4 *>(a.in + s0));
+                else if (a.accum)
+                    t4 = *reinterpret_cast<const float4 *>(a.out + s0);
+                const float yv[4] = {y4.x, y4.y, y4.z, y4.w};
+                const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
+                const float av[4] = {a4.x, a4.y, a4.z, a4.w};
+                const float tv[4] = {t4.x, t4.y, t4.z, t4.w};
+                if constexpr (TOD2MAP) {
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        t2m_sample<RESP, PERIODIC>(a, tile, T, yv[k], xv[k], av[k], tv[k], s0 + k, rot, o0, o1, o2,
+                                                   err);
+                } else {
+                    float r[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        r[k] = tv[k] + m2t_sample<RESP, PERIODIC>(a, tile, T, yv[k], xv[k], av[k], s0 + k, err);
+                    __stcs(reinterpret_cast<float4 *>(a.out + s0), make_float4(r[0], r[1], r[2], r[3]));
+                }
+            }
+            if (fmask != 0u)
                 break;
         }
         __syncthreads();
@@ -426,7 +540,7 @@ unplanned_kernel(OpArgs a)
             Located L;
             err |= locate(y[k], x[k], a.ny, a.nx, a.periodic, L);
             float sn, cs;
-            sincosf(2.0f * al[k], &sn, &cs);
+            sincos2a(al[k], &sn, &cs);
             const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
             if constexpr (TOD2MAP) {
                 const float t = tv[k], q = t * cs, u = t * sn;
@@ -452,25 +566,47 @@ unplanned_kernel(OpArgs a)
     block_publish_err(err, s_err, a.errword);
 }
 
-template<bool TOD2MAP, bool RESP>
+// Which directions use the 16-byte kernel when the arrays allow it.  tod2map keeps one sample per
+// lane: with four lines in one atomic instruction its shared-memory bank conflicts cost more than
+// the wider loads save.
+constexpr bool kVecMap2tod = true;
+constexpr bool kVecTod2map = false;   // its atomics conflict more in shared-memory banks
+
+template<bool TOD2MAP, bool RESP, bool PERIODIC>
 cudaError_t launch_planned_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                 cudaStream_t stream)
 {
     if (nowner <= 0)
         return cudaSuccess;
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(planned_kernel<TOD2MAP, RESP>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kTileBytes);
-        if (e != cudaSuccess)
-            return e;
-        attr_done = true;
-    }
     // Two CTAs per SM; never fewer than ~64 cache lines per CTA, so small plans reload few tiles.
     int64_t g = 2 * (int64_t) device_sm_count();
     g = std::max<int64_t>(1, std::min<int64_t>(g, (nowner + 63) / 64));
-    planned_kernel<TOD2MAP, RESP><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner, cellmap);
+    if constexpr (TOD2MAP ? kVecTod2map : kVecMap2tod) {
+        const float *tod = TOD2MAP ? a.in : a.out;
+        if (((((uintptr_t) a.xp) | ((uintptr_t) tod)) & 15) == 0) {
+            static std::atomic<uint64_t> attr_v4_done{0};
+            cudaError_t e = set_smem_limit(planned_kernel_v4<TOD2MAP, RESP, PERIODIC>, kTileBytes, attr_v4_done);
+            if (e != cudaSuccess)
+                return e;
+            planned_kernel_v4<TOD2MAP, RESP, PERIODIC><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner,
+                                                                                                 cellmap);
+            return cudaGetLastError();
+        }
+    }
+    static std::atomic<uint64_t> attr_done{0};
+    cudaError_t e = set_smem_limit(planned_kernel<TOD2MAP, RESP, PERIODIC>, kTileBytes, attr_done);
+    if (e != cudaSuccess)
+        return e;
+    planned_kernel<TOD2MAP, RESP, PERIODIC><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner, cellmap);
     return cudaGetLastError();
+}
+
+template<bool TOD2MAP, bool RESP>
+cudaError_t launch_planned_dispatch(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                    cudaStream_t stream)
+{
+    return a.periodic ? launch_planned_impl<TOD2MAP, RESP, true>(a, owner_mt, nowner, cellmap, stream)
+                      : launch_planned_impl<TOD2MAP, RESP, false>(a, owner_mt, nowner, cellmap, stream);
 }
 
 template<bool TOD2MAP>
@@ -493,15 +629,15 @@ cudaError_t launch_unplanned_impl(const OpArgs &a, cudaStream_t stream)
 cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                    cudaStream_t stream)
 {
-    return a.response ? launch_planned_impl<false, true>(a, owner_mt, nowner, cellmap, stream)
-                      : launch_planned_impl<false, false>(a, owner_mt, nowner, cellmap, stream);
+    return a.response ? launch_planned_dispatch<false, true>(a, owner_mt, nowner, cellmap, stream)
+                      : launch_planned_dispatch<false, false>(a, owner_mt, nowner, cellmap, stream);
 }
 
 cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                    cudaStream_t stream)
 {
-    return a.response ? launch_planned_impl<true, true>(a, owner_mt, nowner, cellmap, stream)
-                      : launch_planned_impl<true, false>(a, owner_mt, nowner, cellmap, stream);
+    return a.response ? launch_planned_dispatch<true, true>(a, owner_mt, nowner, cellmap, stream)
+                      : launch_planned_dispatch<true, false>(a, owner_mt, nowner, cellmap, stream);
 }
 
 cudaError_t launch_unplanned_map2tod(const OpArgs &a, cudaStream_t stream)

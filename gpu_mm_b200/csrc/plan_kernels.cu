@@ -539,16 +539,13 @@ cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, 
     const int xbits = bits_for(nxcells_max), ybits = bits_for(nycells_max);
     const int G = sort_grid_for(n);
     const int64_t chunk = (((n + G - 1) / G) + 255) / 256 * 256;
-    const int nd = 1 << digit_bits;
     constexpr int K = 8;
-    const size_t up_smem = nd * sizeof(uint32_t);
-    const size_t down_smem = (size_t) (kSortWarps + 1) * nd * sizeof(uint32_t);
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaFuncSetAttribute(sort_downsweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        cudaFuncSetAttribute(sort_upsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-        attr_done = true;
-    }
+    static std::atomic<uint64_t> down_done{0}, up_done{0};
+    cudaError_t e = set_smem_limit(sort_downsweep_kernel<K>, 200 * 1024, down_done);
+    if (e == cudaSuccess)
+        e = set_smem_limit(sort_upsweep_kernel, 64 * 1024, up_done);
+    if (e != cudaSuccess)
+        return e;
     uint64_t *src = a, *dst = b;
     for (int p = 0; p < npasses; p++) {
         DigitSpec ds;
@@ -563,7 +560,6 @@ cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, 
         sort_downsweep_kernel<K><<<G, kSortWarps * 32, (kSortWarps + 1) * ndp * sizeof(uint32_t), stream>>>(
             src, dst, n, chunk, ds, hist);
         uint64_t *t = src; src = dst; dst = t;
-        (void) up_smem; (void) down_smem;
     }
     return cudaGetLastError();
 }
