@@ -33,7 +33,7 @@ struct Located {
 __device__ __forceinline__ uint32_t locate(float ypix, float xpix, int ny, int nx, bool periodic, Located &L)
 {
     uint32_t err = 0;
-    int y0 = int(ypix);
+    int y0 = __float2int_rz(ypix);   // truncation; NaN gives 0
     y0 = max(y0, 0);
     y0 = min(y0, ny - 2);
     L.iy0 = y0;
@@ -47,7 +47,7 @@ __device__ __forceinline__ uint32_t locate(float ypix, float xpix, int ny, int n
         err |= xvalid ? 0u : kErrBadXpix;
         xpix = (xpix >= 0.0f) ? xpix : (xpix + float(nx));
         xpix = (xpix <= float(nx)) ? xpix : (xpix - float(nx));
-        int x0 = int(xpix);
+        int x0 = __float2int_rz(xpix);
         x0 = max(x0, 0);
         L.dx = xpix - float(x0);
         x0 = (x0 < nx) ? x0 : 0;
@@ -57,7 +57,7 @@ __device__ __forceinline__ uint32_t locate(float ypix, float xpix, int ny, int n
     } else {
         bool xvalid = (xpix >= 0.0f) && (xpix <= float(nx - 2));
         err |= xvalid ? 0u : kErrBadXpix;
-        int x0 = int(xpix);
+        int x0 = __float2int_rz(xpix);
         x0 = max(x0, 0);
         x0 = min(x0, nx - 2);
         L.ix0 = x0;
@@ -108,23 +108,27 @@ __device__ __forceinline__ void line_slot_masks(const int slots[6], unsigned ama
     }
 }
 
-// sin(2a) and cos(2a) for the detector response.  2a is reduced to [-pi, pi] by a two-term
-// Cody-Waite split of 2*pi (W. J. Cody and W. Waite, "Software Manual for the Elementary
-// Functions", 1980): head 6.28125 (exact in 8 bits, so j*head is exact for |j| < 2^16) plus the
-// float tail 2*pi - 6.28125; then the hardware approximations __sinf/__cosf.  Absolute error
-// about 5e-7 against CUDA's sincosf for |2a| <= 1024 (the hardware approximations' own error
-// dominates; the tail term adds at most 163 * 2^-34 there); larger arguments use sincosf.
+// sin(th) and cos(th) for |th| <= 1024: th is reduced to [-pi, pi] by a two-term Cody-Waite split of
+// 2*pi (W. J. Cody and W. Waite, "Software Manual for the Elementary Functions", 1980): head
+// 6.28125 (exact in 8 bits, so j*head is exact for |j| < 2^16) plus the float tail 2*pi - 6.28125;
+// then the hardware approximations __sinf/__cosf.  Absolute error about 6e-7 against CUDA's sincosf
+// (the hardware approximations' own error dominates; the tail term adds at most 163 * 2^-34).
+__device__ __forceinline__ void sincos_reduced(float th, float *s, float *c)
+{
+    const float j = rintf(th * 0.15915494309189535f);
+    float r = fmaf(j, -6.28125f, th);
+    r = fmaf(j, -1.9353071795864769e-3f, r);
+    __sincosf(r, s, c);
+}
+
+// sin(2a) and cos(2a) for the detector response: sincos_reduced for |2a| <= 1024, sincosf beyond.
 __device__ __forceinline__ void sincos2a(float alpha, float *s, float *c)
 {
     const float th = 2.0f * alpha;
-    if (fabsf(th) <= 1024.0f) {
-        const float j = rintf(th * 0.15915494309189535f);
-        float r = fmaf(j, -6.28125f, th);
-        r = fmaf(j, -1.9353071795864769e-3f, r);
-        __sincosf(r, s, c);
-    } else {
+    if (fabsf(th) <= 1024.0f)
+        sincos_reduced(th, s, c);
+    else
         sincosf(th, s, c);
-    }
 }
 
 // OR-reduce an error word over the block and publish it with one atomicOr per block (only if

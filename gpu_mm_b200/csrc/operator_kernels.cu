@@ -48,20 +48,30 @@ struct Tile {
     int gx0;   // unwrapped global column of tile column 0
 };
 
-__device__ __forceinline__ int64_t tile_pixel_offset(int r, int c, const Tile &T, const OpArgs &a)
+// Per-tile offset table, computed once per tile: tab[b * TX + c] is the local-map offset of tile
+// column c in row 0 of row block b (tile rows [64b, 64b + 64), all in one cell row), or -1 if that
+// column is outside the map or its cell is absent.  Tile pixel (r, c) is then at
+// tab[(r / 64) * TX + c] + (r % 64) * ystride, so the tile loops issue their map loads with no
+// cell_offsets lookup in between.
+constexpr int kTabEntries = 2 * TX;
+
+__device__ void tile_offsets(int64_t *tab, const Tile &T, const OpArgs &a)
 {
-    const int gy = T.gy0 + r;
-    int gx = T.gx0 + c;
-    if (a.periodic) {
-        gx %= a.nx;
-        gx += (gx < 0) ? a.nx : 0;
+    for (int i = threadIdx.x; i < kTabEntries; i += blockDim.x) {
+        const int b = i / TX, c = i % TX;
+        const int cy = (T.gy0 >> 6) + b;
+        int gx = T.gx0 + c;
+        if (a.periodic) {
+            gx %= a.nx;
+            gx += (gx < 0) ? a.nx : 0;
+        }
+        int64_t off = -1;
+        if ((gx >= 0) && (cy < a.nycells) && (gx < 64 * a.nxcells)) {
+            const int64_t co = __ldg(a.cell_offsets + (int64_t) cy * a.nxcells + (gx >> 6));
+            off = (co >= 0) ? (co + (gx & 63)) : -1;
+        }
+        tab[i] = off;
     }
-    if ((gx < 0) || (gy >= 64 * a.nycells) || (gx >= 64 * a.nxcells))
-        return -1;
-    const int64_t off = __ldg(a.cell_offsets + (int64_t) (gy >> 6) * a.nxcells + (gx >> 6));
-    if (off < 0)
-        return -1;
-    return off + (int64_t) (gy & 63) * a.ystride + (gx & 63);
 }
 
 // Global-memory pixel offset (map_evaluator / map_accumulator addressing,
@@ -92,30 +102,55 @@ __device__ __forceinline__ void sample_response(const OpArgs &a, uint32_t s, flo
     pr = __ldg(a.response + det + a.ndet);
 }
 
-// Loads the tile of 'cell' from the local map (absent pixels read as zero).
-__device__ void load_tile(float *tile, const Tile &T, const OpArgs &a, const float *__restrict__ lmap)
+// Loads the tile from the local map (absent pixels read as zero).  'tab' must hold the tile's
+// offset table (tile_offsets) and be visible to all threads.  Pixels move in groups of four
+// columns: a group whose four map pixels are consecutive and 16-byte aligned (the usual case: cell
+// offsets, ystride and polstride multiples of 4) is read with one float4 load per plane, so a
+// thread has all of its loads in flight at once; other groups are read pixel by pixel.
+__device__ void load_tile(float *tile, const int64_t *tab, const OpArgs &a, const float *__restrict__ lmap)
 {
-    for (int idx = threadIdx.x; idx < TY * TX; idx += NT) {
-        const int r = idx / TX, c = idx % TX;
-        const int64_t off = tile_pixel_offset(r, c, T, a);
-        const bool p = off >= 0;
+    constexpr int NG = TY * (TX / 4);   // column groups
+    const bool vec_ok = ((((uintptr_t) lmap) & 15) == 0) && ((a.ystride & 3) == 0) && ((a.polstride & 3) == 0);
+#pragma unroll 4
+    for (int gi = threadIdx.x; gi < NG; gi += NT) {
+        const int r = gi / (TX / 4), c = 4 * (gi % (TX / 4));
+        const int64_t *tb = tab + (r >> 6) * TX + c;
+        const int64_t b0 = tb[0];
+        const int64_t roff = (int64_t) (r & 63) * a.ystride;
         float *dst = tile + r * TS + c;
-        dst[0] = p ? __ldg(lmap + off) : 0.0f;
-        dst[PS] = p ? __ldg(lmap + off + a.polstride) : 0.0f;
-        dst[2 * PS] = p ? __ldg(lmap + off + 2 * a.polstride) : 0.0f;
+        if (vec_ok && (b0 >= 0) && ((b0 & 3) == 0) && (tb[1] == b0 + 1) && (tb[2] == b0 + 2) && (tb[3] == b0 + 3)) {
+            const float4 *src = reinterpret_cast<const float4 *>(lmap + b0 + roff);
+            const float4 t = __ldg(src);
+            const float4 q = __ldg(src + a.polstride / 4);
+            const float4 u = __ldg(src + a.polstride / 2);
+            dst[0] = t.x; dst[1] = t.y; dst[2] = t.z; dst[3] = t.w;
+            dst[PS] = q.x; dst[PS + 1] = q.y; dst[PS + 2] = q.z; dst[PS + 3] = q.w;
+            dst[2 * PS] = u.x; dst[2 * PS + 1] = u.y; dst[2 * PS + 2] = u.z; dst[2 * PS + 3] = u.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int64_t bk = tb[k];
+                const bool p = bk >= 0;
+                const int64_t off = bk + roff;
+                dst[k] = p ? __ldg(lmap + off) : 0.0f;
+                dst[PS + k] = p ? __ldg(lmap + off + a.polstride) : 0.0f;
+                dst[2 * PS + k] = p ? __ldg(lmap + off + 2 * a.polstride) : 0.0f;
+            }
+        }
     }
 }
 
 // Adds the tile into the map (one atomic per non-zero pixel and polarisation) and clears it.
-__device__ void flush_tile(float *tile, const Tile &T, const OpArgs &a, float *__restrict__ lmap)
+__device__ void flush_tile(float *tile, const int64_t *tab, const OpArgs &a, float *__restrict__ lmap)
 {
     for (int idx = threadIdx.x; idx < TY * TX; idx += NT) {
         const int r = idx / TX, c = idx % TX;
         float *src = tile + r * TS + c;
         const float t = src[0], q = src[PS], u = src[2 * PS];
         if ((t != 0.0f) || (q != 0.0f) || (u != 0.0f)) {
-            const int64_t off = tile_pixel_offset(r, c, T, a);
-            if (off >= 0) {
+            const int64_t base = tab[(r >> 6) * TX + c];
+            if (base >= 0) {
+                const int64_t off = base + (int64_t) (r & 63) * a.ystride;
                 atomicAdd(lmap + off, t);
                 atomicAdd(lmap + off + a.polstride, q);
                 atomicAdd(lmap + off + 2 * a.polstride, u);
@@ -165,16 +200,41 @@ __device__ __forceinline__ void global_accum(const OpArgs &a, float *__restrict_
     err |= (valid || a.partial) ? 0u : kErrNotInPixelization;
 }
 
-// One sample of map2tod against the staged tile (or global memory if it does not fit).
-template<bool RESP, bool PERIODIC>
-__device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, const Tile &T, float y, float x,
-                                            float al, uint32_t s, uint32_t &err)
+// Bilinear map2tod value of a sample at tile offset p: sum over the four neighbours of weight x
+// (ct*T + cq*Q + cu*U) (map_evaluator, gpu_mm_internals.hpp:243-293, on the staged tile).
+template<bool RESP>
+__device__ __forceinline__ float tile_eval(const float *tile, int p, float ct, float cq, float cu, float dy, float dx)
 {
-    Located L;
-    err |= locate(y, x, a.ny, a.nx, PERIODIC, L);
-    float sn, cs;
-    sincos2a(al, &sn, &cs);
-    float ct = 1.0f, cq = cs, cu = sn;
+    const float *q = tile + p;
+    float e00, e01, e10, e11;
+    if constexpr (RESP) {
+        e00 = ct * q[0] + cq * q[PS] + cu * q[2 * PS];
+        e01 = ct * q[1] + cq * q[PS + 1] + cu * q[2 * PS + 1];
+        e10 = ct * q[TS] + cq * q[PS + TS] + cu * q[2 * PS + TS];
+        e11 = ct * q[TS + 1] + cq * q[PS + TS + 1] + cu * q[2 * PS + TS + 1];
+    } else {
+        e00 = q[0] + cq * q[PS] + cu * q[2 * PS];
+        e01 = q[1] + cq * q[PS + 1] + cu * q[2 * PS + 1];
+        e10 = q[TS] + cq * q[PS + TS] + cu * q[2 * PS + TS];
+        e11 = q[TS + 1] + cq * q[PS + TS + 1] + cu * q[2 * PS + TS + 1];
+    }
+    const float wy0 = 1.0f - dy, wx0 = 1.0f - dx;
+    float r = (wy0 * wx0) * e00;
+    r += (wy0 * dx) * e01;
+    r += (dy * wx0) * e10;
+    r += (dy * dx) * e11;
+    return r;
+}
+
+// Response factors of a sample as (ct, cq, cu) = (t_resp, p_resp cos 2a, p_resp sin 2a), or
+// (1, cos 2a, sin 2a) without a response.
+template<bool RESP>
+__device__ __forceinline__ void sample_factors(const OpArgs &a, uint32_t s, float sn, float cs, float &ct, float &cq,
+                                               float &cu)
+{
+    ct = 1.0f;
+    cq = cs;
+    cu = sn;
     if constexpr (RESP) {
         float tr, pr;
         sample_response(a, s, tr, pr);
@@ -182,29 +242,28 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
         cq = pr * cs;
         cu = pr * sn;
     }
+}
+
+// One sample of map2tod, general path: exact locate with error bits, then the staged tile or, if the
+// footprint is not inside it, global memory.
+template<bool RESP, bool PERIODIC>
+__device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, const Tile &T, float y, float x,
+                                            float al, uint32_t s, uint32_t &err)
+{
+    Located L;
+    err |= locate(y, x, a.ny, a.nx, PERIODIC, L);
+    float sn, cs, ct, cq, cu;
+    sincos2a(al, &sn, &cs);
+    sample_factors<RESP>(a, s, sn, cs, ct, cq, cu);
     int ry, rx;
-    float e00, e01, e10, e11;
-    if (tile_position<PERIODIC>(L, T, a, ry, rx)) {
-        const float *p = tile + ry * TS + rx;
-        if constexpr (RESP) {
-            e00 = ct * p[0] + cq * p[PS] + cu * p[2 * PS];
-            e01 = ct * p[1] + cq * p[PS + 1] + cu * p[2 * PS + 1];
-            e10 = ct * p[TS] + cq * p[PS + TS] + cu * p[2 * PS + TS];
-            e11 = ct * p[TS + 1] + cq * p[PS + TS + 1] + cu * p[2 * PS + TS + 1];
-        } else {
-            e00 = p[0] + cq * p[PS] + cu * p[2 * PS];
-            e01 = p[1] + cq * p[PS + 1] + cu * p[2 * PS + 1];
-            e10 = p[TS] + cq * p[PS + TS] + cu * p[2 * PS + TS];
-            e11 = p[TS + 1] + cq * p[PS + TS + 1] + cu * p[2 * PS + TS + 1];
-        }
-    } else {
-        // Absent cells are already reported through the plan's cell bitmap.
-        uint32_t unused = 0;
-        e00 = global_eval(a, a.in, L.iy0, L.ix0, ct, cq, cu, unused);
-        e01 = global_eval(a, a.in, L.iy0, L.ix1, ct, cq, cu, unused);
-        e10 = global_eval(a, a.in, L.iy1, L.ix0, ct, cq, cu, unused);
-        e11 = global_eval(a, a.in, L.iy1, L.ix1, ct, cq, cu, unused);
-    }
+    if (tile_position<PERIODIC>(L, T, a, ry, rx))
+        return tile_eval<RESP>(tile, ry * TS + rx, ct, cq, cu, L.dy, L.dx);
+    // Absent cells are already reported through the plan's cell bitmap.
+    uint32_t unused = 0;
+    const float e00 = global_eval(a, a.in, L.iy0, L.ix0, ct, cq, cu, unused);
+    const float e01 = global_eval(a, a.in, L.iy0, L.ix1, ct, cq, cu, unused);
+    const float e10 = global_eval(a, a.in, L.iy1, L.ix0, ct, cq, cu, unused);
+    const float e11 = global_eval(a, a.in, L.iy1, L.ix1, ct, cq, cu, unused);
     const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
     float r = (wy0 * wx0) * e00;
     r += (wy0 * L.dx) * e01;
@@ -213,8 +272,10 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
     return r;
 }
 
-// One sample of tod2map.  o0..o2 are this lane's polarisation plane offsets in rotated order and
-// 'rot' selects the matching rotation of (t, q, u).
+// One sample of tod2map: exact locate with error bits, then 12 shared-memory atomics into the staged
+// tile or, if the footprint is not inside it, global atomics.  o0..o2 are this lane's polarisation
+// plane offsets in rotated order and 'rot' selects the matching rotation of (t, q, u): in one atomic
+// instruction, lanes on the same pixel then target different words.
 template<bool RESP, bool PERIODIC>
 __device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const Tile &T, float y, float x, float al,
                                            float tv, uint32_t s, int rot, int o0, int o1, int o2, uint32_t &err)
@@ -265,6 +326,51 @@ __device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const T
     }
 }
 
+// A sample on the fast path: tile offset, bilinear fractions and sin/cos 2a.
+struct TileSample {
+    int p;
+    float dy, dx, sn, cs;
+};
+
+// The common case of locate + tile_position + sincos2a, without branches: true if the sample is
+// valid (no error bit), needs no clamp and no x = nx wrap, lies inside the tile and has |2a| <= 1024.
+// S then holds what the general path computes from the same operations (bit for bit); otherwise
+// S.p = 0 and the caller must take the general path.
+template<bool PERIODIC>
+__device__ __forceinline__ bool tile_sample(float y, float x, float al, const Tile &T, const OpArgs &a, TileSample &S)
+{
+    // y in [0, ny-1): trunc(y) is in [0, ny-2], so locate's clamp does nothing.
+    bool fast = (y >= 0.0f) && (y < (float) (a.ny - 1));
+    const int iy0 = __float2int_rz(y);
+    S.dy = y - (float) iy0;
+    int ix0;
+    if constexpr (PERIODIC) {
+        // locate's fold; a folded x in [0, nx) comes only from a valid x and needs no wrap of ix0.
+        const float fnx = (float) a.nx;
+        float xf = (x >= 0.0f) ? x : (x + fnx);
+        xf = (xf <= fnx) ? xf : (xf - fnx);
+        fast = fast && (xf >= 0.0f) && (xf < fnx);
+        ix0 = __float2int_rz(xf);
+        S.dx = xf - (float) ix0;
+    } else {
+        fast = fast && (x >= 0.0f) && (x < (float) (a.nx - 2));
+        ix0 = __float2int_rz(x);
+        S.dx = x - (float) ix0;
+    }
+    const int ry = iy0 - T.gy0;
+    int rx = ix0 - T.gx0;
+    if constexpr (PERIODIC) {
+        rx += (rx < 0) ? a.nx : 0;
+        rx -= (rx > TX - 2) ? a.nx : 0;
+    }
+    fast = fast && ((unsigned) ry <= (unsigned) (TY - 2)) && ((unsigned) rx <= (unsigned) (TX - 2));
+    const float th = 2.0f * al;
+    fast = fast && (fabsf(th) <= 1024.0f);
+    sincos_reduced(th, &S.sn, &S.cs);
+    S.p = fast ? (ry * TS + rx) : 0;
+    return fast;
+}
+
 // Not-in-pixelization check of the plan's cells (this CTA's share of the bitmap).
 __device__ uint32_t check_plan_cells(const uint32_t *__restrict__ cellmap, const OpArgs &a)
 {
@@ -298,6 +404,7 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
     extern __shared__ float tile[];
     __shared__ int s_run[2];
     __shared__ uint32_t s_err[NW];
+    __shared__ int64_t s_tab[kTabEntries];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t e0 = (nowner * (int64_t) blockIdx.x) / gridDim.x;
@@ -326,9 +433,12 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
         T.gx0 = ((int) (cell & 1023u) << 6) - HX;
         if (threadIdx.x == 0)
             s_run[parity] = (int) (e1 - start);
-        if constexpr (!TOD2MAP)
-            load_tile(tile, T, a, a.in);
+        tile_offsets(s_tab, T, a);
         __syncthreads();
+        if constexpr (!TOD2MAP) {
+            load_tile(tile, s_tab, a, a.in);
+            __syncthreads();
+        }
 
         // The next chunk's owner word is fetched while this chunk is processed.
         int64_t c = start + warp * CH;
@@ -374,10 +484,23 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
                 for (int u = 0; u < UNR; u++) {
                     if (!ok[u])
                         continue;
+                    // tod2map runs the general path for every sample: its time goes to the shared
+                    // atomics, and the vote below would keep the compiler from overlapping one
+                    // sample's arithmetic with the previous sample's atomics (measured slower).
                     if constexpr (TOD2MAP) {
                         t2m_sample<RESP, PERIODIC>(a, tile, T, y[u], x[u], al[u], tv[u], s[u], rot, o0, o1, o2, err);
                     } else {
-                        const float r = m2t_sample<RESP, PERIODIC>(a, tile, T, y[u], x[u], al[u], s[u], err);
+                        // map2tod: fast path when every lane's sample passes tile_sample (the line
+                        // is warp-uniform), else the general path.
+                        TileSample S;
+                        float r;
+                        if (__all_sync(kFullMask, tile_sample<PERIODIC>(y[u], x[u], al[u], T, a, S))) {
+                            float ct, cq, cu;
+                            sample_factors<RESP>(a, s[u], S.sn, S.cs, ct, cq, cu);
+                            r = tile_eval<RESP>(tile, S.p, ct, cq, cu, S.dy, S.dx);
+                        } else {
+                            r = m2t_sample<RESP, PERIODIC>(a, tile, T, y[u], x[u], al[u], s[u], err);
+                        }
                         __stcs(a.out + s[u], a.accum ? (tv[u] + r) : r);
                     }
                 }
@@ -388,7 +511,7 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
         __syncthreads();
         const int64_t next = start + s_run[parity];
         if constexpr (TOD2MAP)
-            flush_tile(tile, T, a, a.out);
+            flush_tile(tile, s_tab, a, a.out);
         parity ^= 1;
         __syncthreads();
         start = next;
@@ -396,18 +519,19 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
     block_publish_err(err, s_err, a.errword);
 }
 
-// Planned operator kernel, 16-byte form (xpointing and TOD 16-byte aligned).  A warp takes four
-// owner entries at a time: lane group g = lane/8 handles entry g's cache line, each lane four
-// consecutive samples of it, so xpointing and TOD move with one float4 load (or store) per lane
-// and row, and the owner word needs no shuffle.
-template<bool TOD2MAP, bool RESP, bool PERIODIC>
+// map2tod, 16-byte form (xpointing and TOD 16-byte aligned).  A warp takes four owner entries at a
+// time: lane group g = lane/8 handles entry g's cache line, each lane four consecutive samples of it,
+// so xpointing and TOD move with one float4 load (or store) per lane and row, and the owner word
+// needs no shuffle.
+template<bool RESP, bool PERIODIC>
 __global__ void __launch_bounds__(NT, 2)
-planned_kernel_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner,
-                  const uint32_t *__restrict__ cellmap)
+planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner,
+                   const uint32_t *__restrict__ cellmap)
 {
     extern __shared__ float tile[];
     __shared__ int s_run[2];
     __shared__ uint32_t s_err[NW];
+    __shared__ int64_t s_tab[kTabEntries];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int grp = lane >> 3, sub = lane & 7;
@@ -420,14 +544,6 @@ planned_kernel_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowne
     const float *__restrict__ arow = a.xp + 2 * (size_t) nsamp;
     uint32_t err = a.partial ? 0u : check_plan_cells(cellmap, a);
 
-    const int rot = lane % 3;
-    const int o0 = rot * PS, o1 = ((rot + 1) % 3) * PS, o2 = ((rot + 2) % 3) * PS;
-
-    if constexpr (TOD2MAP) {
-        for (int i = threadIdx.x; i < 3 * PS; i += NT)
-            tile[i] = 0.0f;
-    }
-
     int64_t start = e0;
     int parity = 0;
     while (start < e1) {
@@ -437,8 +553,9 @@ planned_kernel_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowne
         T.gx0 = ((int) (cell & 1023u) << 6) - HX;
         if (threadIdx.x == 0)
             s_run[parity] = (int) (e1 - start);
-        if constexpr (!TOD2MAP)
-            load_tile(tile, T, a, a.in);
+        tile_offsets(s_tab, T, a);
+        __syncthreads();
+        load_tile(tile, s_tab, a, a.in);
         __syncthreads();
 
         int64_t c = start + 4 * warp;
@@ -458,40 +575,52 @@ planned_kernel_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowne
             if ((fmask != 0u) && (lane == 0))
                 atomicMin(&s_run[parity], (int) (c - start) + ((__ffs(fmask) - 1) >> 3));
 
+            const uint32_t s0 = (line << 5) + 4u * (uint32_t) sub;
+            float4 y4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), x4 = y4, a4 = y4, t4 = y4;
             if (ok) {
-                const uint32_t s0 = (line << 5) + 4u * (uint32_t) sub;
-                const float4 y4 = __ldcs(reinterpret_cast<const float4 *>(yrow + s0));
-                const float4 x4 = __ldcs(reinterpret_cast<const float4 *>(xrow + s0));
-                const float4 a4 = __ldcs(reinterpret_cast<const float4 *>(arow + s0));
-                float4 t4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                if constexpr (TOD2MAP)
-                    t4 = __ldcs(reinterpret_cast<const float4 *>(a.in + s0));
-                else if (a.accum)
+                y4 = __ldcs(reinterpret_cast<const float4 *>(yrow + s0));
+                x4 = __ldcs(reinterpret_cast<const float4 *>(xrow + s0));
+                a4 = __ldcs(reinterpret_cast<const float4 *>(arow + s0));
+                if (a.accum)
                     t4 = *reinterpret_cast<const float4 *>(a.out + s0);
-                const float yv[4] = {y4.x, y4.y, y4.z, y4.w};
-                const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
-                const float av[4] = {a4.x, a4.y, a4.z, a4.w};
-                const float tv[4] = {t4.x, t4.y, t4.z, t4.w};
-                if constexpr (TOD2MAP) {
-#pragma unroll
-                    for (int k = 0; k < 4; k++)
-                        t2m_sample<RESP, PERIODIC>(a, tile, T, yv[k], xv[k], av[k], tv[k], s0 + k, rot, o0, o1, o2,
-                                                   err);
-                } else {
+            }
+            const float tv[4] = {t4.x, t4.y, t4.z, t4.w};
+            // Fast path when all four samples of every lane pass tile_sample, else the general path.
+            TileSample S[4];
+            bool fast = tile_sample<PERIODIC>(y4.x, x4.x, a4.x, T, a, S[0]);
+            fast = tile_sample<PERIODIC>(y4.y, x4.y, a4.y, T, a, S[1]) && fast;
+            fast = tile_sample<PERIODIC>(y4.z, x4.z, a4.z, T, a, S[2]) && fast;
+            fast = tile_sample<PERIODIC>(y4.w, x4.w, a4.w, T, a, S[3]) && fast;
+            if (__all_sync(kFullMask, fast || !ok)) {
+                if (ok) {
                     float r[4];
 #pragma unroll
-                    for (int k = 0; k < 4; k++)
-                        r[k] = tv[k] + m2t_sample<RESP, PERIODIC>(a, tile, T, yv[k], xv[k], av[k], s0 + k, err);
+                    for (int k = 0; k < 4; k++) {
+                        float ct, cq, cu;
+                        sample_factors<RESP>(a, s0 + k, S[k].sn, S[k].cs, ct, cq, cu);
+                        r[k] = tv[k] + tile_eval<RESP>(tile, S[k].p, ct, cq, cu, S[k].dy, S[k].dx);
+                    }
                     __stcs(reinterpret_cast<float4 *>(a.out + s0), make_float4(r[0], r[1], r[2], r[3]));
                 }
+            } else if (ok) {
+                // General path: the pointing is read again rather than kept live across the fast path.
+                const float4 yy = __ldcs(reinterpret_cast<const float4 *>(yrow + s0));
+                const float4 xx = __ldcs(reinterpret_cast<const float4 *>(xrow + s0));
+                const float4 aa = __ldcs(reinterpret_cast<const float4 *>(arow + s0));
+                const float yv[4] = {yy.x, yy.y, yy.z, yy.w};
+                const float xv[4] = {xx.x, xx.y, xx.z, xx.w};
+                const float av[4] = {aa.x, aa.y, aa.z, aa.w};
+                float r[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    r[k] = tv[k] + m2t_sample<RESP, PERIODIC>(a, tile, T, yv[k], xv[k], av[k], s0 + k, err);
+                __stcs(reinterpret_cast<float4 *>(a.out + s0), make_float4(r[0], r[1], r[2], r[3]));
             }
             if (fmask != 0u)
                 break;
         }
         __syncthreads();
         const int64_t next = start + s_run[parity];
-        if constexpr (TOD2MAP)
-            flush_tile(tile, T, a, a.out);
         parity ^= 1;
         __syncthreads();
         start = next;
@@ -566,11 +695,9 @@ unplanned_kernel(OpArgs a)
     block_publish_err(err, s_err, a.errword);
 }
 
-// Which directions use the 16-byte kernel when the arrays allow it.  tod2map keeps one sample per
-// lane: with four lines in one atomic instruction its shared-memory bank conflicts cost more than
-// the wider loads save.
-constexpr bool kVecMap2tod = true;
-constexpr bool kVecTod2map = false;   // its atomics conflict more in shared-memory banks
+// map2tod uses the 16-byte kernel when xpointing and TOD are 16-byte aligned.  tod2map keeps one
+// sample per lane: with four lines in one atomic instruction its shared-memory bank conflicts cost
+// more than the wider loads save (measured).
 
 template<bool TOD2MAP, bool RESP, bool PERIODIC>
 cudaError_t launch_planned_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
@@ -581,15 +708,13 @@ cudaError_t launch_planned_impl(const OpArgs &a, const uint64_t *owner_mt, int64
     // Two CTAs per SM; never fewer than ~64 cache lines per CTA, so small plans reload few tiles.
     int64_t g = 2 * (int64_t) device_sm_count();
     g = std::max<int64_t>(1, std::min<int64_t>(g, (nowner + 63) / 64));
-    if constexpr (TOD2MAP ? kVecTod2map : kVecMap2tod) {
-        const float *tod = TOD2MAP ? a.in : a.out;
-        if (((((uintptr_t) a.xp) | ((uintptr_t) tod)) & 15) == 0) {
+    if constexpr (!TOD2MAP) {
+        if (((((uintptr_t) a.xp) | ((uintptr_t) a.out)) & 15) == 0) {
             static std::atomic<uint64_t> attr_v4_done{0};
-            cudaError_t e = set_smem_limit(planned_kernel_v4<TOD2MAP, RESP, PERIODIC>, kTileBytes, attr_v4_done);
+            cudaError_t e = set_smem_limit(planned_map2tod_v4<RESP, PERIODIC>, kTileBytes, attr_v4_done);
             if (e != cudaSuccess)
                 return e;
-            planned_kernel_v4<TOD2MAP, RESP, PERIODIC><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner,
-                                                                                                 cellmap);
+            planned_map2tod_v4<RESP, PERIODIC><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner, cellmap);
             return cudaGetLastError();
         }
     }

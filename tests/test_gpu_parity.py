@@ -294,6 +294,60 @@ def test_aligned_and_unaligned_arrays(g):
     np.testing.assert_array_equal(tods[0], tods[1])
 
 
+@pytest.mark.parametrize("periodic", [True, False])
+def test_fast_and_general_paths(g, periodic):
+    """The planned kernels take a branch-free path for a line (or group of lines) whose samples are all
+    ordinary, and the general per-sample path otherwise.  Plant the cases the general path exists
+    for: large angles (|2a| > 1024), periodic x that needs folding or lands on x = nx, y = ny-1 and
+    non-periodic x = nx-2.  Both alignments; results against the oracle."""
+    import torch
+    rng = np.random.default_rng(5150 + periodic)
+    ny, nx = 256, 512
+    ndet, nt = 16, 2048
+    xp = random_raster(rng, ndet, nt, ny, nx, periodic, speed=0.4)
+    xp64 = xp.astype(np.float64)
+    pick = lambda k: (rng.integers(0, ndet, k), rng.integers(0, nt, k))
+    d, t = pick(40)
+    xp64[2, d, t] = rng.choice([-600.0, 600.0, 5000.0], 40)
+    d, t = pick(20)
+    xp64[0, d, t] = ny - 1.0
+    if periodic:
+        d, t = pick(60)
+        xp64[1, d, t] -= nx
+        d, t = pick(60)
+        xp64[1, d, t] = np.minimum(xp64[1, d, t] + nx, 2.0 * nx)
+        d, t = pick(10)
+        xp64[1, d, t] = float(nx)
+    else:
+        d, t = pick(20)
+        xp64[1, d, t] = nx - 2.0
+    xp = xp64.astype(np.float32)
+    lp_o = oracle.Lpix.rectangle(ny, nx, periodic)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, periodic)
+    m = rng.standard_normal(3 * lp.npix).astype(np.float32)
+    tv = rng.standard_normal((ndet, nt)).astype(np.float32)
+    lmap = g.LocalMap(lp, cuda(m))
+    want_tod = np.zeros((ndet, nt), np.float32)
+    oracle.map2tod(want_tod, m, xp, lp_o, False, False)
+    want_map = np.zeros(3 * lp.npix, np.float32)
+    oracle.tod2map(want_map, tv, xp, lp_o)
+    for off in (0, 1):
+        flat = torch.zeros(xp.size + off, dtype=torch.float32, device="cuda")
+        xg = flat[off:].view(xp.shape)
+        xg.copy_(torch.from_numpy(xp))
+        pp, plan = build_plan(g, xg, ny, nx, periodic)
+        tflat = torch.zeros(tv.size + off, dtype=torch.float32, device="cuda")
+        tod = tflat[off:].view(tv.shape)
+        g.map2tod(tod, lmap, xg, plan)
+        rl1, mx = rel_stats(host(tod), want_tod)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, (off, rl1, mx)
+        tod.copy_(torch.from_numpy(tv))
+        out = g.LocalMap(lp, cuda(np.zeros(3 * lp.npix, np.float32)))
+        g.tod2map(out, tod, xg, plan)
+        rl1, mx = rel_stats(host(out.arr), want_map)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, (off, rl1, mx)
+
+
 def test_plan_reuse_and_buffers(g):
     """Caller-supplied buffers (gpu_mm.py:1253-1299): one shared tmp_buf for several plans; a plan is
     reusable across calls and gives identical results."""
