@@ -20,6 +20,9 @@ Other numbers on the JSON line:
   cpu_baseline the reference's CPU operators (oracle/_ref: the reference header; else the oracle
                port) on all host cores over a bounded prefix of the same workload
   clocks       NVML SM clock samples during the timed region
+  precision    tod2map precision variants (float atomics, compensated float flush, float64 map) on
+               the high-hit workload (2^28 samples in a 512x512 box, tod = 1e3 + N(0,1)): throughput
+               and max/rms relative error against the FP64 oracle on the host cores
 
 N > 1 (torchrun): every rank runs its own replica of the workload on its own GPU (weak scaling, no
 data-path collective); the step time is the max over ranks.  --impl reference runs the CPU
@@ -49,6 +52,7 @@ def parse_args():
     p.add_argument("--ndet-rows", type=int, default=32, help="detector rows (32 = full 2^28-sample workload)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-precision", action="store_true", help="skip the tod2map precision study")
     p.add_argument("--only", default="", help="profiling aid: 'map2tod' or 'tod2map' runs only that operator")
     return p.parse_args()
 
@@ -206,6 +210,74 @@ def run_reference_arm(args):
         "e2e": {"value": round(value, 4), "unit": "Gsamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def precision_study(max_run_lines=1024):
+    """tod2map precision variants on the high-hit workload: 64 detectors x 2^22 samples (2^28)
+    confined to the 512x512 box [256, 768)^2 of a 3x1024x1024 map (~1000 hits/pixel), tod = 1e3 +
+    N(0,1).  Each mode is timed with CUDA events (3 calls after 1 warm-up) and compared with the FP64
+    oracle (reference_tod2map<double> on the float32 inputs widened) on the host cores."""
+    import numpy as np
+    import torch
+    import oracle
+    import gpu_mm_b200 as g
+    from gpu_mm_b200 import synthetic
+    ny = nx = 1024
+    xp = synthetic.config3_xpointing(device="cuda")
+    nsamp = xp.numel() // 3
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    tod = 1e3 + torch.randn(xp.shape[1:], generator=gen, device="cuda")
+    pp = g.PointingPrePlan(xp, ny, nx, periodic_xcoord=False)
+    plan = g.PointingPlan(pp, xp)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, False)
+    n = 3 * lp.npix
+    f32 = torch.zeros(n, device="cuda")
+    comp = torch.zeros(n, device="cuda")
+    f64 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    lmap = g.LocalMap(lp, f32)
+    calls = {
+        "fp32_atomics": lambda: g.tod2map(lmap, tod, xp, plan),
+        "fp32_compensated_flush": lambda: (g.tod2map_compensated(lmap, comp, tod, xp, plan, max_run_lines=max_run_lines),
+                                           g.fold_compensation(lmap, comp)),
+        "fp64_map": lambda: g.tod2map_f64(f64, lp, tod, xp, plan, max_run_lines=max_run_lines),
+    }
+    results = {}
+    for name, fn in calls.items():
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        f32.zero_()
+        comp.zero_()
+        f64.zero_()
+        fn()
+        torch.cuda.synchronize()
+        out = (f64 if name == "fp64_map" else f32).cpu().numpy().astype(np.float64)
+        results[name] = {"ms": round(ms, 4), "gsamples_s": round(nsamp / (ms * 1e-3) / 1e9, 3), "out": out}
+    xp_h = xp.cpu().numpy()
+    tod_h = tod.cpu().numpy()
+    want = np.zeros(n, np.float64)
+    nthreads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    assert oracle.tod2map_f64w_mt(want, tod_h, xp_h, oracle.Lpix.rectangle(ny, nx, False), nthreads) == 0
+    oracle_s = time.perf_counter() - t0
+    for name, r in results.items():
+        d = r.pop("out") - want
+        r["max_rel_err"] = float(f"{np.abs(d).max() / np.abs(want).max():.3e}")
+        r["rms_rel_err"] = float(f"{np.sqrt((d * d).sum() / (want * want).sum()):.3e}")
+    return {
+        "workload": "64 detectors x 2^22 samples (2^28) in the 512x512 box of a 3x1024x1024 map, ~1000 hits/pixel, "
+                    "tod = 1e3 + N(0,1)",
+        "error_metric": "max_rel = max|a-b| / max|b|, rms_rel = sqrt(sum (a-b)^2 / sum b^2), all three planes, "
+                        "b = FP64 oracle (reference_tod2map<double> on the float32 inputs widened)",
+        "max_run_lines": max_run_lines, "oracle_seconds": round(oracle_s, 2), "oracle_threads": nthreads,
+        "modes": results,
+    }
 
 
 # ------------------------------------------------------------------------------------------------
@@ -401,6 +473,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.ndet_rows)
+    precision = None
+    if rank == 0 and world == 1 and not args.no_precision:
+        precision = precision_study()
 
     if rank == 0:
         value = world * nsamp / (ms_step * 1e-3) / 1e9
@@ -419,7 +494,7 @@ def main():
                            **unplanned, "plan_build": round(statistics.mean(plan_ms), 4),
                            "first_plan_build_s": round(first_plan_s, 3)},
             "plan": {"nmt": int(pp.plan_nmt), "overhead": round(pp.overhead, 4), "sort_digit_bits": pp.sort_digit_bits},
-            "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "precision": precision,
             "gpu_launches": args.steps * (int(do_m2t) + int(do_t2m)),
         }
         print(json.dumps(line), flush=True)

@@ -21,10 +21,12 @@ except ImportError as _e:   # pragma: no cover - exercised only on unbuilt trees
 
 from .gpu_mm import *            # noqa: F401,F403
 from .gpu_mm import (map2tod, tod2map, LocalPixelization, LocalMap, DynamicMap, PointingPrePlan,  # noqa: F401
-                     PointingPlan, read_xpointing_npzfile, mm_dtype)
+                     PointingPlan, read_xpointing_npzfile, mm_dtype, tod2map_compensated, fold_compensation,
+                     tod2map_f64)
 
 __all__ = ["map2tod", "tod2map", "LocalPixelization", "LocalMap", "DynamicMap", "PointingPrePlan",
-           "PointingPlan", "read_xpointing_npzfile", "mm_dtype", "gpu_mm_pybind11"]
+           "PointingPlan", "read_xpointing_npzfile", "mm_dtype", "gpu_mm_pybind11", "tod2map_compensated",
+           "fold_compensation", "tod2map_f64"]
 
 
 def library_path():

@@ -166,6 +166,14 @@ OpArgs make_args(const gmm_lpix *lp, const float *xp, int64_t nsamp, bool partia
     a.partial = partial;
     a.accum = accum;
     a.errword = errword;
+    a.flush = kFlushF32;
+    a.comp = nullptr;
+    a.out64 = nullptr;
+    a.max_run_lines = 0;
+    a.descs = nullptr;
+    a.ntod = 0;
+    a.ctas_per_sm = 0;
+    a.min_lines_per_cta = 0;
     return a;
 }
 
@@ -362,11 +370,29 @@ int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum, con
     return err_bits(err, where, 0);
 }
 
+// tod2map precision mode of planned_op (OpArgs::flush and friends).
+struct Precision {
+    int flush = kFlushF32;
+    float *comp = nullptr;
+    double *out64 = nullptr;
+    int64_t max_run_lines = 0;
+};
+
 static int planned_op(bool tod2map, float *out, const float *in, const float *xp, const float *response, int64_t ndet,
                       const gmm_lpix *lp, const gmm_preplan_info *info, const void *plan_buf, int32_t partial,
-                      int32_t accum, uint32_t *errword, cudaStream_t stream, const char *where)
+                      int32_t accum, uint32_t *errword, cudaStream_t stream, const char *where,
+                      const Precision &prec = Precision())
 {
-    if (int rc = check_ptr(out, where, tod2map ? "local_map" : "tod")) return rc;
+    if (prec.flush == kFlushF64) {
+        if (int rc = check_ptr(prec.out64, where, "local_map")) return rc;
+    } else if (int rc = check_ptr(out, where, tod2map ? "local_map" : "tod")) {
+        return rc;
+    }
+    if (prec.flush == kFlushCompensated) {
+        if (int rc = check_ptr(prec.comp, where, "comp")) return rc;
+    }
+    if (prec.max_run_lines < 0)
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": max_run_lines must be >= 0");
     if (int rc = check_ptr(in, where, tod2map ? "tod" : "local_map")) return rc;
     if (int rc = check_ptr(xp, where, "xpointing")) return rc;
     if (int rc = check_ptr(info, where, "plan")) return rc;
@@ -390,6 +416,10 @@ static int planned_op(bool tod2map, float *out, const float *in, const float *xp
     OpArgs a = make_args(lp, xp, info->nsamp, partial != 0, accum != 0, word);
     a.out = out;
     a.in = in;
+    a.flush = prec.flush;
+    a.comp = prec.comp;
+    a.out64 = prec.out64;
+    a.max_run_lines = prec.max_run_lines;
     if (response) {
         a.response = response;
         a.ndet = ndet;
@@ -436,6 +466,194 @@ int gmm_response_tod2map(float *lmap, const float *tod, const float *xp, const f
 {
     if (int rc = check_ptr(response, "response_tod2map", "response")) return rc;
     return planned_op(true, lmap, tod, xp, response, ndet, lp, info, plan_buf, partial, 0, errword, stream, "tod2map");
+}
+
+int gmm_planned_tod2map_compensated(float *lmap, float *comp, const float *tod, const float *xp, const gmm_lpix *lp,
+                                    const gmm_preplan_info *info, const void *plan_buf, int32_t partial,
+                                    int64_t max_run_lines, uint32_t *errword, cudaStream_t stream)
+{
+    Precision prec;
+    prec.flush = kFlushCompensated;
+    prec.comp = comp;
+    prec.max_run_lines = max_run_lines;
+    return planned_op(true, lmap, tod, xp, nullptr, 1, lp, info, plan_buf, partial, 0, errword, stream,
+                      "tod2map_compensated", prec);
+}
+
+int gmm_planned_tod2map_f64(double *lmap, const float *tod, const float *xp, const gmm_lpix *lp,
+                            const gmm_preplan_info *info, const void *plan_buf, int32_t partial, int64_t max_run_lines,
+                            uint32_t *errword, cudaStream_t stream)
+{
+    Precision prec;
+    prec.flush = kFlushF64;
+    prec.out64 = lmap;
+    prec.max_run_lines = max_run_lines;
+    return planned_op(true, nullptr, tod, xp, nullptr, 1, lp, info, plan_buf, partial, 0, errword, stream,
+                      "tod2map_f64", prec);
+}
+
+int gmm_fold_compensation(float *lmap, float *comp, int64_t n, cudaStream_t stream)
+{
+    if (int rc = check_ptr(lmap, "fold_compensation", "local_map")) return rc;
+    if (int rc = check_ptr(comp, "fold_compensation", "comp")) return rc;
+    if (n < 0)
+        return fail(GMM_ERR_INVALID_ARGUMENT, "fold_compensation: n must be >= 0");
+    cudaError_t e = launch_fold_compensation(lmap, comp, n, stream);
+    return (e == cudaSuccess) ? 0 : cuda_fail(e, "fold_compensation");
+}
+
+// ---- Batches of TODs ----
+
+static int check_tuning(const gmm_batch_tuning *t, const char *where)
+{
+    if (!t) return 0;
+    if ((t->sort_digit_bits < 4) || (t->sort_digit_bits > 11) || (t->ctas_per_sm < 1) || (t->ctas_per_sm > 8) ||
+        (t->min_lines_per_cta < 1)) {
+        std::ostringstream ss;
+        ss << where << ": bad tuning (sort_digit_bits=" << t->sort_digit_bits << " in [4,11], ctas_per_sm="
+           << t->ctas_per_sm << " in [1,8], min_lines_per_cta=" << t->min_lines_per_cta << " >= 1)";
+        return fail(GMM_ERR_INVALID_ARGUMENT, ss.str());
+    }
+    return 0;
+}
+
+static int check_batch(const gmm_tod_desc *descs, int32_t ntod, int64_t total_lines, const char *where)
+{
+    if (int rc = check_ptr(descs, where, "descs")) return rc;
+    if ((ntod < 1) || (ntod > 65535)) {
+        std::ostringstream ss;
+        ss << where << ": ntod=" << ntod << " must be in [1, 65535]";
+        return fail(GMM_ERR_INVALID_ARGUMENT, ss.str());
+    }
+    if ((total_lines < ntod) || (total_lines > (1ll << 40))) {
+        std::ostringstream ss;
+        ss << where << ": total_lines=" << total_lines << " must be >= ntod (every TOD has a cache line)";
+        return fail(GMM_ERR_INVALID_ARGUMENT, ss.str());
+    }
+    return 0;
+}
+
+int gmm_batch_tuning_default(gmm_batch_tuning *tuning)
+{
+    if (int rc = check_ptr(tuning, "batch_tuning_default", "tuning")) return rc;
+    tuning->sort_digit_bits = g_sort_max_digit_bits;
+    tuning->ctas_per_sm = 2;
+    tuning->min_lines_per_cta = 64;
+    tuning->reserved = 0;
+    return 0;
+}
+
+static void batch_layout(int64_t total_lines, int ny, int nx, const gmm_batch_tuning *t, int64_t *owner_off,
+                         int64_t *cellmap_off, int64_t *plan_nbytes, int64_t *hist_off, int64_t *tmp_nbytes,
+                         int *dbits, int *passes)
+{
+    const int nyc = (ny + 63) / 64, nxc = (nx + 63) / 64;
+    *passes = sort_passes(nyc, nxc, t ? t->sort_digit_bits : g_sort_max_digit_bits, dbits);
+    *owner_off = 0;
+    *cellmap_off = align128(8 * total_lines);
+    *plan_nbytes = *cellmap_off + kCellmapBytes;
+    *hist_off = align128(8 * total_lines);
+    *tmp_nbytes = *hist_off + std::max<int64_t>(sort_scratch_nbytes(*dbits, kSortGridMax), 128);
+}
+
+int gmm_batch_plan_nbytes(int64_t total_lines, int32_t ny, int32_t nx, const gmm_batch_tuning *tuning,
+                          int64_t *plan_nbytes, int64_t *tmp_nbytes)
+{
+    const char *where = "batch_plan_nbytes";
+    if (int rc = check_npix(ny, nx, where)) return rc;
+    if (int rc = check_tuning(tuning, where)) return rc;
+    if (int rc = check_ptr(plan_nbytes, where, "plan_nbytes")) return rc;
+    if (int rc = check_ptr(tmp_nbytes, where, "tmp_nbytes")) return rc;
+    if (total_lines < 1)
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": total_lines must be >= 1");
+    int64_t oo, co, ho;
+    int dbits, passes;
+    batch_layout(total_lines, ny, nx, tuning, &oo, &co, plan_nbytes, &ho, tmp_nbytes, &dbits, &passes);
+    return 0;
+}
+
+int gmm_batch_plan_build(const gmm_tod_desc *descs, int32_t ntod, int64_t total_lines, int32_t ny, int32_t nx,
+                         int32_t periodic, void *plan_buf, int64_t plan_nbytes, void *tmp, int64_t tmp_nbytes,
+                         const gmm_batch_tuning *tuning, uint32_t *errword, cudaStream_t stream)
+{
+    const char *where = "batch_plan_build";
+    if (int rc = check_batch(descs, ntod, total_lines, where)) return rc;
+    if (int rc = check_npix(ny, nx, where)) return rc;
+    if (int rc = check_tuning(tuning, where)) return rc;
+    if (int rc = check_ptr(plan_buf, where, "plan_buf")) return rc;
+    if (int rc = check_ptr(tmp, where, "tmp")) return rc;
+    if (int rc = check_ptr(errword, where, "errword")) return rc;
+    if ((((uintptr_t) plan_buf) | ((uintptr_t) tmp)) & 127)
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": 'plan_buf' and 'tmp' must be 128-byte aligned");
+    int64_t oo, co, need_plan, ho, need_tmp;
+    int dbits, passes;
+    batch_layout(total_lines, ny, nx, tuning, &oo, &co, &need_plan, &ho, &need_tmp, &dbits, &passes);
+    if ((plan_nbytes < need_plan) || (tmp_nbytes < need_tmp)) {
+        std::ostringstream ss;
+        ss << where << ": buffers too small (plan " << plan_nbytes << " < " << need_plan << " or tmp " << tmp_nbytes
+           << " < " << need_tmp << ")";
+        return fail(GMM_ERR_BUFFER_TOO_SMALL, ss.str());
+    }
+    char *b = (char *) plan_buf, *t = (char *) tmp;
+    uint64_t *owner = (uint64_t *) (b + oo), *alt = (uint64_t *) t;
+    uint32_t *cellmap = (uint32_t *) (b + co), *hist = (uint32_t *) (t + ho);
+    const bool even = (passes % 2) == 0;
+    const int nyc = (ny + 63) / 64, nxc = (nx + 63) / 64;
+    cudaError_t e = cudaMemsetAsync(errword, 0, sizeof(uint32_t), stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(cellmap, 0, kCellmapBytes, stream);
+    if (e == cudaSuccess)
+        e = launch_batch_owner(descs, ntod, total_lines, ny, nx, periodic != 0, even ? owner : alt, cellmap, errword,
+                               stream);
+    if (e == cudaSuccess)
+        e = radix_sort_mt(even ? owner : alt, even ? alt : owner, total_lines, nyc, nxc, dbits, passes, hist, stream);
+    return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
+}
+
+static int batch_op(bool tod2map, const gmm_tod_desc *descs, int32_t ntod, int64_t total_lines, float *lmap_out,
+                    const float *lmap_in, const gmm_lpix *lp, const void *plan_buf, int32_t partial, int32_t accum,
+                    const gmm_batch_tuning *tuning, uint32_t *errword, cudaStream_t stream, const char *where)
+{
+    if (int rc = check_batch(descs, ntod, total_lines, where)) return rc;
+    if (int rc = check_lpix(lp, where)) return rc;
+    if (int rc = check_tuning(tuning, where)) return rc;
+    if (int rc = check_ptr(plan_buf, where, "plan_buf")) return rc;
+    if (int rc = check_ptr(errword, where, "errword")) return rc;
+    if (int rc = check_ptr(tod2map ? (const void *) lmap_out : (const void *) lmap_in, where, "local_map")) return rc;
+    int64_t oo, co, pn, ho, tn;
+    int dbits, passes;
+    batch_layout(total_lines, lp->nypix_global, lp->nxpix_global, tuning, &oo, &co, &pn, &ho, &tn, &dbits, &passes);
+    const char *b = (const char *) plan_buf;
+    OpArgs a = make_args(lp, nullptr, 0, partial != 0, accum != 0, errword);
+    a.out = lmap_out;
+    a.in = lmap_in;
+    a.descs = descs;
+    a.ntod = ntod;
+    if (tuning) {
+        a.ctas_per_sm = tuning->ctas_per_sm;
+        a.min_lines_per_cta = tuning->min_lines_per_cta;
+    }
+    cudaError_t e = cudaMemsetAsync(errword, 0, sizeof(uint32_t), stream);
+    if (e == cudaSuccess)
+        e = tod2map ? launch_batch_tod2map(a, (const uint64_t *) (b + oo), total_lines, (const uint32_t *) (b + co), stream)
+                    : launch_batch_map2tod(a, (const uint64_t *) (b + oo), total_lines, (const uint32_t *) (b + co), stream);
+    return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
+}
+
+int gmm_batch_map2tod(const gmm_tod_desc *descs, int32_t ntod, int64_t total_lines, const float *local_map,
+                      const gmm_lpix *lp, const void *plan_buf, int32_t partial, int32_t accum,
+                      const gmm_batch_tuning *tuning, uint32_t *errword, cudaStream_t stream)
+{
+    return batch_op(false, descs, ntod, total_lines, nullptr, local_map, lp, plan_buf, partial, accum, tuning, errword,
+                    stream, "batch_map2tod");
+}
+
+int gmm_batch_tod2map(const gmm_tod_desc *descs, int32_t ntod, int64_t total_lines, float *local_map,
+                      const gmm_lpix *lp, const void *plan_buf, int32_t partial, const gmm_batch_tuning *tuning,
+                      uint32_t *errword, cudaStream_t stream)
+{
+    return batch_op(true, descs, ntod, total_lines, local_map, nullptr, lp, plan_buf, partial, 0, tuning, errword,
+                    stream, "batch_tod2map");
 }
 
 static int unplanned_op(bool tod2map, float *out, const float *in, const float *xp, int64_t nsamp, const gmm_lpix *lp,

@@ -505,6 +505,45 @@ void launch_planned_tod2map(Array<T> &local_map, const Array<T> &tod, const Arra
                                        &v, &plan.pp.info, plan.buf.data, partial, nullptr, 0));
 }
 
+void launch_planned_tod2map_compensated(Array<float> &local_map, Array<float> &comp, const Array<float> &tod,
+                                        const Array<float> &xpointing, const LocalPixelization &lpix,
+                                        const PointingPlan &plan, bool partial, long max_run_lines)
+{
+    const char *where = "launch_tod2map_compensated";
+    check_tod(tod, plan.nsamp, where, true);
+    check_local_map(local_map, lpix, where, true);
+    check_local_map(comp, lpix, where, true);
+    check_xpointing(xpointing, plan.nsamp, where, true);
+    check_op<float>(lpix, plan, where);
+    gmm_lpix v = lpix.device_view();
+    throw_on_error(gmm_planned_tod2map_compensated(local_map.data, comp.data, tod.data, xpointing.data, &v,
+                                                   &plan.pp.info, plan.buf.data, partial, max_run_lines, nullptr, 0));
+}
+
+void launch_planned_tod2map_f64(Array<double> &local_map, const Array<float> &tod, const Array<float> &xpointing,
+                                const LocalPixelization &lpix, const PointingPlan &plan, bool partial,
+                                long max_run_lines)
+{
+    const char *where = "launch_tod2map_f64";
+    check_tod(tod, plan.nsamp, where, true);
+    check_local_map(local_map, lpix, where, true);
+    check_xpointing(xpointing, plan.nsamp, where, true);
+    check_op<float>(lpix, plan, where);
+    gmm_lpix v = lpix.device_view();
+    throw_on_error(gmm_planned_tod2map_f64(local_map.data, tod.data, xpointing.data, &v, &plan.pp.info,
+                                           plan.buf.data, partial, max_run_lines, nullptr, 0));
+}
+
+void fold_compensation(Array<float> &local_map, Array<float> &comp)
+{
+    GMM_ASSERT(local_map.is_fully_contiguous() && comp.is_fully_contiguous(), "fold_compensation");
+    GMM_ASSERT(local_map.size == comp.size, "fold_compensation");
+    check_location(local_map.gpu, "fold_compensation", "map", true);
+    check_location(comp.gpu, "fold_compensation", "comp", true);
+    throw_on_error(gmm_fold_compensation(local_map.data, comp.data, local_map.size, 0));
+    cuda_check(cudaStreamSynchronize(0), "fold_compensation");
+}
+
 template<typename T>
 static long check_response(const Array<T> &response, long nsamp, const char *where)
 {

@@ -50,7 +50,27 @@ struct OpArgs {
     int64_t ystride, polstride;
     bool partial, accum;
     uint32_t *errword;
+    // tod2map precision modes (planned operators only).  flush: how tile partials and out-of-tile
+    // samples reach the map -- 0 float atomics into 'out'; 1 float atomics into 'out' plus each
+    // addition's rounding error (two-sum) into 'comp'; 2 double atomics into 'out64'.
+    // max_run_lines > 0 flushes the tile at least every that many cache lines.
+    int flush;
+    float *comp;
+    double *out64;
+    int64_t max_run_lines;
+    // Batches: per-TOD descriptors (owner words carry the TOD index in bits 48-63); xp, nsamp and
+    // the TOD pointer of the OpArgs are then unused.
+    const gmm_tod_desc *descs;
+    int ntod;
+    // Grid: operator CTAs per SM and minimum cache lines per CTA (0: the defaults).
+    int ctas_per_sm;
+    int min_lines_per_cta;
 };
+
+// Tile flush modes of OpArgs::flush.
+constexpr int kFlushF32 = 0;
+constexpr int kFlushCompensated = 1;
+constexpr int kFlushF64 = 2;
 
 // Raises a kernel's dynamic shared-memory limit, once per device: 'done' holds one bit per device
 // ordinal (ordinals >= 64 set it on every call).
@@ -74,6 +94,15 @@ cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, in
                                    cudaStream_t stream);
 cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                    cudaStream_t stream);
+cudaError_t launch_fold_compensation(float *lmap, float *comp, int64_t n, cudaStream_t stream);
+// Batches of TODs.
+constexpr int kBatchTodShift = 48;
+cudaError_t launch_batch_owner(const gmm_tod_desc *descs, int ntod, int64_t total_lines, int ny, int nx, bool periodic,
+                               uint64_t *owner_out, uint32_t *cellmap, uint32_t *errword, cudaStream_t stream);
+cudaError_t launch_batch_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                 cudaStream_t stream);
+cudaError_t launch_batch_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                 cudaStream_t stream);
 cudaError_t launch_unplanned_map2tod(const OpArgs &a, cudaStream_t stream);
 cudaError_t launch_unplanned_tod2map(const OpArgs &a, cudaStream_t stream);
 

@@ -140,9 +140,38 @@ __device__ void load_tile(float *tile, const int64_t *tab, const OpArgs &a, cons
     }
 }
 
-// Adds the tile into the map (one atomic per non-zero pixel and polarisation) and clears it.
+// One addition into the map at element 'off' in flush mode FLUSH (OpArgs::flush).  The
+// compensated mode keeps the rounding error of each float atomic (Knuth's two-sum, from the old
+// value the atomic returns) in 'comp', so that map + comp carries the sum to about twice float
+// precision until gmm_fold_compensation folds it in.
+// Rounding error of the float addition old + v (Knuth's two-sum), added into 'comp'.
+__device__ __forceinline__ void add_rounding_error(const OpArgs &a, int64_t off, float old, float v)
+{
+    const float sum = __fadd_rn(old, v);
+    const float bv = __fsub_rn(sum, old);
+    const float e = __fadd_rn(__fsub_rn(old, __fsub_rn(sum, bv)), __fsub_rn(v, bv));
+    if (e != 0.0f)
+        atomicAdd(a.comp + off, e);
+}
+
+template<int FLUSH>
+__device__ __forceinline__ void global_add(const OpArgs &a, int64_t off, float v)
+{
+    if constexpr (FLUSH == kFlushF64) {
+        atomicAdd(a.out64 + off, (double) v);
+    } else if constexpr (FLUSH == kFlushCompensated) {
+        add_rounding_error(a, off, atomicAdd(a.out + off, v), v);
+    } else {
+        atomicAdd(a.out + off, v);
+    }
+}
+
+// Adds the tile into the map (one atomic per non-zero pixel and polarisation, in flush mode FLUSH)
+// and clears it.
+template<int FLUSH = kFlushF32>
 __device__ void flush_tile(float *tile, const int64_t *tab, const OpArgs &a, float *__restrict__ lmap)
 {
+#pragma unroll(FLUSH == kFlushF32 ? 1 : 4)
     for (int idx = threadIdx.x; idx < TY * TX; idx += NT) {
         const int r = idx / TX, c = idx % TX;
         float *src = tile + r * TS + c;
@@ -151,9 +180,24 @@ __device__ void flush_tile(float *tile, const int64_t *tab, const OpArgs &a, flo
             const int64_t base = tab[(r >> 6) * TX + c];
             if (base >= 0) {
                 const int64_t off = base + (int64_t) (r & 63) * a.ystride;
-                atomicAdd(lmap + off, t);
-                atomicAdd(lmap + off + a.polstride, q);
-                atomicAdd(lmap + off + 2 * a.polstride, u);
+                if constexpr (FLUSH == kFlushF32) {
+                    atomicAdd(lmap + off, t);
+                    atomicAdd(lmap + off + a.polstride, q);
+                    atomicAdd(lmap + off + 2 * a.polstride, u);
+                } else if constexpr (FLUSH == kFlushCompensated) {
+                    // The three returning atomics are issued before any result is used, so their
+                    // round trips overlap.
+                    const float ot = atomicAdd(lmap + off, t);
+                    const float oq = atomicAdd(lmap + off + a.polstride, q);
+                    const float ou = atomicAdd(lmap + off + 2 * a.polstride, u);
+                    add_rounding_error(a, off, ot, t);
+                    add_rounding_error(a, off + a.polstride, oq, q);
+                    add_rounding_error(a, off + 2 * a.polstride, ou, u);
+                } else {
+                    global_add<FLUSH>(a, off, t);
+                    global_add<FLUSH>(a, off + a.polstride, q);
+                    global_add<FLUSH>(a, off + 2 * a.polstride, u);
+                }
             }
             src[0] = 0.0f;
             src[PS] = 0.0f;
@@ -187,15 +231,22 @@ __device__ __forceinline__ float global_eval(const OpArgs &a, const float *__res
     return ct * t + cq * q + cu * u;
 }
 
+template<int FLUSH = kFlushF32>
 __device__ __forceinline__ void global_accum(const OpArgs &a, float *__restrict__ lmap, int iy, int ix,
                                              float t, float q, float u, float w, uint32_t &err)
 {
     const int64_t off = global_pixel_offset(iy, ix, a);
     const bool valid = off >= 0;
     if (valid) {
-        atomicAdd(lmap + off, w * t);
-        atomicAdd(lmap + off + a.polstride, w * q);
-        atomicAdd(lmap + off + 2 * a.polstride, w * u);
+        if constexpr (FLUSH == kFlushF32) {
+            atomicAdd(lmap + off, w * t);
+            atomicAdd(lmap + off + a.polstride, w * q);
+            atomicAdd(lmap + off + 2 * a.polstride, w * u);
+        } else {
+            global_add<FLUSH>(a, off, w * t);
+            global_add<FLUSH>(a, off + a.polstride, w * q);
+            global_add<FLUSH>(a, off + 2 * a.polstride, w * u);
+        }
     }
     err |= (valid || a.partial) ? 0u : kErrNotInPixelization;
 }
@@ -276,7 +327,7 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
 // tile or, if the footprint is not inside it, global atomics.  o0..o2 are this lane's polarisation
 // plane offsets in rotated order and 'rot' selects the matching rotation of (t, q, u): in one atomic
 // instruction, lanes on the same pixel then target different words.
-template<bool RESP, bool PERIODIC>
+template<bool RESP, bool PERIODIC, int FLUSH = kFlushF32>
 __device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const Tile &T, float y, float x, float al,
                                            float tv, uint32_t s, int rot, int o0, int o1, int o2, uint32_t &err)
 {
@@ -319,10 +370,10 @@ __device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const T
         atomicAdd(p2 + TS + 1, w11 * v2);
     } else {
         uint32_t unused = 0;
-        global_accum(a, a.out, L.iy0, L.ix0, t, q, u, w00, unused);
-        global_accum(a, a.out, L.iy0, L.ix1, t, q, u, w01, unused);
-        global_accum(a, a.out, L.iy1, L.ix0, t, q, u, w10, unused);
-        global_accum(a, a.out, L.iy1, L.ix1, t, q, u, w11, unused);
+        global_accum<FLUSH>(a, a.out, L.iy0, L.ix0, t, q, u, w00, unused);
+        global_accum<FLUSH>(a, a.out, L.iy0, L.ix1, t, q, u, w01, unused);
+        global_accum<FLUSH>(a, a.out, L.iy1, L.ix0, t, q, u, w10, unused);
+        global_accum<FLUSH>(a, a.out, L.iy1, L.ix1, t, q, u, w11, unused);
     }
 }
 
@@ -397,10 +448,11 @@ __device__ uint32_t check_plan_cells(const uint32_t *__restrict__ cellmap, const
 // give the chunk's usable lines and the first entry of another cell (which ends the CTA's run).
 // The lines are then processed UNR at a time with one sample per lane, so the per-line decoding
 // costs a shuffle per sample.
-template<bool TOD2MAP, bool RESP, bool PERIODIC>
+template<bool TOD2MAP, bool RESP, bool PERIODIC, int FLUSH = kFlushF32, bool BATCH = false>
 __global__ void __launch_bounds__(NT, 2)
 planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, const uint32_t *__restrict__ cellmap)
 {
+    static_assert(!BATCH || (TOD2MAP && !RESP), "batched map2tod uses planned_map2tod_v4; no response variant");
     extern __shared__ float tile[];
     __shared__ int s_run[2];
     __shared__ uint32_t s_err[NW];
@@ -431,8 +483,11 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
         Tile T;
         T.gy0 = (int) (cell >> 10) << 6;
         T.gx0 = ((int) (cell & 1023u) << 6) - HX;
+        // With a run cap (precision modes) a run also ends after max_run_lines entries; the next run
+        // then continues the same cell with a fresh tile partial.
+        const int64_t erun = ((FLUSH != kFlushF32) && (a.max_run_lines > 0)) ? min(e1, start + a.max_run_lines) : e1;
         if (threadIdx.x == 0)
-            s_run[parity] = (int) (e1 - start);
+            s_run[parity] = (int) (erun - start);
         tile_offsets(s_tab, T, a);
         __syncthreads();
         if constexpr (!TOD2MAP) {
@@ -442,19 +497,24 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
 
         // The next chunk's owner word is fetched while this chunk is processed.
         int64_t c = start + warp * CH;
-        uint64_t wnext = ((lane < CH) && (c + lane < e1)) ? __ldg(owner_mt + c + lane) : 0ull;
-        for (; c < e1; c += NW * CH) {
-            const bool in = (lane < CH) && (c + lane < e1);
+        uint64_t wnext = ((lane < CH) && (c + lane < erun)) ? __ldg(owner_mt + c + lane) : 0ull;
+        for (; c < erun; c += NW * CH) {
+            const bool in = (lane < CH) && (c + lane < erun);
             const uint64_t w = wnext;
             const int64_t cn = c + NW * CH;
-            wnext = ((lane < CH) && (cn + lane < e1)) ? __ldg(owner_mt + cn + lane) : 0ull;
+            wnext = ((lane < CH) && (cn + lane < erun)) ? __ldg(owner_mt + cn + lane) : 0ull;
             // The owner list is sorted by cell: the first entry of another cell ends this run for
             // the whole CTA, and every later entry is past it as well.
             const bool same = in && ((uint32_t) (w & kCellMask) == cell);
             // A plan word always names a line < nsamp/32; anything else means the plan does not
             // belong to this xpointing, so flag it and skip the line.
             const uint32_t line = (uint32_t) ((w >> 20) & kClMask);
-            const bool line_ok = line < nlines;
+            uint32_t nl = nlines;
+            if constexpr (BATCH) {
+                const uint32_t td = (uint32_t) (w >> kBatchTodShift);
+                nl = ((td < (uint32_t) a.ntod) && !(w & kZflag)) ? (uint32_t) (__ldg(&a.descs[td].nsamp) >> 5) : 0u;
+            }
+            const bool line_ok = line < nl;
             err |= (same && !line_ok) ? kErrInconsistentNmt : 0u;
             const unsigned okmask = __ballot_sync(kFullMask, same && line_ok);
             const unsigned fmask = __ballot_sync(kFullMask, in && !same);
@@ -472,13 +532,26 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
                 float y[UNR], x[UNR], al[UNR], tv[UNR];
 #pragma unroll
                 for (int u = 0; u < UNR; u++) {
-                    y[u] = ok[u] ? __ldcs(yrow + s[u]) : 0.0f;
-                    x[u] = ok[u] ? __ldcs(xrow + s[u]) : 0.0f;
-                    al[u] = ok[u] ? __ldcs(arow + s[u]) : 0.0f;
-                    if constexpr (TOD2MAP)
-                        tv[u] = ok[u] ? __ldcs(a.in + s[u]) : 0.0f;
-                    else
-                        tv[u] = (a.accum && ok[u]) ? a.out[s[u]] : 0.0f;
+                    if constexpr (BATCH) {
+                        // Rows of the line's TOD (the TOD index is warp-uniform per line).
+                        const uint32_t td = __shfl_sync(kFullMask, (uint32_t) (w >> kBatchTodShift), g + u);
+                        const gmm_tod_desc *d = a.descs + ((td < (uint32_t) a.ntod) ? td : 0u);
+                        const float *yb = (const float *) __ldg((const unsigned long long *) &d->xpointing);
+                        const float *tb = (const float *) __ldg((const unsigned long long *) &d->tod);
+                        const int64_t ns = __ldg(&d->nsamp);
+                        y[u] = ok[u] ? __ldcs(yb + s[u]) : 0.0f;
+                        x[u] = ok[u] ? __ldcs(yb + ns + s[u]) : 0.0f;
+                        al[u] = ok[u] ? __ldcs(yb + 2 * ns + s[u]) : 0.0f;
+                        tv[u] = ok[u] ? __ldcs(tb + s[u]) : 0.0f;
+                    } else {
+                        y[u] = ok[u] ? __ldcs(yrow + s[u]) : 0.0f;
+                        x[u] = ok[u] ? __ldcs(xrow + s[u]) : 0.0f;
+                        al[u] = ok[u] ? __ldcs(arow + s[u]) : 0.0f;
+                        if constexpr (TOD2MAP)
+                            tv[u] = ok[u] ? __ldcs(a.in + s[u]) : 0.0f;
+                        else
+                            tv[u] = (a.accum && ok[u]) ? a.out[s[u]] : 0.0f;
+                    }
                 }
 #pragma unroll
                 for (int u = 0; u < UNR; u++) {
@@ -488,7 +561,7 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
                     // atomics, and the vote below would keep the compiler from overlapping one
                     // sample's arithmetic with the previous sample's atomics (measured slower).
                     if constexpr (TOD2MAP) {
-                        t2m_sample<RESP, PERIODIC>(a, tile, T, y[u], x[u], al[u], tv[u], s[u], rot, o0, o1, o2, err);
+                        t2m_sample<RESP, PERIODIC, FLUSH>(a, tile, T, y[u], x[u], al[u], tv[u], s[u], rot, o0, o1, o2, err);
                     } else {
                         // map2tod: fast path when every lane's sample passes tile_sample (the line
                         // is warp-uniform), else the general path.
@@ -511,7 +584,7 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
         __syncthreads();
         const int64_t next = start + s_run[parity];
         if constexpr (TOD2MAP)
-            flush_tile(tile, s_tab, a, a.out);
+            flush_tile<FLUSH>(tile, s_tab, a, a.out);
         parity ^= 1;
         __syncthreads();
         start = next;
@@ -523,11 +596,12 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
 // time: lane group g = lane/8 handles entry g's cache line, each lane four consecutive samples of it,
 // so xpointing and TOD move with one float4 load (or store) per lane and row, and the owner word
 // needs no shuffle.
-template<bool RESP, bool PERIODIC>
+template<bool RESP, bool PERIODIC, bool BATCH = false>
 __global__ void __launch_bounds__(NT, 2)
 planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner,
                    const uint32_t *__restrict__ cellmap)
 {
+    static_assert(!(BATCH && RESP), "batches have no response variant");
     extern __shared__ float tile[];
     __shared__ int s_run[2];
     __shared__ uint32_t s_err[NW];
@@ -568,7 +642,21 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
             // The owner list is sorted by cell: the first entry of another cell ends this run.
             const bool same = in && ((uint32_t) (w & kCellMask) == cell);
             const uint32_t line = (uint32_t) ((w >> 20) & kClMask);
-            const bool line_ok = line < nlines;
+            // Rows of this lane's line: the call's arrays, or (batches) those of the line's TOD.
+            const float *yb = yrow, *xb = xrow, *ab = arow;
+            float *ob = a.out;
+            uint32_t nl = nlines;
+            if constexpr (BATCH) {
+                const uint32_t td = (uint32_t) (w >> kBatchTodShift);
+                const gmm_tod_desc *d = a.descs + ((td < (uint32_t) a.ntod) ? td : 0u);
+                yb = (const float *) __ldg((const unsigned long long *) &d->xpointing);
+                const int64_t ns = __ldg(&d->nsamp);
+                xb = yb + ns;
+                ab = yb + 2 * ns;
+                ob = (float *) __ldg((const unsigned long long *) &d->tod);
+                nl = ((td < (uint32_t) a.ntod) && !(w & kZflag)) ? (uint32_t) (ns >> 5) : 0u;
+            }
+            const bool line_ok = line < nl;
             err |= (same && !line_ok) ? kErrInconsistentNmt : 0u;
             const bool ok = same && line_ok;
             const unsigned fmask = __ballot_sync(kFullMask, in && !same) & 0x01010101u;
@@ -578,11 +666,11 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
             const uint32_t s0 = (line << 5) + 4u * (uint32_t) sub;
             float4 y4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), x4 = y4, a4 = y4, t4 = y4;
             if (ok) {
-                y4 = __ldcs(reinterpret_cast<const float4 *>(yrow + s0));
-                x4 = __ldcs(reinterpret_cast<const float4 *>(xrow + s0));
-                a4 = __ldcs(reinterpret_cast<const float4 *>(arow + s0));
+                y4 = __ldcs(reinterpret_cast<const float4 *>(yb + s0));
+                x4 = __ldcs(reinterpret_cast<const float4 *>(xb + s0));
+                a4 = __ldcs(reinterpret_cast<const float4 *>(ab + s0));
                 if (a.accum)
-                    t4 = *reinterpret_cast<const float4 *>(a.out + s0);
+                    t4 = *reinterpret_cast<const float4 *>(ob + s0);
             }
             const float tv[4] = {t4.x, t4.y, t4.z, t4.w};
             // Fast path when all four samples of every lane pass tile_sample, else the general path.
@@ -600,13 +688,13 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
                         sample_factors<RESP>(a, s0 + k, S[k].sn, S[k].cs, ct, cq, cu);
                         r[k] = tv[k] + tile_eval<RESP>(tile, S[k].p, ct, cq, cu, S[k].dy, S[k].dx);
                     }
-                    __stcs(reinterpret_cast<float4 *>(a.out + s0), make_float4(r[0], r[1], r[2], r[3]));
+                    __stcs(reinterpret_cast<float4 *>(ob + s0), make_float4(r[0], r[1], r[2], r[3]));
                 }
             } else if (ok) {
                 // General path: the pointing is read again rather than kept live across the fast path.
-                const float4 yy = __ldcs(reinterpret_cast<const float4 *>(yrow + s0));
-                const float4 xx = __ldcs(reinterpret_cast<const float4 *>(xrow + s0));
-                const float4 aa = __ldcs(reinterpret_cast<const float4 *>(arow + s0));
+                const float4 yy = __ldcs(reinterpret_cast<const float4 *>(yb + s0));
+                const float4 xx = __ldcs(reinterpret_cast<const float4 *>(xb + s0));
+                const float4 aa = __ldcs(reinterpret_cast<const float4 *>(ab + s0));
                 const float yv[4] = {yy.x, yy.y, yy.z, yy.w};
                 const float xv[4] = {xx.x, xx.y, xx.z, xx.w};
                 const float av[4] = {aa.x, aa.y, aa.z, aa.w};
@@ -614,7 +702,7 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
 #pragma unroll
                 for (int k = 0; k < 4; k++)
                     r[k] = tv[k] + m2t_sample<RESP, PERIODIC>(a, tile, T, yv[k], xv[k], av[k], s0 + k, err);
-                __stcs(reinterpret_cast<float4 *>(a.out + s0), make_float4(r[0], r[1], r[2], r[3]));
+                __stcs(reinterpret_cast<float4 *>(ob + s0), make_float4(r[0], r[1], r[2], r[3]));
             }
             if (fmask != 0u)
                 break;
@@ -699,15 +787,23 @@ unplanned_kernel(OpArgs a)
 // sample per lane: with four lines in one atomic instruction its shared-memory bank conflicts cost
 // more than the wider loads save (measured).
 
-template<bool TOD2MAP, bool RESP, bool PERIODIC>
+// Grid of the planned kernels: 'ctas_per_sm' CTAs per SM (default 2, all resident), never fewer
+// than 'min_lines' cache lines per CTA (default 64) so that small plans reload few tiles.
+static int64_t planned_grid(const OpArgs &a, int64_t nowner)
+{
+    const int64_t per_sm = (a.ctas_per_sm > 0) ? a.ctas_per_sm : 2;
+    const int64_t min_lines = (a.min_lines_per_cta > 0) ? a.min_lines_per_cta : 64;
+    int64_t g = per_sm * (int64_t) device_sm_count();
+    return std::max<int64_t>(1, std::min<int64_t>(g, (nowner + min_lines - 1) / min_lines));
+}
+
+template<bool TOD2MAP, bool RESP, bool PERIODIC, int FLUSH = kFlushF32>
 cudaError_t launch_planned_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                 cudaStream_t stream)
 {
     if (nowner <= 0)
         return cudaSuccess;
-    // Two CTAs per SM; never fewer than ~64 cache lines per CTA, so small plans reload few tiles.
-    int64_t g = 2 * (int64_t) device_sm_count();
-    g = std::max<int64_t>(1, std::min<int64_t>(g, (nowner + 63) / 64));
+    const int64_t g = planned_grid(a, nowner);
     if constexpr (!TOD2MAP) {
         if (((((uintptr_t) a.xp) | ((uintptr_t) a.out)) & 15) == 0) {
             static std::atomic<uint64_t> attr_v4_done{0};
@@ -719,19 +815,44 @@ cudaError_t launch_planned_impl(const OpArgs &a, const uint64_t *owner_mt, int64
         }
     }
     static std::atomic<uint64_t> attr_done{0};
-    cudaError_t e = set_smem_limit(planned_kernel<TOD2MAP, RESP, PERIODIC>, kTileBytes, attr_done);
+    cudaError_t e = set_smem_limit(planned_kernel<TOD2MAP, RESP, PERIODIC, FLUSH>, kTileBytes, attr_done);
     if (e != cudaSuccess)
         return e;
-    planned_kernel<TOD2MAP, RESP, PERIODIC><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner, cellmap);
+    planned_kernel<TOD2MAP, RESP, PERIODIC, FLUSH><<<(unsigned) g, NT, kTileBytes, stream>>>(a, owner_mt, nowner,
+                                                                                            cellmap);
     return cudaGetLastError();
+}
+
+template<bool TOD2MAP, bool RESP, int FLUSH>
+cudaError_t launch_planned_periodic(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                    cudaStream_t stream)
+{
+    return a.periodic ? launch_planned_impl<TOD2MAP, RESP, true, FLUSH>(a, owner_mt, nowner, cellmap, stream)
+                      : launch_planned_impl<TOD2MAP, RESP, false, FLUSH>(a, owner_mt, nowner, cellmap, stream);
 }
 
 template<bool TOD2MAP, bool RESP>
 cudaError_t launch_planned_dispatch(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                     cudaStream_t stream)
 {
-    return a.periodic ? launch_planned_impl<TOD2MAP, RESP, true>(a, owner_mt, nowner, cellmap, stream)
-                      : launch_planned_impl<TOD2MAP, RESP, false>(a, owner_mt, nowner, cellmap, stream);
+    if constexpr (TOD2MAP) {
+        if (a.flush == kFlushCompensated)
+            return launch_planned_periodic<true, RESP, kFlushCompensated>(a, owner_mt, nowner, cellmap, stream);
+        if (a.flush == kFlushF64)
+            return launch_planned_periodic<true, RESP, kFlushF64>(a, owner_mt, nowner, cellmap, stream);
+    }
+    return launch_planned_periodic<TOD2MAP, RESP, kFlushF32>(a, owner_mt, nowner, cellmap, stream);
+}
+
+__global__ void fold_compensation_kernel(float *__restrict__ lmap, float *__restrict__ comp, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+        const float c = comp[i];
+        if (c != 0.0f) {
+            lmap[i] += c;
+            comp[i] = 0.0f;
+        }
+    }
 }
 
 template<bool TOD2MAP>
@@ -763,6 +884,59 @@ cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, in
 {
     return a.response ? launch_planned_dispatch<true, true>(a, owner_mt, nowner, cellmap, stream)
                       : launch_planned_dispatch<true, false>(a, owner_mt, nowner, cellmap, stream);
+}
+
+template<bool PERIODIC>
+cudaError_t launch_batch_map2tod_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner,
+                                      const uint32_t *cellmap, cudaStream_t stream)
+{
+    static std::atomic<uint64_t> attr_done{0};
+    cudaError_t e = set_smem_limit(planned_map2tod_v4<false, PERIODIC, true>, kTileBytes, attr_done);
+    if (e != cudaSuccess)
+        return e;
+    planned_map2tod_v4<false, PERIODIC, true><<<(unsigned) planned_grid(a, nowner), NT, kTileBytes, stream>>>(
+        a, owner_mt, nowner, cellmap);
+    return cudaGetLastError();
+}
+
+template<bool PERIODIC>
+cudaError_t launch_batch_tod2map_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner,
+                                      const uint32_t *cellmap, cudaStream_t stream)
+{
+    static std::atomic<uint64_t> attr_done{0};
+    cudaError_t e = set_smem_limit(planned_kernel<true, false, PERIODIC, kFlushF32, true>, kTileBytes, attr_done);
+    if (e != cudaSuccess)
+        return e;
+    planned_kernel<true, false, PERIODIC, kFlushF32, true><<<(unsigned) planned_grid(a, nowner), NT, kTileBytes, stream>>>(
+        a, owner_mt, nowner, cellmap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_compensation(float *lmap, float *comp, int64_t n, cudaStream_t stream)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 8 * (int64_t) device_sm_count()));
+    fold_compensation_kernel<<<(unsigned) g, 256, 0, stream>>>(lmap, comp, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                 cudaStream_t stream)
+{
+    if (nowner <= 0)
+        return cudaSuccess;
+    return a.periodic ? launch_batch_map2tod_impl<true>(a, owner_mt, nowner, cellmap, stream)
+                      : launch_batch_map2tod_impl<false>(a, owner_mt, nowner, cellmap, stream);
+}
+
+cudaError_t launch_batch_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                 cudaStream_t stream)
+{
+    if (nowner <= 0)
+        return cudaSuccess;
+    return a.periodic ? launch_batch_tod2map_impl<true>(a, owner_mt, nowner, cellmap, stream)
+                      : launch_batch_tod2map_impl<false>(a, owner_mt, nowner, cellmap, stream);
 }
 
 cudaError_t launch_unplanned_map2tod(const OpArgs &a, cudaStream_t stream)

@@ -564,6 +564,98 @@ cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, 
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------------------------
+// Batch plan: one owner word per cache line of every TOD of a batch.
+
+// Index of the TOD holding global cache line 'gl' (descs[i].line0 ascending): binary search.
+__device__ __forceinline__ int batch_tod_of_line(const gmm_tod_desc *__restrict__ descs, int ntod, int64_t gl)
+{
+    int lo = 0, hi = ntod - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&descs[mid].line0) <= gl)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// One warp per cache line (lane = sample), grid-stride over the batch's lines.  The owner cell is
+// the lowest cell among the four neighbours of the line's samples (the cells of a line are those of
+// cell_enumerator, gpu_mm_internals.hpp:179-237); every cell the line touches is marked in the
+// cell bitmap.  Word = cell | line << 20 | mflag << 46 | tod << 48, at the line's global index.
+__global__ void __launch_bounds__(256)
+batch_owner_kernel(const gmm_tod_desc *__restrict__ descs, int ntod, int64_t total_lines, int ny, int nx,
+                   bool periodic, uint64_t *__restrict__ owner_out, uint32_t *__restrict__ cellmap,
+                   uint32_t *__restrict__ errword)
+{
+    __shared__ uint32_t s_err[8];
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t) gridDim.x * (blockDim.x >> 5);
+    uint32_t err = 0;
+    for (int64_t gl = (int64_t) blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); gl < total_lines; gl += nwarps) {
+        const int tod = batch_tod_of_line(descs, ntod, gl);
+        const float *xp = (const float *) __ldg((const unsigned long long *) &descs[tod].xpointing);
+        const int64_t nsamp = __ldg(&descs[tod].nsamp);
+        const int64_t line = gl - __ldg(&descs[tod].line0);
+        // Descriptors that do not match total_lines (line outside its TOD) are flagged; the line's
+        // word carries bit 47 ("invalid"), which the operators refuse.
+        if ((line < 0) || (32 * line >= nsamp) || (line >= (1ll << 26))) {
+            err |= kErrInconsistentNmt;
+            if (lane == 0)
+                owner_out[gl] = kZflag | ((uint64_t) tod << kBatchTodShift);
+            continue;
+        }
+        const int64_t s = 32 * line + lane;
+        Located L;
+        err |= locate(__ldcs(xp + s), __ldcs(xp + nsamp + s), ny, nx, periodic, L);
+        const uint32_t c00 = ((uint32_t) (L.iy0 >> 6) << 10) | (uint32_t) (L.ix0 >> 6);
+        const uint32_t c01 = ((uint32_t) (L.iy0 >> 6) << 10) | (uint32_t) (L.ix1 >> 6);
+        const uint32_t c10 = ((uint32_t) (L.iy1 >> 6) << 10) | (uint32_t) (L.ix0 >> 6);
+        const uint32_t c11 = ((uint32_t) (L.iy1 >> 6) << 10) | (uint32_t) (L.ix1 >> 6);
+        const uint32_t lo = min(min(c00, c01), min(c10, c11));
+        const uint32_t hi = max(max(c00, c01), max(c10, c11));
+        const uint32_t owner = __reduce_min_sync(kFullMask, lo);
+        const bool multi = __any_sync(kFullMask, hi != owner);
+        if (lane == 0) {
+            owner_out[gl] = (uint64_t) owner | ((uint64_t) line << 20) | ((uint64_t) multi << 46) |
+                            ((uint64_t) tod << kBatchTodShift);
+            atomicOr(cellmap + (owner >> 5), 1u << (owner & 31));
+        }
+        if (multi) {
+            // Cells other than the owner: each lane marks its own (duplicates are harmless).
+            const uint32_t cs[4] = {c00, c01, c10, c11};
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (cs[k] != owner)
+                    atomicOr(cellmap + (cs[k] >> 5), 1u << (cs[k] & 31));
+        }
+    }
+    err = __reduce_or_sync(kFullMask, err);
+    if (lane == 0)
+        s_err[threadIdx.x >> 5] = err;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t e = 0;
+        for (int w = 0; w < (int) (blockDim.x >> 5); w++)
+            e |= s_err[w];
+        if (e)
+            atomicOr(errword, e);
+    }
+}
+
+cudaError_t launch_batch_owner(const gmm_tod_desc *descs, int ntod, int64_t total_lines, int ny, int nx, bool periodic,
+                               uint64_t *owner_out, uint32_t *cellmap, uint32_t *errword, cudaStream_t stream)
+{
+    if (total_lines <= 0)
+        return cudaSuccess;
+    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((total_lines + 7) / 8, 16 * (int64_t) device_sm_count()));
+    batch_owner_kernel<<<(unsigned) g, 256, 0, stream>>>(descs, ntod, total_lines, ny, nx, periodic, owner_out, cellmap,
+                                                         errword);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_preplan(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
                            int nblocks, uint32_t *nmt, uint32_t *err, cudaStream_t stream)
 {

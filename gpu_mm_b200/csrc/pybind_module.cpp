@@ -105,6 +105,81 @@ PYBIND11_MODULE(gpu_mm_pybind11, m)
     m.doc() = "gpu_mm_b200: B200-native pointing operators (drop-in for gpu_mm.gpu_mm_pybind11)";
 
     m.def("_get_tsize", []() { return sizeof(float); });
+    // ---- Batches of TODs (raw device pointers; gpu_mm_b200.batch.TodBatch wraps them) ----
+    auto tuning_of = [](py::object t) {
+        gmm_batch_tuning bt;
+        throw_on_error(gmm_batch_tuning_default(&bt));
+        if (!t.is_none()) {
+            py::tuple tt = t.cast<py::tuple>();
+            bt.sort_digit_bits = tt[0].cast<int>();
+            bt.ctas_per_sm = tt[1].cast<int>();
+            bt.min_lines_per_cta = tt[2].cast<int>();
+        }
+        return bt;
+    };
+    m.def("batch_tuning_default", []() {
+        gmm_batch_tuning bt;
+        throw_on_error(gmm_batch_tuning_default(&bt));
+        return py::make_tuple(bt.sort_digit_bits, bt.ctas_per_sm, bt.min_lines_per_cta);
+    });
+    m.def("batch_plan_nbytes", [tuning_of](long total_lines, int ny, int nx, py::object tuning) {
+        gmm_batch_tuning bt = tuning_of(tuning);
+        int64_t pn = 0, tn = 0;
+        throw_on_error(gmm_batch_plan_nbytes(total_lines, ny, nx, &bt, &pn, &tn));
+        return py::make_tuple(pn, tn);
+    }, py::arg("total_lines"), py::arg("nypix_global"), py::arg("nxpix_global"), py::arg("tuning") = py::none());
+    m.def("batch_plan_build",
+          [tuning_of](uintptr_t descs, int ntod, long total_lines, int ny, int nx, bool periodic, uintptr_t plan,
+                      long plan_nbytes, uintptr_t tmp, long tmp_nbytes, py::object tuning, uintptr_t errword,
+                      uintptr_t stream) {
+              gmm_batch_tuning bt = tuning_of(tuning);
+              py::gil_scoped_release rel;
+              throw_on_error(gmm_batch_plan_build((const gmm_tod_desc *) descs, ntod, total_lines, ny, nx, periodic,
+                                                  (void *) plan, plan_nbytes, (void *) tmp, tmp_nbytes, &bt,
+                                                  (uint32_t *) errword, (cudaStream_t) stream));
+          },
+          py::arg("descs"), py::arg("ntod"), py::arg("total_lines"), py::arg("nypix_global"), py::arg("nxpix_global"),
+          py::arg("periodic_xcoord"), py::arg("plan"), py::arg("plan_nbytes"), py::arg("tmp"), py::arg("tmp_nbytes"),
+          py::arg("tuning"), py::arg("errword"), py::arg("stream") = 0);
+    m.def("batch_map2tod",
+          [tuning_of](uintptr_t descs, int ntod, long total_lines, py::object local_map, const LocalPixelization &lpix,
+                      uintptr_t plan, bool partial_pixelization, bool accum, py::object tuning, uintptr_t errword,
+                      uintptr_t stream) {
+              Array<float> m_ = to_array<float>(local_map, "local_map");
+              if (!m_.gpu || m_.size != 3 * lpix.npix)
+                  throw std::runtime_error("batch_map2tod: local_map must be a GPU array of size 3*npix");
+              gmm_batch_tuning bt = tuning_of(tuning);
+              gmm_lpix v = lpix.device_view();
+              py::gil_scoped_release rel;
+              throw_on_error(gmm_batch_map2tod((const gmm_tod_desc *) descs, ntod, total_lines, m_.data, &v,
+                                               (const void *) plan, partial_pixelization, accum, &bt,
+                                               (uint32_t *) errword, (cudaStream_t) stream));
+          },
+          py::arg("descs"), py::arg("ntod"), py::arg("total_lines"), py::arg("local_map"), py::arg("local_pixelization"),
+          py::arg("plan"), py::arg("partial_pixelization"), py::arg("accum"), py::arg("tuning"), py::arg("errword"),
+          py::arg("stream") = 0);
+    m.def("batch_tod2map",
+          [tuning_of](uintptr_t descs, int ntod, long total_lines, py::object local_map, const LocalPixelization &lpix,
+                      uintptr_t plan, bool partial_pixelization, py::object tuning, uintptr_t errword,
+                      uintptr_t stream) {
+              Array<float> m_ = to_array<float>(local_map, "local_map");
+              if (!m_.gpu || m_.size != 3 * lpix.npix)
+                  throw std::runtime_error("batch_tod2map: local_map must be a GPU array of size 3*npix");
+              gmm_batch_tuning bt = tuning_of(tuning);
+              gmm_lpix v = lpix.device_view();
+              py::gil_scoped_release rel;
+              throw_on_error(gmm_batch_tod2map((const gmm_tod_desc *) descs, ntod, total_lines, m_.data, &v,
+                                               (const void *) plan, partial_pixelization, &bt, (uint32_t *) errword,
+                                               (cudaStream_t) stream));
+          },
+          py::arg("descs"), py::arg("ntod"), py::arg("total_lines"), py::arg("local_map"), py::arg("local_pixelization"),
+          py::arg("plan"), py::arg("partial_pixelization"), py::arg("tuning"), py::arg("errword"),
+          py::arg("stream") = 0);
+    m.def("errword_read", [](uintptr_t errword, unsigned ignore, uintptr_t stream) {
+        py::gil_scoped_release rel;
+        throw_on_error(gmm_errword_read((const uint32_t *) errword, ignore, (cudaStream_t) stream));
+    }, py::arg("errword"), py::arg("ignore") = 0, py::arg("stream") = 0);
+
     m.def("_version", []() { return std::string(gmm_version()); });
     m.def("_set_sort_digit_bits", [](int bits) { throw_on_error(gmm_set_sort_digit_bits(bits)); });
     m.def("_get_sort_digit_bits", []() { return gmm_get_sort_digit_bits(); });
@@ -200,6 +275,41 @@ PYBIND11_MODULE(gpu_mm_pybind11, m)
           },
           py::arg("tod"), py::arg("local_map"), py::arg("xpointing"), py::arg("local_pixelization"), py::arg("plan"),
           py::arg("partial_pixelization"), py::arg("debug"), py::arg("accum"));
+
+    // Precision variants of planned tod2map (no counterpart in the reference).
+    m.def("planned_tod2map_compensated",
+          [](py::object local_map, py::object comp, py::object tod, py::object xpointing,
+             const LocalPixelization &lpix, const PointingPlan &plan, bool partial_pixelization, long max_run_lines) {
+              Array<float> m_ = to_array<float>(local_map, "local_map");
+              Array<float> c = to_array<float>(comp, "comp");
+              Array<float> t = to_array<float>(tod, "tod");
+              Array<float> x = to_array<float>(xpointing, "xpointing");
+              py::gil_scoped_release rel;
+              launch_planned_tod2map_compensated(m_, c, t, x, lpix, plan, partial_pixelization, max_run_lines);
+          },
+          py::arg("local_map"), py::arg("comp"), py::arg("tod"), py::arg("xpointing"), py::arg("local_pixelization"),
+          py::arg("plan"), py::arg("partial_pixelization") = false, py::arg("max_run_lines") = 0);
+
+    m.def("planned_tod2map_f64",
+          [](py::object local_map, py::object tod, py::object xpointing, const LocalPixelization &lpix,
+             const PointingPlan &plan, bool partial_pixelization, long max_run_lines) {
+              Array<double> m_ = to_array<double>(local_map, "local_map");
+              Array<float> t = to_array<float>(tod, "tod");
+              Array<float> x = to_array<float>(xpointing, "xpointing");
+              py::gil_scoped_release rel;
+              launch_planned_tod2map_f64(m_, t, x, lpix, plan, partial_pixelization, max_run_lines);
+          },
+          py::arg("local_map"), py::arg("tod"), py::arg("xpointing"), py::arg("local_pixelization"), py::arg("plan"),
+          py::arg("partial_pixelization") = false, py::arg("max_run_lines") = 0);
+
+    m.def("fold_compensation",
+          [](py::object local_map, py::object comp) {
+              Array<float> m_ = to_array<float>(local_map, "local_map");
+              Array<float> c = to_array<float>(comp, "comp");
+              py::gil_scoped_release rel;
+              fold_compensation(m_, c);
+          },
+          py::arg("local_map"), py::arg("comp"));
 
     m.def("planned_tod2map",
           [](py::object local_map, py::object tod, py::object xpointing, const LocalPixelization &lpix,

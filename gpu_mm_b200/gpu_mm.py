@@ -118,6 +118,40 @@ def tod2map(local_map, tod, xpointing, plan, partial_pixelization=False, respons
 
 
 ####################################################################################################
+#
+# Precision variants of planned tod2map (no counterpart in the reference).  The samples are
+# processed exactly as by tod2map() (float arithmetic, float partial sums in a shared-memory tile
+# per cell); only the reduction of those partials into the map differs.
+
+
+def tod2map_compensated(local_map, comp, tod, xpointing, plan, partial_pixelization=False, max_run_lines=0):
+    """tod2map() into a float LocalMap whose float companion 'comp' (same size, zeroed before the
+    first call) collects the rounding error of every float addition into the map (two-sum).
+    local_map + comp then holds the sum to about twice float precision, across any number of calls;
+    fold_compensation() adds comp into the map.  max_run_lines > 0 reduces each shared-memory tile
+    partial into the map after at most that many 32-sample cache lines."""
+    if not isinstance(local_map, LocalMap) or not isinstance(plan, PointingPlan):
+        raise RuntimeError("tod2map_compensated(): expected a LocalMap and a PointingPlan")
+    gpu_mm_pybind11.planned_tod2map_compensated(local_map.arr, comp, tod, xpointing, local_map.pixelization, plan,
+                                                partial_pixelization, int(max_run_lines))
+
+
+def fold_compensation(local_map, comp):
+    """Adds the compensation array of tod2map_compensated() into the map and zeroes it."""
+    arr = local_map.arr if isinstance(local_map, LocalMap) else local_map
+    gpu_mm_pybind11.fold_compensation(arr, comp)
+
+
+def tod2map_f64(map64, local_pixelization, tod, xpointing, plan, partial_pixelization=False, max_run_lines=0):
+    """tod2map() into a float64 map (contiguous, 3*npix doubles, laid out by 'local_pixelization'):
+    float tile partials, reduced with double atomics."""
+    if not isinstance(local_pixelization, LocalPixelization) or not isinstance(plan, PointingPlan):
+        raise RuntimeError("tod2map_f64(): expected a LocalPixelization and a PointingPlan")
+    gpu_mm_pybind11.planned_tod2map_f64(map64, tod, xpointing, local_pixelization, plan, partial_pixelization,
+                                        int(max_run_lines))
+
+
+####################################################################################################
 
 
 def _to_numpy_int64(a):

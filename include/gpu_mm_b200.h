@@ -152,6 +152,74 @@ int gmm_planned_tod2map(float *local_map, const float *tod, const float *xpointi
                         const gmm_preplan_info *info, const void *plan_buf, int32_t partial_pixelization,
                         uint32_t *errword_gpu, cudaStream_t stream);
 
+/* ---- Batches of TODs (no counterpart in the reference, which plans and applies one TOD per call).
+ *
+ * A batch is up to 65535 TODs, each with its own xpointing [3][nsamp] and TOD [nsamp] (16-byte
+ * aligned, nsamp a positive multiple of 32), against one local pixelization.  The caller keeps an
+ * array of gmm_tod_desc in device memory; line0 of TOD i is the sum of nsamp/32 over TODs < i, and
+ * total_lines the sum over all.  A batch plan is one owner list over all the batch's cache lines,
+ * sorted by cell (tile loads are shared by every TOD that hits a cell), plus the bitmap of cells the
+ * lines touch.  Its size depends only on total_lines, so building it needs no host synchronisation
+ * and can be captured in a CUDA graph together with the operators.  Device error bits go to
+ * 'errword_gpu' (required; read it with gmm_errword_read). */
+typedef struct gmm_tod_desc {
+    const float *xpointing;   /* [3][nsamp] */
+    float *tod;               /* [nsamp]: map2tod output, tod2map input */
+    int64_t nsamp;
+    int64_t line0;
+} gmm_tod_desc;
+
+/* Launch and sort parameters of the batched kernels (gmm_batch_tuning_default fills the defaults;
+ * an autotuner may pick others).  sort_digit_bits: radix digit width of the plan sort (4..11);
+ * ctas_per_sm: operator CTAs per SM in the grid (1..8, two are resident at a time);
+ * min_lines_per_cta: lower bound on the cache lines of one CTA's slice. */
+typedef struct gmm_batch_tuning {
+    int32_t sort_digit_bits;
+    int32_t ctas_per_sm;
+    int32_t min_lines_per_cta;
+    int32_t reserved;
+} gmm_batch_tuning;
+
+int gmm_batch_tuning_default(gmm_batch_tuning *tuning);
+
+/* Sizes of a batch plan and of its construction scratch. */
+int gmm_batch_plan_nbytes(int64_t total_lines, int32_t nypix_global, int32_t nxpix_global,
+                          const gmm_batch_tuning *tuning, int64_t *plan_nbytes, int64_t *tmp_nbytes);
+
+/* Builds the batch plan into 'plan_buf' (128-byte aligned) using 'tmp' (128-byte aligned). */
+int gmm_batch_plan_build(const gmm_tod_desc *descs_gpu, int32_t ntod, int64_t total_lines, int32_t nypix_global,
+                         int32_t nxpix_global, int32_t periodic_xcoord, void *plan_buf, int64_t plan_nbytes, void *tmp,
+                         int64_t tmp_nbytes, const gmm_batch_tuning *tuning, uint32_t *errword_gpu, cudaStream_t stream);
+
+/* map2tod / tod2map of every TOD of the batch in one launch each, with the semantics of
+ * gmm_planned_map2tod / gmm_planned_tod2map per TOD. */
+int gmm_batch_map2tod(const gmm_tod_desc *descs_gpu, int32_t ntod, int64_t total_lines, const float *local_map,
+                      const gmm_lpix *lpix, const void *plan_buf, int32_t partial_pixelization, int32_t accum,
+                      const gmm_batch_tuning *tuning, uint32_t *errword_gpu, cudaStream_t stream);
+int gmm_batch_tod2map(const gmm_tod_desc *descs_gpu, int32_t ntod, int64_t total_lines, float *local_map,
+                      const gmm_lpix *lpix, const void *plan_buf, int32_t partial_pixelization,
+                      const gmm_batch_tuning *tuning, uint32_t *errword_gpu, cudaStream_t stream);
+
+/* Precision variants of planned tod2map.  No counterpart in the reference, whose tod2map
+ * accumulates in float only (tod2map.cu:157-226); its sample arithmetic is unchanged here (float,
+ * shared-memory tile partials), only the reduction into the map differs:
+ *   _compensated: float map plus a float 'comp' array of the same size (caller-owned, zeroed
+ *                 before the first call) that collects the rounding error of every float addition
+ *                 into the map (two-sum).  local_map + comp then holds the sum to about twice float
+ *                 precision; gmm_fold_compensation adds comp into local_map and zeroes comp.
+ *   _f64:         double local map (same cell_offsets / ystride / polstride, in doubles); partials
+ *                 are reduced with double atomics.
+ * max_run_lines > 0 bounds how many cache lines a tile partial collects before it is reduced into
+ * the map (0: once per cell, as the float path). */
+int gmm_planned_tod2map_compensated(float *local_map, float *comp, const float *tod, const float *xpointing,
+                                    const gmm_lpix *lpix, const gmm_preplan_info *info, const void *plan_buf,
+                                    int32_t partial_pixelization, int64_t max_run_lines, uint32_t *errword_gpu,
+                                    cudaStream_t stream);
+int gmm_planned_tod2map_f64(double *local_map, const float *tod, const float *xpointing, const gmm_lpix *lpix,
+                            const gmm_preplan_info *info, const void *plan_buf, int32_t partial_pixelization,
+                            int64_t max_run_lines, uint32_t *errword_gpu, cudaStream_t stream);
+int gmm_fold_compensation(float *local_map, float *comp, int64_t n, cudaStream_t stream);
+
 /* Replaces launch_response_map2tod<float> / launch_response_tod2map<float> (gpu_mm.hpp:179-202,
  * map2tod_response.cu:205-290, tod2map_response.cu).  response is [2][ndet] (T, P), ndet divides nsamp. */
 int gmm_response_map2tod(float *tod, const float *local_map, const float *xpointing, const float *response,

@@ -181,6 +181,18 @@ void launch_unplanned_tod2map(Array<T> &local_map, const Array<T> &tod, const Ar
                               const LocalPixelization &local_pixelization, Array<uint> &errflags,
                               bool partial_pixelization);
 
+// Precision variants of planned tod2map (no counterpart in the reference; see gpu_mm_b200.h):
+// float map plus a same-size float compensation array collecting the rounding error of every float
+// addition into the map (fold it in with fold_compensation), or a double map.  max_run_lines > 0
+// bounds how many cache lines a shared-memory tile partial collects before it is reduced.
+void launch_planned_tod2map_compensated(Array<float> &local_map, Array<float> &comp, const Array<float> &tod,
+                                        const Array<float> &xpointing, const LocalPixelization &local_pixelization,
+                                        const PointingPlan &plan, bool partial_pixelization, long max_run_lines = 0);
+void launch_planned_tod2map_f64(Array<double> &local_map, const Array<float> &tod, const Array<float> &xpointing,
+                                const LocalPixelization &local_pixelization, const PointingPlan &plan,
+                                bool partial_pixelization, long max_run_lines = 0);
+void fold_compensation(Array<float> &local_map, Array<float> &comp);
+
 // Non-blocking forms used by batched and served callers: the device error bits are OR-ed into
 // '*errword' (device memory, zeroed by the call) and checked later with check_errword(); nothing
 // synchronises.  'stream' 0 is the legacy default stream.

@@ -102,6 +102,8 @@ def lib():
         L.oracle_map2tod_f32_mt.restype = u32
         L.oracle_tod2map_f32_mt.argtypes = [fp, fp, fp, i64, i64, LP, i32, i32]
         L.oracle_tod2map_f32_mt.restype = u32
+        L.oracle_tod2map_f64w_mt.argtypes = [ctypes.POINTER(ctypes.c_double), fp, fp, i64, i64, LP, i32, i32]
+        L.oracle_tod2map_f64w_mt.restype = u32
         L.oracle_preplan.argtypes = [fp, i64, i32, i32, i32, ctypes.POINTER(u32), ctypes.POINTER(i64),
                                      ctypes.POINTER(u32)]
         L.oracle_preplan.restype = i64
@@ -198,6 +200,15 @@ def tod2map_mt(lmap, tod, xpointing, lpix, nthreads, partial_pixelization=False,
     f = ref().ref_tod2map_f32_mt if use_ref else lib().oracle_tod2map_f32_mt
     return f(_ptr(lmap, ct), _ptr(tod, ct), _ptr(xpointing, ct), _nsamp(xpointing), lmap.size,
              ctypes.byref(lpix.struct), int(partial_pixelization), int(nthreads))
+
+
+def tod2map_f64w_mt(lmap64, tod, xpointing, lpix, nthreads, partial_pixelization=False):
+    """reference_tod2map<double> on float32 tod/xpointing widened to double; lmap64 is float64 and
+    accumulates (the FP64 oracle of the tod2map precision variants)."""
+    assert lmap64.dtype == np.float64 and tod.dtype == np.float32 and xpointing.dtype == np.float32
+    return lib().oracle_tod2map_f64w_mt(_ptr(lmap64, ctypes.c_double), _ptr(tod, ctypes.c_float),
+                                        _ptr(xpointing, ctypes.c_float), _nsamp(xpointing), lmap64.size,
+                                        ctypes.byref(lpix.struct), int(partial_pixelization), int(nthreads))
 
 
 def response_map2tod(tod, lmap, xpointing, response, lpix, partial_pixelization=False, accum=False):

@@ -288,6 +288,75 @@ uint32_t oracle_response_tod2map_f32(float *lmap, const float *tod, const float 
 /* ------------------------------------------------------------------------------------------ */
 /* Multi-threaded CPU baseline: contiguous sample ranges per thread.                           */
 
+/* reference_tod2map<double> (tod2map_reference.cu:32-43) on float32 TOD and xpointing widened to
+ * double: the FP64 oracle of the tod2map precision variants. */
+static uint32_t tod2map_range_f64w(double *lmap, const float *tod, const float *xp, int64_t nsamp, int64_t s0,
+                                   int64_t s1, const oracle_lpix *lp, int partial)
+{
+    uint32_t err = 0;
+    for (int64_t s = s0; s < s1; s++) {
+        double ypix = xp[s], xpix = xp[s + nsamp], alpha = xp[s + 2 * nsamp];
+        double t = tod[s];
+        double sn, cs;
+        sincos(2 * alpha, &sn, &cs);
+        int iy0, iy1, ix0, ix1;
+        double dy, dx;
+        err |= locate_f64(ypix, xpix, lp->nypix_global, lp->nxpix_global, lp->periodic_xcoord, &iy0, &iy1, &ix0,
+                          &ix1, &dy, &dx);
+        double q = t * cs, u = t * sn;
+        accum_f64(lmap, lp, iy0, ix0, t, q, u, (1 - dy) * (1 - dx), partial, &err);
+        accum_f64(lmap, lp, iy0, ix1, t, q, u, (1 - dy) * (dx), partial, &err);
+        accum_f64(lmap, lp, iy1, ix0, t, q, u, (dy) * (1 - dx), partial, &err);
+        accum_f64(lmap, lp, iy1, ix1, t, q, u, (dy) * (dx), partial, &err);
+    }
+    return err;
+}
+
+typedef struct {
+    double *out;
+    const float *tod, *xp;
+    int64_t nsamp, s0, s1;
+    const oracle_lpix *lp;
+    int partial;
+    uint32_t err;
+} mt_job_f64w;
+
+static void *tod2map_f64w_worker(void *arg)
+{
+    mt_job_f64w *j = (mt_job_f64w *) arg;
+    j->err = tod2map_range_f64w(j->out, j->tod, j->xp, j->nsamp, j->s0, j->s1, j->lp, j->partial);
+    return NULL;
+}
+
+uint32_t oracle_tod2map_f64w_mt(double *lmap, const float *tod, const float *xp, int64_t nsamp, int64_t map_size,
+                                const oracle_lpix *lp, int32_t partial, int32_t nthreads)
+{
+    if (nthreads < 1) nthreads = 1;
+    pthread_t *th = (pthread_t *) calloc(nthreads, sizeof(pthread_t));
+    mt_job_f64w *jobs = (mt_job_f64w *) calloc(nthreads, sizeof(mt_job_f64w));
+    double **priv = (double **) calloc(nthreads, sizeof(double *));
+    for (int i = 0; i < nthreads; i++) {
+        priv[i] = (double *) calloc(map_size, sizeof(double));
+        jobs[i] = (mt_job_f64w) {priv[i], tod, xp, nsamp, nsamp * i / nthreads, nsamp * (i + 1) / nthreads, lp,
+                                 partial, 0};
+        pthread_create(&th[i], NULL, tod2map_f64w_worker, &jobs[i]);
+    }
+    uint32_t err = 0;
+    for (int i = 0; i < nthreads; i++) {
+        pthread_join(th[i], NULL);
+        err |= jobs[i].err;
+    }
+    for (int i = 0; i < nthreads; i++) {
+        for (int64_t k = 0; k < map_size; k++)
+            lmap[k] += priv[i][k];
+        free(priv[i]);
+    }
+    free(priv);
+    free(th);
+    free(jobs);
+    return err;
+}
+
 typedef struct {
     float *out;
     const float *lmap;

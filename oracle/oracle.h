@@ -61,6 +61,11 @@ uint32_t oracle_tod2map_f32(float *lmap, const float *tod, const float *xpointin
 uint32_t oracle_tod2map_f64(double *lmap, const double *tod, const double *xpointing, int64_t nsamp,
                             const oracle_lpix *lp, int32_t partial_pixelization);
 
+/* reference_tod2map<double> on float32 TOD/xpointing widened to double, nthreads threads with
+ * private double maps summed at the end (FP64 oracle of the tod2map precision variants). */
+uint32_t oracle_tod2map_f64w_mt(double *lmap, const float *tod, const float *xpointing, int64_t nsamp, int64_t map_size,
+                                const oracle_lpix *lpix, int32_t partial_pixelization, int32_t nthreads);
+
 /* Response variants (map2tod_response.cu:168-186, tod2map_response.cu:108-130): per-detector
  * (t_resp, p_resp) = (response[det], response[det+ndet]) with det = s / nperdet. */
 uint32_t oracle_response_map2tod_f32(float *tod, const float *lmap, const float *xpointing,
