@@ -24,9 +24,12 @@ from .gpu_mm import (map2tod, tod2map, LocalPixelization, LocalMap, DynamicMap, 
                      PointingPlan, read_xpointing_npzfile, mm_dtype, tod2map_compensated, fold_compensation,
                      tod2map_f64)
 
+from .batch import TodBatch  # noqa: E402,F401
+from . import autotune  # noqa: E402,F401
+
 __all__ = ["map2tod", "tod2map", "LocalPixelization", "LocalMap", "DynamicMap", "PointingPrePlan",
            "PointingPlan", "read_xpointing_npzfile", "mm_dtype", "gpu_mm_pybind11", "tod2map_compensated",
-           "fold_compensation", "tod2map_f64"]
+           "fold_compensation", "tod2map_f64", "TodBatch", "autotune"]
 
 
 def library_path():

@@ -171,7 +171,6 @@ __device__ __forceinline__ void global_add(const OpArgs &a, int64_t off, float v
 template<int FLUSH = kFlushF32>
 __device__ void flush_tile(float *tile, const int64_t *tab, const OpArgs &a, float *__restrict__ lmap)
 {
-#pragma unroll(FLUSH == kFlushF32 ? 1 : 4)
     for (int idx = threadIdx.x; idx < TY * TX; idx += NT) {
         const int r = idx / TX, c = idx % TX;
         float *src = tile + r * TS + c;
@@ -219,6 +218,27 @@ __device__ __forceinline__ bool tile_position(const Located &L, const Tile &T, c
     return ((unsigned) ry <= (unsigned) (TY - 2)) && ((unsigned) rx <= (unsigned) (TX - 2));
 }
 
+// The map2tod arithmetic of one sample, written with explicit round-to-nearest operations so that
+// the compiler cannot contract it differently in different kernels: every path (fast or general,
+// single TOD or batch, any grid) then gives the same bits for the same sample.
+//   pol_eval: ct*T + cq*Q + cu*U (ct = 1 without a response, so T enters unscaled);
+//   bilinear: (1-dy)(1-dx) e00 + (1-dy) dx e01 + dy (1-dx) e10 + dy dx e11, in that order.
+template<bool RESP>
+__device__ __forceinline__ float pol_eval(float ct, float cq, float cu, float t, float q, float u)
+{
+    return __fmaf_rn(cu, u, __fmaf_rn(cq, q, RESP ? __fmul_rn(ct, t) : t));
+}
+
+__device__ __forceinline__ float bilinear(float dy, float dx, float e00, float e01, float e10, float e11)
+{
+    const float wy0 = __fsub_rn(1.0f, dy), wx0 = __fsub_rn(1.0f, dx);
+    float r = __fmul_rn(__fmul_rn(wy0, wx0), e00);
+    r = __fmaf_rn(__fmul_rn(wy0, dx), e01, r);
+    r = __fmaf_rn(__fmul_rn(dy, wx0), e10, r);
+    return __fmaf_rn(__fmul_rn(dy, dx), e11, r);
+}
+
+template<bool RESP = false>
 __device__ __forceinline__ float global_eval(const OpArgs &a, const float *__restrict__ lmap, int iy, int ix,
                                              float ct, float cq, float cu, uint32_t &err)
 {
@@ -228,7 +248,7 @@ __device__ __forceinline__ float global_eval(const OpArgs &a, const float *__res
     const float q = valid ? __ldg(lmap + off + a.polstride) : 0.0f;
     const float u = valid ? __ldg(lmap + off + 2 * a.polstride) : 0.0f;
     err |= (valid || a.partial) ? 0u : kErrNotInPixelization;
-    return ct * t + cq * q + cu * u;
+    return pol_eval<RESP>(ct, cq, cu, t, q, u);
 }
 
 template<int FLUSH = kFlushF32>
@@ -257,24 +277,11 @@ template<bool RESP>
 __device__ __forceinline__ float tile_eval(const float *tile, int p, float ct, float cq, float cu, float dy, float dx)
 {
     const float *q = tile + p;
-    float e00, e01, e10, e11;
-    if constexpr (RESP) {
-        e00 = ct * q[0] + cq * q[PS] + cu * q[2 * PS];
-        e01 = ct * q[1] + cq * q[PS + 1] + cu * q[2 * PS + 1];
-        e10 = ct * q[TS] + cq * q[PS + TS] + cu * q[2 * PS + TS];
-        e11 = ct * q[TS + 1] + cq * q[PS + TS + 1] + cu * q[2 * PS + TS + 1];
-    } else {
-        e00 = q[0] + cq * q[PS] + cu * q[2 * PS];
-        e01 = q[1] + cq * q[PS + 1] + cu * q[2 * PS + 1];
-        e10 = q[TS] + cq * q[PS + TS] + cu * q[2 * PS + TS];
-        e11 = q[TS + 1] + cq * q[PS + TS + 1] + cu * q[2 * PS + TS + 1];
-    }
-    const float wy0 = 1.0f - dy, wx0 = 1.0f - dx;
-    float r = (wy0 * wx0) * e00;
-    r += (wy0 * dx) * e01;
-    r += (dy * wx0) * e10;
-    r += (dy * dx) * e11;
-    return r;
+    const float e00 = pol_eval<RESP>(ct, cq, cu, q[0], q[PS], q[2 * PS]);
+    const float e01 = pol_eval<RESP>(ct, cq, cu, q[1], q[PS + 1], q[2 * PS + 1]);
+    const float e10 = pol_eval<RESP>(ct, cq, cu, q[TS], q[PS + TS], q[2 * PS + TS]);
+    const float e11 = pol_eval<RESP>(ct, cq, cu, q[TS + 1], q[PS + TS + 1], q[2 * PS + TS + 1]);
+    return bilinear(dy, dx, e00, e01, e10, e11);
 }
 
 // Response factors of a sample as (ct, cq, cu) = (t_resp, p_resp cos 2a, p_resp sin 2a), or
@@ -311,16 +318,11 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
         return tile_eval<RESP>(tile, ry * TS + rx, ct, cq, cu, L.dy, L.dx);
     // Absent cells are already reported through the plan's cell bitmap.
     uint32_t unused = 0;
-    const float e00 = global_eval(a, a.in, L.iy0, L.ix0, ct, cq, cu, unused);
-    const float e01 = global_eval(a, a.in, L.iy0, L.ix1, ct, cq, cu, unused);
-    const float e10 = global_eval(a, a.in, L.iy1, L.ix0, ct, cq, cu, unused);
-    const float e11 = global_eval(a, a.in, L.iy1, L.ix1, ct, cq, cu, unused);
-    const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
-    float r = (wy0 * wx0) * e00;
-    r += (wy0 * L.dx) * e01;
-    r += (L.dy * wx0) * e10;
-    r += (L.dy * L.dx) * e11;
-    return r;
+    const float e00 = global_eval<RESP>(a, a.in, L.iy0, L.ix0, ct, cq, cu, unused);
+    const float e01 = global_eval<RESP>(a, a.in, L.iy0, L.ix1, ct, cq, cu, unused);
+    const float e10 = global_eval<RESP>(a, a.in, L.iy1, L.ix0, ct, cq, cu, unused);
+    const float e11 = global_eval<RESP>(a, a.in, L.iy1, L.ix1, ct, cq, cu, unused);
+    return bilinear(L.dy, L.dx, e00, e01, e10, e11);
 }
 
 // One sample of tod2map: exact locate with error bits, then 12 shared-memory atomics into the staged
@@ -766,10 +768,11 @@ unplanned_kernel(OpArgs a)
                 global_accum(a, a.out, L.iy1, L.ix0, t, q, u, L.dy * wx0, err);
                 global_accum(a, a.out, L.iy1, L.ix1, t, q, u, L.dy * L.dx, err);
             } else {
-                float rr = (wy0 * wx0) * global_eval(a, a.in, L.iy0, L.ix0, 1.0f, cs, sn, err);
-                rr += (wy0 * L.dx) * global_eval(a, a.in, L.iy0, L.ix1, 1.0f, cs, sn, err);
-                rr += (L.dy * wx0) * global_eval(a, a.in, L.iy1, L.ix0, 1.0f, cs, sn, err);
-                rr += (L.dy * L.dx) * global_eval(a, a.in, L.iy1, L.ix1, 1.0f, cs, sn, err);
+                const float e00 = global_eval(a, a.in, L.iy0, L.ix0, 1.0f, cs, sn, err);
+                const float e01 = global_eval(a, a.in, L.iy0, L.ix1, 1.0f, cs, sn, err);
+                const float e10 = global_eval(a, a.in, L.iy1, L.ix0, 1.0f, cs, sn, err);
+                const float e11 = global_eval(a, a.in, L.iy1, L.ix1, 1.0f, cs, sn, err);
+                const float rr = bilinear(L.dy, L.dx, e00, e01, e10, e11);
                 r[k] = a.accum ? (tv[k] + rr) : rr;
             }
         }

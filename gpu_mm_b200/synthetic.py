@@ -94,3 +94,48 @@ def cells_of_plan(plan_mt):
     else:
         c = np.unique(np.asarray(plan_mt).astype(np.uint64) & np.uint64((1 << 20) - 1)).astype(np.int64)
     return [(int(v) >> 10, int(v) & 1023) for v in c]
+
+
+def rotated_raster(ndet_side, nt, spacing, speed, theta, x0, y0, xspan, yspan, yspeed, nxpix, alpha_period=4096.0,
+                   device="cpu"):
+    """xpointing (3, ndet_side^2, nt) float32 of a detector grid rotated by 'theta' about its first
+    detector: x bounces over [x0, x0+xspan] at 'speed' px/sample, y over [y0, y0+yspan] at 'yspeed'."""
+    ndet = ndet_side * ndet_side
+    t = torch.arange(nt, dtype=torch.float64, device=device)
+    xs = x0 + triangle(speed * t, float(xspan))
+    ys = y0 + triangle(yspeed * t, float(yspan))
+    i = torch.arange(ndet_side, dtype=torch.float64, device=device).repeat_interleave(ndet_side)
+    j = torch.arange(ndet_side, dtype=torch.float64, device=device).repeat(ndet_side)
+    c, s = math.cos(theta), math.sin(theta)
+    oy = spacing * (c * i - s * j)
+    ox = spacing * (s * i + c * j)
+    out = torch.empty((3, ndet, nt), dtype=torch.float32, device=device)
+    out[0] = (ys[None, :] + oy[:, None]).to(torch.float32)
+    out[1] = (xs[None, :] + ox[:, None]).to(torch.float32)
+    d = torch.arange(ndet, dtype=torch.float64, device=device)[:, None]
+    out[2] = (2.0 * math.pi * torch.remainder(t[None, :] / alpha_period + d / float(ndet), 1.0)).to(torch.float32)
+    return out
+
+
+def config4_tods(device="cuda", ntod=64, seed=1000, median=2 ** 20, sigma=1.0, ny=4096, nx=8192, ndet_side=4):
+    """The batched workload: 'ntod' TODs whose nsamp is lognormal (median 2^20, sigma 1.0), clipped to
+    [2^16, 2^24] and rounded to a multiple of 32 * ndet; TOD i is seeded with seed + i: random start
+    pixel, sweep speed U(0.3, 1.0) px/sample, random detector-grid rotation, inside an ny x nx map.
+    Returns a list of xpointing tensors of shape (3, nsamp)."""
+    out = []
+    quantum = 32 * ndet_side * ndet_side
+    for i in range(ntod):
+        rng = np.random.default_rng(seed + i)
+        nsamp = int(np.clip(np.exp(np.log(median) + sigma * rng.standard_normal()), 2 ** 16, 2 ** 24))
+        nsamp = max(quantum, (nsamp // quantum) * quantum)
+        nt = nsamp // (ndet_side * ndet_side)
+        speed = rng.uniform(0.3, 1.0)
+        theta = rng.uniform(0.0, 2.0 * math.pi)
+        margin = 4.0 + 2.0 * ndet_side * 1.5
+        xspan = rng.uniform(256.0, 2048.0)
+        yspan = rng.uniform(16.0, 128.0)
+        x0 = rng.uniform(margin, nx - margin - xspan - 1.0)
+        y0 = rng.uniform(margin, ny - margin - yspan - 1.0)
+        xp = rotated_raster(ndet_side, nt, 1.5, speed, theta, x0, y0, xspan, yspan, speed * 0.01, nx, device=device)
+        out.append(xp.reshape(3, nsamp).contiguous())
+    return out

@@ -255,7 +255,8 @@ def test_config1_full_size(g):
 def test_aligned_and_unaligned_arrays(g):
     """The planned operators have a 16-byte-load kernel (xpointing and TOD 16-byte aligned) and a
     one-sample-per-lane kernel for other alignments.  Both must match the oracle, and map2tod must
-    give the same bits through either (each sample is computed by the same code)."""
+    give the same bits through either, and through the unplanned operator (each sample is evaluated
+    with the same explicitly rounded operations)."""
     import torch
     rng = np.random.default_rng(77)
     ny, nx, periodic = 512, 1024, True
@@ -292,6 +293,11 @@ def test_aligned_and_unaligned_arrays(g):
         rl1, mx = rel_stats(host(out.arr), want_map)
         assert rl1 < RL1_TOL and mx < MAX_TOL, (off, rl1, mx)
     np.testing.assert_array_equal(tods[0], tods[1])
+    # The unplanned operator evaluates each sample with the same rounded operations.
+    xg = offset_copy(xp, 0)
+    tod = offset_copy(np.zeros((ndet, nt), np.float32), 0)
+    g.map2tod(tod, lmap, xg, None)
+    np.testing.assert_array_equal(host(tod), tods[0])
 
 
 @pytest.mark.parametrize("periodic", [True, False])
