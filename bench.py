@@ -20,6 +20,9 @@ Other numbers on the JSON line:
   cpu_baseline the reference's CPU operators (oracle/_ref: the reference header; else the oracle
                port) on all host cores over a bounded prefix of the same workload
   clocks       NVML SM clock samples during the timed region
+  batched      64 uneven TODs (lognormal nsamp) into one map: plain per-TOD calls against one
+               autotuned TodBatch replayed as CUDA graphs; speed-up, bitwise map2tod equality and
+               tod2map error against the FP64 oracle
   precision    tod2map precision variants (float atomics, compensated float flush, float64 map) on
                the high-hit workload (2^28 samples in a 512x512 box, tod = 1e3 + N(0,1)): throughput
                and max/rms relative error against the FP64 oracle on the host cores
@@ -53,6 +56,7 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-precision", action="store_true", help="skip the tod2map precision study")
+    p.add_argument("--no-batch", action="store_true", help="skip the batched-TOD study")
     p.add_argument("--only", default="", help="profiling aid: 'map2tod' or 'tod2map' runs only that operator")
     return p.parse_args()
 
@@ -280,6 +284,98 @@ def precision_study(max_run_lines=1024):
     }
 
 
+def batch_study(reps=3):
+    """64 TODs of lognormal nsamp (median 2^20, sigma 1.0, clipped to [2^16, 2^24]), each its own
+    rotated raster, into one 3x4096x8192 map: plan build + map2tod + tod2map of every TOD, (a) as
+    plain per-TOD calls (PointingPrePlan, PointingPlan, map2tod per TOD, then tod2map per TOD) and
+    (b) as a TodBatch, autotuned, as two CUDA-graph replays (plan build + map2tod; tod2map).  Both
+    timed with CUDA events; throughput = samples of the batch / time of the whole stage pair."""
+    import numpy as np
+    import torch
+    import oracle
+    import gpu_mm_b200 as g
+    from gpu_mm_b200 import synthetic
+    ny, nx = 4096, 8192
+    xps = synthetic.config4_tods(device="cuda")
+    nsamps = [x.shape[1] for x in xps]
+    total = int(sum(nsamps))
+    lp = g.LocalPixelization.make_rectangle(ny, nx, False)
+    gen = torch.Generator(device="cuda").manual_seed(44)
+    lmap = g.LocalMap(lp, torch.randn(3 * lp.npix, generator=gen, device="cuda"))
+    tods_in = [torch.randn(n, generator=gen, device="cuda") for n in nsamps]
+    out_plain = [torch.zeros(n, device="cuda") for n in nsamps]
+    out_batch = [torch.zeros(n, device="cuda") for n in nsamps]
+    map_plain = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+    map_batch = torch.zeros(3 * lp.npix, device="cuda")
+
+    def plain():
+        plans = []
+        for xp, to in zip(xps, out_plain):
+            pl = g.PointingPlan(g.PointingPrePlan(xp, ny, nx, periodic_xcoord=False), xp)
+            plans.append(pl)
+            g.map2tod(to, lmap, xp, pl)
+        for xp, ti, pl in zip(xps, tods_in, plans):
+            g.tod2map(map_plain, ti, xp, pl)
+
+    b_out = g.TodBatch(xps, out_batch, lp)
+    scratch = torch.zeros(3 * lp.npix, device="cuda")
+    best, cand_ms = g.autotune.autotune(b_out, lmap, scratch)
+    b_in = b_out.with_tods(tods_in)
+    graph1 = b_out.capture(lambda st: (b_out.build_plan(st), b_out.map2tod(lmap, stream=st)))
+    graph2 = b_in.capture(lambda st: b_in.tod2map(map_batch, stream=st))
+
+    def batched():
+        graph1.replay()
+        graph2.replay()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    plain_ms = timed(plain)
+    batch_ms = timed(batched)
+    b_out.check()
+    b_in.check()
+    map2tod_equal = all(torch.equal(a, b) for a, b in zip(out_plain, out_batch))
+    # One clean tod2map of each path against the FP64 oracle.
+    map_plain.arr.zero_()
+    plain()
+    map_batch.zero_()
+    batched()
+    torch.cuda.synchronize()
+    want = np.zeros(3 * lp.npix, np.float64)
+    lp_o = oracle.Lpix.rectangle(ny, nx, False)
+    nthreads = os.cpu_count() or 1
+    for xp, t in zip(xps, tods_in):
+        assert oracle.tod2map_f64w_mt(want, t.cpu().numpy(), xp.cpu().numpy(), lp_o, nthreads) == 0
+
+    def errs(a):
+        d = a.cpu().numpy().astype(np.float64) - want
+        return float(f"{np.abs(d).max() / np.abs(want).max():.3e}"), float(f"{np.sqrt((d * d).sum() / (want * want).sum()):.3e}")
+
+    pe, be = errs(map_plain.arr), errs(map_batch)
+    return {
+        "workload": f"64 TODs, nsamp lognormal (median 2^20, sigma 1.0, clipped [2^16, 2^24]), total {total} samples, "
+                    "rotated rasters, 3x4096x8192 map",
+        "stage": "plan build + map2tod + tod2map of every TOD",
+        "plain_ms": round(plain_ms, 3), "batched_ms": round(batch_ms, 3),
+        "plain_gsamples_s": round(total / (plain_ms * 1e-3) / 1e9, 3),
+        "batched_gsamples_s": round(total / (batch_ms * 1e-3) / 1e9, 3),
+        "speedup": round(plain_ms / batch_ms, 3),
+        "map2tod_bitwise_equal": bool(map2tod_equal),
+        "tod2map_vs_fp64": {"plain": {"max_rel_err": pe[0], "rms_rel_err": pe[1]},
+                            "batched": {"max_rel_err": be[0], "rms_rel_err": be[1]}},
+        "autotune": {"best": list(best), "candidates_ms": cand_ms},
+    }
+
+
 # ------------------------------------------------------------------------------------------------
 
 
@@ -476,6 +572,9 @@ def main():
     precision = None
     if rank == 0 and world == 1 and not args.no_precision:
         precision = precision_study()
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batched = batch_study()
 
     if rank == 0:
         value = world * nsamp / (ms_step * 1e-3) / 1e9
@@ -495,6 +594,7 @@ def main():
                            "first_plan_build_s": round(first_plan_s, 3)},
             "plan": {"nmt": int(pp.plan_nmt), "overhead": round(pp.overhead, 4), "sort_digit_bits": pp.sort_digit_bits},
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "precision": precision,
+            "batched": batched,
             "gpu_launches": args.steps * (int(do_m2t) + int(do_t2m)),
         }
         print(json.dumps(line), flush=True)

@@ -581,8 +581,24 @@ __device__ __forceinline__ int batch_tod_of_line(const gmm_tod_desc *__restrict_
     return lo;
 }
 
-// One warp per cache line (lane = sample), grid-stride over the batch's lines.  The owner cell is
-// the lowest cell among the four neighbours of the line's samples (the cells of a line are those of
+// Marks 'cell' in the cell bitmap unless it is in this warp's cache of recently marked cells (one
+// entry per lane 0..7, round robin); 'cell' is warp-uniform.
+__device__ __forceinline__ void mark_cell(uint32_t cell, uint32_t *cellmap, uint32_t &cache, int &next)
+{
+    const int lane = threadIdx.x & 31;
+    if (__ballot_sync(kFullMask, (lane < 8) && (cache == cell)) != 0u)
+        return;
+    if (lane == 0)
+        atomicOr(cellmap + (cell >> 5), 1u << (cell & 31));
+    if (lane == next)
+        cache = cell;
+    next = (next + 1) & 7;
+}
+
+// One warp per cache line (lane = sample).  Each CTA takes a contiguous range of the batch's lines
+// and its warps interleave over it, so a warp sees nearby pointing and its cache of marked cells
+// keeps the bitmap atomics to about one per cell and warp.  The owner cell is the lowest cell
+// among the four neighbours of the line's samples (the cells of a line are those of
 // cell_enumerator, gpu_mm_internals.hpp:179-237); every cell the line touches is marked in the
 // cell bitmap.  Word = cell | line << 20 | mflag << 46 | tod << 48, at the line's global index.
 __global__ void __launch_bounds__(256)
@@ -591,10 +607,13 @@ batch_owner_kernel(const gmm_tod_desc *__restrict__ descs, int ntod, int64_t tot
                    uint32_t *__restrict__ errword)
 {
     __shared__ uint32_t s_err[8];
-    const int lane = threadIdx.x & 31;
-    const int64_t nwarps = (int64_t) gridDim.x * (blockDim.x >> 5);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int64_t l0 = (total_lines * (int64_t) blockIdx.x) / gridDim.x;
+    const int64_t l1 = (total_lines * (int64_t) (blockIdx.x + 1)) / gridDim.x;
     uint32_t err = 0;
-    for (int64_t gl = (int64_t) blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); gl < total_lines; gl += nwarps) {
+    uint32_t cache = 0xffffffffu;   // no cell id is all ones
+    int next = 0;
+    for (int64_t gl = l0 + warp; gl < l1; gl += nw) {
         const int tod = batch_tod_of_line(descs, ntod, gl);
         const float *xp = (const float *) __ldg((const unsigned long long *) &descs[tod].xpointing);
         const int64_t nsamp = __ldg(&descs[tod].nsamp);
@@ -610,35 +629,39 @@ batch_owner_kernel(const gmm_tod_desc *__restrict__ descs, int ntod, int64_t tot
         const int64_t s = 32 * line + lane;
         Located L;
         err |= locate(__ldcs(xp + s), __ldcs(xp + nsamp + s), ny, nx, periodic, L);
-        const uint32_t c00 = ((uint32_t) (L.iy0 >> 6) << 10) | (uint32_t) (L.ix0 >> 6);
-        const uint32_t c01 = ((uint32_t) (L.iy0 >> 6) << 10) | (uint32_t) (L.ix1 >> 6);
-        const uint32_t c10 = ((uint32_t) (L.iy1 >> 6) << 10) | (uint32_t) (L.ix0 >> 6);
-        const uint32_t c11 = ((uint32_t) (L.iy1 >> 6) << 10) | (uint32_t) (L.ix1 >> 6);
-        const uint32_t lo = min(min(c00, c01), min(c10, c11));
-        const uint32_t hi = max(max(c00, c01), max(c10, c11));
+        const uint32_t c[4] = {((uint32_t) (L.iy0 >> 6) << 10) | (uint32_t) (L.ix0 >> 6),
+                               ((uint32_t) (L.iy0 >> 6) << 10) | (uint32_t) (L.ix1 >> 6),
+                               ((uint32_t) (L.iy1 >> 6) << 10) | (uint32_t) (L.ix0 >> 6),
+                               ((uint32_t) (L.iy1 >> 6) << 10) | (uint32_t) (L.ix1 >> 6)};
+        const uint32_t lo = min(min(c[0], c[1]), min(c[2], c[3]));
+        const uint32_t hi = max(max(c[0], c[1]), max(c[2], c[3]));
         const uint32_t owner = __reduce_min_sync(kFullMask, lo);
         const bool multi = __any_sync(kFullMask, hi != owner);
-        if (lane == 0) {
+        if (lane == 0)
             owner_out[gl] = (uint64_t) owner | ((uint64_t) line << 20) | ((uint64_t) multi << 46) |
                             ((uint64_t) tod << kBatchTodShift);
-            atomicOr(cellmap + (owner >> 5), 1u << (owner & 31));
-        }
+        mark_cell(owner, cellmap, cache, next);
         if (multi) {
-            // Cells other than the owner: each lane marks its own (duplicates are harmless).
-            const uint32_t cs[4] = {c00, c01, c10, c11};
+            // The line's other cells: one representative lane per distinct value of each corner.
 #pragma unroll
-            for (int k = 0; k < 4; k++)
-                if (cs[k] != owner)
-                    atomicOr(cellmap + (cs[k] >> 5), 1u << (cs[k] & 31));
+            for (int k = 0; k < 4; k++) {
+                const unsigned peers = __match_any_sync(kFullMask, c[k]);
+                unsigned lead = __ballot_sync(kFullMask, ((peers & ((1u << lane) - 1u)) == 0u) && (c[k] != owner));
+                while (lead) {
+                    const int src = __ffs(lead) - 1;
+                    lead &= lead - 1;
+                    mark_cell(__shfl_sync(kFullMask, c[k], src), cellmap, cache, next);
+                }
+            }
         }
     }
     err = __reduce_or_sync(kFullMask, err);
     if (lane == 0)
-        s_err[threadIdx.x >> 5] = err;
+        s_err[warp] = err;
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t e = 0;
-        for (int w = 0; w < (int) (blockDim.x >> 5); w++)
+        for (int w = 0; w < nw; w++)
             e |= s_err[w];
         if (e)
             atomicOr(errword, e);
@@ -650,7 +673,8 @@ cudaError_t launch_batch_owner(const gmm_tod_desc *descs, int ntod, int64_t tota
 {
     if (total_lines <= 0)
         return cudaSuccess;
-    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((total_lines + 7) / 8, 16 * (int64_t) device_sm_count()));
+    // Contiguous ranges of >= 256 lines per CTA (8 warps).
+    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((total_lines + 255) / 256, 8 * (int64_t) device_sm_count()));
     batch_owner_kernel<<<(unsigned) g, 256, 0, stream>>>(descs, ntod, total_lines, ny, nx, periodic, owner_out, cellmap,
                                                          errword);
     return cudaGetLastError();
