@@ -93,6 +93,30 @@ class TodBatch:
         b._set_tods(tods)
         return b
 
+    def merge_plans(self, singles, stream=None):
+        """Builds this batch's plan from built single-TOD batches (TodBatch of one TOD each, in this
+        batch's TOD order) instead of from the pointing: their owner lists are concatenated with the
+        TOD index set, the cell bitmaps OR-ed and the list sorted by cell.  The result is the plan
+        build_plan() gives."""
+        if len(singles) != self.ntod or any(s.ntod != 1 or s.total_lines != n // 32
+                                            for s, n in zip(singles, self.nsamps)):
+            raise RuntimeError("TodBatch.merge_plans: need one single-TOD batch per TOD, with matching sizes")
+        host = torch.tensor([[s.plan.data_ptr() for s in singles], [s.total_lines for s in singles]],
+                            dtype=torch.int64).pin_memory()
+        if isinstance(stream, torch.cuda.Stream) or stream is None:
+            # Copy on the stream that runs the merge, so it is ordered before it.
+            with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+                self._merge_args = host.cuda(non_blocking=True)
+        else:
+            self._merge_args = host.cuda()
+            torch.cuda.current_stream().synchronize()
+        self._merge_host = host            # kept alive until the next merge (the copy is asynchronous)
+        self._merge_refs = list(singles)
+        _m.batch_plan_merge(self._merge_args[0].data_ptr(), self._merge_args[1].data_ptr(), self.ntod,
+                            self.total_lines, self.lpix.nypix_global, self.lpix.nxpix_global, self.plan.data_ptr(),
+                            self.plan.numel(), self.tmp.data_ptr(), self.tmp.numel(), self.tuning,
+                            _stream_handle(stream))
+
     def set_tuning(self, tuning):
         """Launch/sort parameters (sort_digit_bits, ctas_per_sm, min_lines_per_cta); the plan must be
         rebuilt afterwards."""

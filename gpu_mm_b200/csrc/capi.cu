@@ -610,6 +610,39 @@ int gmm_batch_plan_build(const gmm_tod_desc *descs, int32_t ntod, int64_t total_
     return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
 }
 
+int gmm_batch_plan_merge(const void *const *plans, const int64_t *nlines, int32_t ntod, int64_t total_lines,
+                         int32_t ny, int32_t nx, void *plan_buf, int64_t plan_nbytes, void *tmp, int64_t tmp_nbytes,
+                         const gmm_batch_tuning *tuning, cudaStream_t stream)
+{
+    const char *where = "batch_plan_merge";
+    if (int rc = check_ptr(plans, where, "plans")) return rc;
+    if (int rc = check_ptr(nlines, where, "nlines")) return rc;
+    if ((ntod < 1) || (ntod > 65535) || (total_lines < ntod))
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": need 1 <= ntod <= 65535 and total_lines >= ntod");
+    if (int rc = check_npix(ny, nx, where)) return rc;
+    if (int rc = check_tuning(tuning, where)) return rc;
+    if (int rc = check_ptr(plan_buf, where, "plan_buf")) return rc;
+    if (int rc = check_ptr(tmp, where, "tmp")) return rc;
+    if ((((uintptr_t) plan_buf) | ((uintptr_t) tmp)) & 127)
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": 'plan_buf' and 'tmp' must be 128-byte aligned");
+    int64_t oo, co, need_plan, ho, need_tmp;
+    int dbits, passes;
+    batch_layout(total_lines, ny, nx, tuning, &oo, &co, &need_plan, &ho, &need_tmp, &dbits, &passes);
+    if ((plan_nbytes < need_plan) || (tmp_nbytes < need_tmp))
+        return fail(GMM_ERR_BUFFER_TOO_SMALL, std::string(where) + ": buffers too small");
+    char *b = (char *) plan_buf, *t = (char *) tmp;
+    uint64_t *owner = (uint64_t *) (b + oo), *alt = (uint64_t *) t;
+    uint32_t *cellmap = (uint32_t *) (b + co), *hist = (uint32_t *) (t + ho);
+    const bool even = (passes % 2) == 0;
+    const int nyc = (ny + 63) / 64, nxc = (nx + 63) / 64;
+    cudaError_t e = cudaMemsetAsync(cellmap, 0, kCellmapBytes, stream);
+    if (e == cudaSuccess)
+        e = launch_batch_merge(plans, nlines, ntod, total_lines, even ? owner : alt, cellmap, stream);
+    if (e == cudaSuccess)
+        e = radix_sort_mt(even ? owner : alt, even ? alt : owner, total_lines, nyc, nxc, dbits, passes, hist, stream);
+    return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
+}
+
 static int batch_op(bool tod2map, const gmm_tod_desc *descs, int32_t ntod, int64_t total_lines, float *lmap_out,
                     const float *lmap_in, const gmm_lpix *lp, const void *plan_buf, int32_t partial, int32_t accum,
                     const gmm_batch_tuning *tuning, uint32_t *errword, cudaStream_t stream, const char *where)

@@ -99,6 +99,8 @@ cudaError_t launch_fold_compensation(float *lmap, float *comp, int64_t n, cudaSt
 constexpr int kBatchTodShift = 48;
 cudaError_t launch_batch_owner(const gmm_tod_desc *descs, int ntod, int64_t total_lines, int ny, int nx, bool periodic,
                                uint64_t *owner_out, uint32_t *cellmap, uint32_t *errword, cudaStream_t stream);
+cudaError_t launch_batch_merge(const void *const *plans, const int64_t *nlines, int ntod, int64_t total_lines,
+                               uint64_t *owner_out, uint32_t *cellmap, cudaStream_t stream);
 cudaError_t launch_batch_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                  cudaStream_t stream);
 cudaError_t launch_batch_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,

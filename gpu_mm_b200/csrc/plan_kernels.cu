@@ -668,6 +668,46 @@ batch_owner_kernel(const gmm_tod_desc *__restrict__ descs, int ntod, int64_t tot
     }
 }
 
+// Merge of single-TOD batch plans: CTA b of the grid copies TOD (b % ntod)'s owner words with the
+// TOD index set, grid-striding over that TOD; destination offsets are the prefix sums of nlines.
+__global__ void __launch_bounds__(256)
+batch_merge_kernel(const void *const *__restrict__ plans, const int64_t *__restrict__ nlines, int ntod,
+                   uint64_t *__restrict__ owner_out, uint32_t *__restrict__ cellmap)
+{
+    __shared__ int64_t s_off;
+    const int tod = blockIdx.x % ntod;
+    const int part = blockIdx.x / ntod, nparts = gridDim.x / ntod;
+    if (threadIdx.x == 0) {
+        int64_t off = 0;
+        for (int i = 0; i < tod; i++)
+            off += nlines[i];
+        s_off = off;
+    }
+    __syncthreads();
+    const int64_t n = nlines[tod];
+    const uint64_t *src = (const uint64_t *) plans[tod];
+    const uint64_t tag = (uint64_t) tod << kBatchTodShift;
+    for (int64_t k = part * (int64_t) blockDim.x + threadIdx.x; k < n; k += (int64_t) nparts * blockDim.x)
+        owner_out[s_off + k] = (src[k] & ((1ull << kBatchTodShift) - 1)) | tag;
+    // A single-TOD plan holds its n owner words, then (128-byte aligned) its cell bitmap.
+    const uint32_t *cm = (const uint32_t *) ((const char *) plans[tod] + ((8 * n + 127) & ~127ll));
+    for (int w = part * blockDim.x + threadIdx.x; w < (1 << 15); w += nparts * blockDim.x) {
+        const uint32_t bits = cm[w];
+        if (bits)
+            atomicOr(cellmap + w, bits);
+    }
+}
+
+cudaError_t launch_batch_merge(const void *const *plans, const int64_t *nlines, int ntod, int64_t total_lines,
+                               uint64_t *owner_out, uint32_t *cellmap, cudaStream_t stream)
+{
+    if (ntod <= 0)
+        return cudaSuccess;
+    const int64_t per_tod = std::max<int64_t>(1, std::min<int64_t>(64, (total_lines / ntod + 4095) / 4096));
+    batch_merge_kernel<<<(unsigned) (per_tod * ntod), 256, 0, stream>>>(plans, nlines, ntod, owner_out, cellmap);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_batch_owner(const gmm_tod_desc *descs, int ntod, int64_t total_lines, int ny, int nx, bool periodic,
                                uint64_t *owner_out, uint32_t *cellmap, uint32_t *errword, cudaStream_t stream)
 {

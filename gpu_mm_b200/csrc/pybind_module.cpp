@@ -141,6 +141,18 @@ PYBIND11_MODULE(gpu_mm_pybind11, m)
           py::arg("descs"), py::arg("ntod"), py::arg("total_lines"), py::arg("nypix_global"), py::arg("nxpix_global"),
           py::arg("periodic_xcoord"), py::arg("plan"), py::arg("plan_nbytes"), py::arg("tmp"), py::arg("tmp_nbytes"),
           py::arg("tuning"), py::arg("errword"), py::arg("stream") = 0);
+    m.def("batch_plan_merge",
+          [tuning_of](uintptr_t plans, uintptr_t nlines, int ntod, long total_lines, int ny, int nx, uintptr_t plan,
+                      long plan_nbytes, uintptr_t tmp, long tmp_nbytes, py::object tuning, uintptr_t stream) {
+              gmm_batch_tuning bt = tuning_of(tuning);
+              py::gil_scoped_release rel;
+              throw_on_error(gmm_batch_plan_merge((const void *const *) plans, (const int64_t *) nlines, ntod,
+                                                  total_lines, ny, nx, (void *) plan, plan_nbytes, (void *) tmp,
+                                                  tmp_nbytes, &bt, (cudaStream_t) stream));
+          },
+          py::arg("plans"), py::arg("nlines"), py::arg("ntod"), py::arg("total_lines"), py::arg("nypix_global"),
+          py::arg("nxpix_global"), py::arg("plan"), py::arg("plan_nbytes"), py::arg("tmp"), py::arg("tmp_nbytes"),
+          py::arg("tuning"), py::arg("stream") = 0);
     m.def("batch_map2tod",
           [tuning_of](uintptr_t descs, int ntod, long total_lines, py::object local_map, const LocalPixelization &lpix,
                       uintptr_t plan, bool partial_pixelization, bool accum, py::object tuning, uintptr_t errword,

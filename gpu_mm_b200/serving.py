@@ -1,0 +1,251 @@
+"""A serving loop for pointing operations with continuous batching (no counterpart in the reference).
+
+PointingServer keeps a pool of TODs' pointing, a resident input map (read by map2tod) and an output
+map (into which tod2map accumulates) on the device, and serves three kinds of requests:
+
+  * ('plan', tod_id):    build the TOD's plan and keep it in the device plan cache;
+  * ('map2tod', tod_id): the TOD's samples from the input map (a new device array per request);
+  * ('tod2map', tod_id, tod): accumulate a TOD array into the output map.
+
+A worker thread runs the loop.  Every iteration it
+
+  1. takes the newly submitted requests and admits them in arrival order while their device memory
+     (plans, output TODs, batch plans) fits the HBM budget, evicting least-recently-used plans that no
+     admitted request needs; requests that do not fit wait and are admitted as memory frees up;
+  2. launches the admitted work on one of several CUDA streams: plan builds (one single-TOD batch plan
+     each), then all admitted map2tod requests as one TodBatch whose plan is merged from the cached
+     single-TOD plans, then all admitted tod2map requests likewise -- so requests that arrive while
+     others are on the GPU join the next launch, and launches of successive iterations overlap;
+  3. completes the requests whose launches have finished (CUDA events) and releases their memory.
+
+Results do not depend on the mix: map2tod evaluates every sample with the same rounded operations as
+the single-TOD operator (bit-identical), and tod2map adds the same per-sample contributions into the
+output map (float atomics: the order, and so the last bits, differ).
+
+Latency of a request = completion time - submission time, on the host clock.
+"""
+
+import collections
+import concurrent.futures
+import threading
+import time
+
+import numpy as np
+import torch
+
+from .batch import TodBatch
+
+
+class PointingServer:
+    def __init__(self, xpointings, in_map, out_map, local_pixelization, hbm_budget_bytes, nstreams=3,
+                 max_batch=256, tuning=None):
+        self.xpointings = dict(xpointings)                # tod_id -> (3, nsamp) CUDA tensor
+        self.in_map, self.out_map = in_map, out_map
+        self.lpix = local_pixelization
+        self.budget = int(hbm_budget_bytes)
+        self.tuning = tuning
+        self.max_batch = max_batch
+        self.streams = [torch.cuda.Stream() for _ in range(nstreams)]
+        self._next_stream = 0
+        self._lock = threading.Lock()
+        self._submitted = collections.deque()
+        self._waiting = collections.deque()
+        self._inflight = []                                # (event, requests, bytes, keepalive)
+        self._plans = collections.OrderedDict()            # tod_id -> (single TodBatch, ready event, nbytes)
+        self._used = 0
+        self._stop = False
+        self.latencies = {"plan": [], "map2tod": [], "tod2map": []}
+        self.samples_done = 0
+        self.launches = 0
+        self.evictions = 0
+        self.errors = []
+        self._errwords = []
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+
+    # ---- client side ----
+
+    def submit(self, kind, tod_id, tod=None):
+        if kind not in ("plan", "map2tod", "tod2map"):
+            raise ValueError(f"unknown request kind {kind}")
+        if tod_id not in self.xpointings:
+            raise KeyError(f"unknown tod_id {tod_id}")
+        if kind == "tod2map" and tod is None:
+            raise ValueError("tod2map needs a TOD array")
+        fut = concurrent.futures.Future()
+        with self._lock:
+            self._submitted.append({"kind": kind, "id": tod_id, "tod": tod, "t0": time.perf_counter(), "fut": fut})
+        return fut
+
+    def drain(self, timeout=60.0):
+        """Waits until every submitted request has completed."""
+        t_end = time.perf_counter() + timeout
+        while time.perf_counter() < t_end:
+            with self._lock:
+                busy = bool(self._submitted or self._waiting or self._inflight)
+            if not busy:
+                return
+            time.sleep(0.0005)
+        raise TimeoutError("PointingServer.drain: requests still pending")
+
+    def close(self):
+        self._stop = True
+        self._thread.join()
+        torch.cuda.synchronize()
+
+    def stats(self):
+        out = {}
+        for k, v in self.latencies.items():
+            if v:
+                a = np.asarray(v) * 1e3
+                out[k] = {"n": len(v), "p50_ms": round(float(np.percentile(a, 50)), 3),
+                          "p99_ms": round(float(np.percentile(a, 99)), 3)}
+        allv = sum(self.latencies.values(), [])
+        if allv:
+            a = np.asarray(allv) * 1e3
+            out["all"] = {"n": len(allv), "p50_ms": round(float(np.percentile(a, 50)), 3),
+                          "p99_ms": round(float(np.percentile(a, 99)), 3)}
+        out["launches"] = self.launches
+        out["evictions"] = self.evictions
+        out["plan_cache"] = {"plans": len(self._plans), "bytes": self._used}
+        return out
+
+    # ---- memory accounting ----
+
+    def _plan_nbytes(self, tod_id):
+        n = self.xpointings[tod_id][0].numel()
+        return 16 * (n // 32) + (1 << 17) + (1 << 20)    # plan (owner list + cell bitmap) + sort scratch
+
+    def _request_nbytes(self, r):
+        n = self.xpointings[r["id"]][0].numel()
+        extra = 4 * n if r["kind"] == "map2tod" else 0
+        return extra + 16 * (n // 32) + (1 << 18)                      # output TOD + its share of the batch plan
+
+    def _evict(self, need, pinned):
+        for tid in list(self._plans.keys()):
+            if self._used + need <= self.budget:
+                return True
+            if tid in pinned:
+                continue
+            _, ev, nb = self._plans.pop(tid)
+            ev.synchronize()
+            self._used -= nb
+            self.evictions += 1
+        return self._used + need <= self.budget
+
+    # ---- worker ----
+
+    def _stream(self):
+        s = self.streams[self._next_stream]
+        self._next_stream = (self._next_stream + 1) % len(self.streams)
+        return s
+
+    def _ensure_plan(self, tod_id, stream, rebuild=False):
+        if tod_id in self._plans and not rebuild:
+            self._plans.move_to_end(tod_id)
+            return self._plans[tod_id]
+        xp = self.xpointings[tod_id]
+        # A plan needs no TOD array; the y row stands in for it (never read or written by a build).
+        single = TodBatch([xp], [xp[0]], self.lpix, tuning=self.tuning)
+        # Charged at the admission estimate, which bounds the plan and its sort scratch.
+        nb = max(self._plan_nbytes(tod_id), single.plan.numel() + single.tmp.numel())
+        if tod_id in self._plans:
+            self._used -= self._plans.pop(tod_id)[2]
+        single.build_plan(stream)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        self._plans[tod_id] = (single, ev, nb)
+        self._used += nb
+        return self._plans[tod_id]
+
+    def _run(self):
+        while not self._stop:
+            with self._lock:
+                while self._submitted:
+                    self._waiting.append(self._submitted.popleft())
+            try:
+                progressed = self._complete()
+                progressed |= self._launch()
+            except Exception as e:   # surfaced to the waiting requests
+                self.errors.append(repr(e))
+                with self._lock:
+                    for r in list(self._waiting):
+                        r["fut"].set_exception(e)
+                    self._waiting.clear()
+            if not progressed:
+                time.sleep(0.0002)
+
+    def _complete(self):
+        done = False
+        keep = []
+        for ev, reqs, nb, keepalive in self._inflight:
+            if ev.query():
+                t1 = time.perf_counter()
+                for r in reqs:
+                    self.latencies[r["kind"]].append(t1 - r["t0"])
+                    r["fut"].set_result(r.get("result"))
+                self._used -= nb
+                done = True
+            else:
+                keep.append((ev, reqs, nb, keepalive))
+        self._inflight = keep
+        return done
+
+    def _launch(self):
+        admitted, pinned = [], set()
+        while self._waiting and len(admitted) < self.max_batch:
+            r = self._waiting[0]
+            need = self._request_nbytes(r) + (0 if r["id"] in self._plans else self._plan_nbytes(r["id"]))
+            pinned.add(r["id"])
+            if not self._evict(need, pinned | {q["id"] for q in admitted}):
+                pinned.discard(r["id"])
+                break
+            admitted.append(self._waiting.popleft())
+            self._used += self._request_nbytes(r)
+        if not admitted:
+            return False
+        stream = self._stream()
+        # Everything below is allocated and launched on 'stream', so allocations, copies and kernels
+        # of one iteration are ordered, and iterations on different streams overlap.
+        with torch.cuda.stream(stream):
+            for r in admitted:
+                self._ensure_plan(r["id"], stream, rebuild=(r["kind"] == "plan"))
+            batches = []
+            for kind in ("map2tod", "tod2map"):
+                reqs = [r for r in admitted if r["kind"] == kind]
+                if not reqs:
+                    continue
+                singles = [self._plans[r["id"]] for r in reqs]
+                for _, ev, _ in singles:
+                    stream.wait_event(ev)
+                xps = [self.xpointings[r["id"]] for r in reqs]
+                if kind == "map2tod":
+                    tods = [torch.empty(x.shape[1:], device="cuda") for x in xps]
+                    for r, t in zip(reqs, tods):
+                        r["result"] = t
+                else:
+                    tods = [r["tod"] for r in reqs]
+                b = TodBatch(xps, tods, self.lpix, tuning=self.tuning)
+                b.merge_plans([sg for sg, _, _ in singles], stream)
+                if kind == "map2tod":
+                    b.map2tod(self.in_map, stream=stream)
+                else:
+                    b.tod2map(self.out_map, stream=stream)
+                self.samples_done += b.total_samples
+                self.launches += 1
+                batches.append(b)
+                self._errwords.append(b.err)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        nb = sum(self._request_nbytes(r) for r in admitted)
+        self._inflight.append((ev, admitted, nb, batches))
+        return True
+
+    def check(self):
+        """Raises if any plan build or launch reported device error bits (waits for the GPU)."""
+        torch.cuda.synchronize()
+        for single, _, _ in self._plans.values():
+            single.check()
+        words = [int(w) for e in self._errwords for w in e.cpu().tolist()]
+        if any(words):
+            raise RuntimeError(f"PointingServer: device error bits {sorted(set(w for w in words if w))}")

@@ -191,6 +191,16 @@ int gmm_batch_plan_build(const gmm_tod_desc *descs_gpu, int32_t ntod, int64_t to
                          int32_t nxpix_global, int32_t periodic_xcoord, void *plan_buf, int64_t plan_nbytes, void *tmp,
                          int64_t tmp_nbytes, const gmm_batch_tuning *tuning, uint32_t *errword_gpu, cudaStream_t stream);
 
+/* Merges single-TOD batch plans (each built by gmm_batch_plan_build with ntod = 1) into the plan of
+ * a batch whose TOD i has plans_gpu[i]: the owner words are copied with their TOD index set to i,
+ * the cell bitmaps OR-ed, and the list sorted by cell (stable: the order gmm_batch_plan_build gives
+ * for the same batch).  plans_gpu and nlines_gpu are device arrays of ntod entries; nlines[i] is TOD
+ * i's line count (its nsamp/32); their sum is total_lines.  'plan_buf' and 'tmp' are sized by
+ * gmm_batch_plan_nbytes(total_lines, ...). */
+int gmm_batch_plan_merge(const void *const *plans_gpu, const int64_t *nlines_gpu, int32_t ntod, int64_t total_lines,
+                         int32_t nypix_global, int32_t nxpix_global, void *plan_buf, int64_t plan_nbytes, void *tmp,
+                         int64_t tmp_nbytes, const gmm_batch_tuning *tuning, cudaStream_t stream);
+
 /* map2tod / tod2map of every TOD of the batch in one launch each, with the semantics of
  * gmm_planned_map2tod / gmm_planned_tod2map per TOD. */
 int gmm_batch_map2tod(const gmm_tod_desc *descs_gpu, int32_t ntod, int64_t total_lines, const float *local_map,

@@ -1,0 +1,131 @@
+"""GPU tests of the serving loop (gpu_mm_b200.PointingServer): continuous batching of plan, map2tod
+and tod2map requests over a pool of TODs.  Each result must be the same alone and in the mix:
+map2tod bit for bit (the same rounded arithmetic per sample), tod2map within the float tolerance
+against the oracle (float atomics reorder the sums).  A tight HBM budget forces plan evictions."""
+
+import random
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+from tests._common import random_raster, rel_stats
+
+pytestmark = pytest.mark.gpu
+
+RL1_TOL = 1e-6
+MAX_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def g():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import gpu_mm_b200
+    return gpu_mm_b200
+
+
+def pool(seed, n=10, ny=256, nx=512):
+    rng = np.random.default_rng(seed)
+    xps = {i: random_raster(rng, int(rng.integers(1, 6)), 32 * int(rng.integers(16, 96)), ny, nx, True,
+                            speed=float(rng.uniform(0.3, 1.1))) for i in range(n)}
+    tods = {i: rng.standard_normal(x.shape[1:]).astype(np.float32) for i, x in xps.items()}
+    return rng, xps, tods
+
+
+def run_mix(g, xps_np, tods_np, m, requests, budget, ny=256, nx=512, jitter=True):
+    import torch
+    lp = g.LocalPixelization.make_rectangle(ny, nx, True)
+    xg = {i: torch.from_numpy(x).cuda() for i, x in xps_np.items()}
+    tg = {i: torch.from_numpy(t).cuda() for i, t in tods_np.items()}
+    in_map = torch.from_numpy(m).cuda()
+    out_map = torch.zeros(3 * lp.npix, device="cuda")
+    torch.cuda.synchronize()
+    srv = g.PointingServer(xg, in_map, out_map, lp, hbm_budget_bytes=budget)
+    futs = []
+    rnd = random.Random(7)
+    for kind, i in requests:
+        futs.append((kind, i, srv.submit(kind, i, tod=tg[i] if kind == "tod2map" else None)))
+        if jitter and rnd.random() < 0.3:
+            time.sleep(rnd.uniform(0.0, 0.002))
+    srv.drain()
+    results = [(kind, i, f.result(timeout=30)) for kind, i, f in futs]
+    srv.check()
+    stats = srv.stats()
+    srv.close()
+    m2t = [(i, r.cpu().numpy()) for kind, i, r in results if kind == "map2tod"]
+    return m2t, out_map.cpu().numpy(), stats, srv
+
+
+def test_serving_mix_matches_alone(g):
+    ny, nx = 256, 512
+    rng, xps, tods = pool(3)
+    lp_o = oracle.Lpix.rectangle(ny, nx, True)
+    m = rng.standard_normal(3 * lp_o.npix).astype(np.float32)
+    kinds = ["plan"] * 4 + ["map2tod"] * 3 + ["tod2map"] * 3
+    requests = [(kinds[int(rng.integers(0, 10))], int(rng.integers(0, len(xps)))) for _ in range(60)]
+    m2t_mix, out_mix, stats, srv = run_mix(g, xps, tods, m, requests, budget=8 << 30)
+    assert stats["launches"] >= 1 and not srv.errors
+    # Alone: the same requests one at a time through the plain planned operators.
+    import torch
+    lpg = g.LocalPixelization.make_rectangle(ny, nx, True)
+    lmap = g.LocalMap(lpg, torch.from_numpy(m).cuda())
+    for i, r in m2t_mix:
+        xg = torch.from_numpy(xps[i]).cuda()
+        alone = torch.zeros(xps[i].shape[1:], device="cuda")
+        g.map2tod(alone, lmap, xg, g.PointingPlan(g.PointingPrePlan(xg, ny, nx), xg))
+        np.testing.assert_array_equal(r, alone.cpu().numpy())
+    want = np.zeros(3 * lp_o.npix, np.float32)
+    for kind, i in requests:
+        if kind == "tod2map":
+            oracle.tod2map(want, tods[i], xps[i], lp_o)
+    rl1, mx = rel_stats(out_mix, want)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+
+
+def test_serving_tight_budget_evicts_and_stays_correct(g):
+    ny, nx = 256, 512
+    rng, xps, tods = pool(5, n=12)
+    lp_o = oracle.Lpix.rectangle(ny, nx, True)
+    m = rng.standard_normal(3 * lp_o.npix).astype(np.float32)
+    # Room for about three cached plans and six requests (the server's own accounting), not for all
+    # twelve plans: plans are evicted and rebuilt as requests come and go.
+    n_max = max(x[0].size for x in xps.values())
+    per_plan = 16 * (n_max // 32) + (1 << 17) + (1 << 20)
+    per_req = 4 * n_max + 16 * (n_max // 32) + (1 << 18)
+    budget = 3 * per_plan + 6 * per_req
+    requests = [("map2tod", i % 12) for i in range(36)] + [("tod2map", (5 * i) % 12) for i in range(24)]
+    m2t_mix, out_mix, stats, srv = run_mix(g, xps, tods, m, requests, budget=budget, jitter=False)
+    assert stats["evictions"] > 0 and stats["plan_cache"]["plans"] < 12, stats
+    assert stats["plan_cache"]["bytes"] <= budget, stats
+    import torch
+    lpg = g.LocalPixelization.make_rectangle(ny, nx, True)
+    lmap = g.LocalMap(lpg, torch.from_numpy(m).cuda())
+    for i, r in m2t_mix:
+        xg = torch.from_numpy(xps[i]).cuda()
+        alone = torch.zeros(xps[i].shape[1:], device="cuda")
+        g.map2tod(alone, lmap, xg, None)
+        np.testing.assert_array_equal(r, alone.cpu().numpy())
+    want = np.zeros(3 * lp_o.npix, np.float32)
+    for kind, i in requests:
+        if kind == "tod2map":
+            oracle.tod2map(want, tods[i], xps[i], lp_o)
+    rl1, mx = rel_stats(out_mix, want)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+
+
+def test_serving_rejects_bad_requests(g):
+    import torch
+    rng, xps, tods = pool(9, n=2)
+    lp = g.LocalPixelization.make_rectangle(256, 512, True)
+    xg = {i: torch.from_numpy(x).cuda() for i, x in xps.items()}
+    srv = g.PointingServer(xg, torch.zeros(3 * lp.npix, device="cuda"), torch.zeros(3 * lp.npix, device="cuda"),
+                           lp, hbm_budget_bytes=1 << 30)
+    with pytest.raises(KeyError):
+        srv.submit("map2tod", 99)
+    with pytest.raises(ValueError):
+        srv.submit("tod2map", 0)
+    with pytest.raises(ValueError):
+        srv.submit("bogus", 0)
+    srv.close()
