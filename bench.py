@@ -23,6 +23,9 @@ Other numbers on the JSON line:
   batched      64 uneven TODs (lognormal nsamp) into one map: plain per-TOD calls against one
                autotuned TodBatch replayed as CUDA graphs; speed-up, bitwise map2tod equality and
                tod2map error against the FP64 oracle
+  served       Poisson request stream (plan / map2tod / tod2map) through PointingServer (continuous
+               batching) and through sequential plain calls: p50/p99 latency, saturated Gsamples/s,
+               bitwise map2tod equality, tod2map error against the FP64 oracle
   precision    tod2map precision variants (float atomics, compensated float flush, float64 map) on
                the high-hit workload (2^28 samples in a 512x512 box, tod = 1e3 + N(0,1)): throughput
                and max/rms relative error against the FP64 oracle on the host cores
@@ -57,6 +60,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-precision", action="store_true", help="skip the tod2map precision study")
     p.add_argument("--no-batch", action="store_true", help="skip the batched-TOD study")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving study")
     p.add_argument("--only", default="", help="profiling aid: 'map2tod' or 'tod2map' runs only that operator")
     return p.parse_args()
 
@@ -284,6 +288,45 @@ def precision_study(max_run_lines=1024):
     }
 
 
+def touched_cells(plan_bytes, total_lines):
+    """(iycell, ixcell) of the cells set in a batch plan's cell bitmap (after the owner list)."""
+    import numpy as np
+    off = ((8 * total_lines + 127) // 128) * 128
+    bits = np.unpackbits(plan_bytes[off:off + (1 << 17)].cpu().numpy(), bitorder="little")
+    return [(int(c) >> 10, int(c) & 1023) for c in np.flatnonzero(bits)]
+
+
+def fp64_oracle_cells(pairs, cells, ny, nx, periodic):
+    """FP64 oracle tod2map (reference_tod2map<double> on the float32 inputs widened) of every
+    (xpointing, tod) CUDA pair, in one multithreaded call, into a compact map of 'cells' (the cells
+    the pairs touch): float64 [ncells][3][64][64]."""
+    import numpy as np
+    import oracle
+    offs = np.full(((ny + 63) // 64, (nx + 63) // 64), -1, dtype=np.int64)
+    for k, (cy, cx) in enumerate(cells):
+        offs[cy, cx] = 3 * 4096 * k
+    lp = oracle.Lpix(ny, nx, offs, 64, 4096, periodic)
+    xp = np.concatenate([x.reshape(3, -1).cpu().numpy() for x, _ in pairs], axis=1)
+    tod = np.concatenate([t.reshape(-1).cpu().numpy() for _, t in pairs])
+    want = np.zeros(3 * 4096 * len(cells), np.float64)
+    assert oracle.tod2map_f64w_mt(want, tod, np.ascontiguousarray(xp), lp, os.cpu_count() or 1) == 0
+    return want.reshape(len(cells), 3, 64, 64)
+
+
+def rect_cells(arr, cells, ny, nx):
+    """The cells of a rectangular-layout map (3, ny, nx) as float64 [ncells][3][64][64]."""
+    import numpy as np
+    a = arr.reshape(3, ny, nx)
+    return np.stack([a[:, 64 * cy:64 * cy + 64, 64 * cx:64 * cx + 64].cpu().numpy() for cy, cx in cells]).astype(np.float64)
+
+
+def rel_errs(a, want):
+    import numpy as np
+    d = a - want
+    return {"max_rel_err": float(f"{np.abs(d).max() / np.abs(want).max():.3e}"),
+            "rms_rel_err": float(f"{np.sqrt((d * d).sum() / (want * want).sum()):.3e}")}
+
+
 def batch_study(reps=3):
     """64 TODs of lognormal nsamp (median 2^20, sigma 1.0, clipped to [2^16, 2^24]), each its own
     rotated raster, into one 3x4096x8192 map: plan build + map2tod + tod2map of every TOD, (a) as
@@ -350,17 +393,10 @@ def batch_study(reps=3):
     map_batch.zero_()
     batched()
     torch.cuda.synchronize()
-    want = np.zeros(3 * lp.npix, np.float64)
-    lp_o = oracle.Lpix.rectangle(ny, nx, False)
-    nthreads = os.cpu_count() or 1
-    for xp, t in zip(xps, tods_in):
-        assert oracle.tod2map_f64w_mt(want, t.cpu().numpy(), xp.cpu().numpy(), lp_o, nthreads) == 0
-
-    def errs(a):
-        d = a.cpu().numpy().astype(np.float64) - want
-        return float(f"{np.abs(d).max() / np.abs(want).max():.3e}"), float(f"{np.sqrt((d * d).sum() / (want * want).sum()):.3e}")
-
-    pe, be = errs(map_plain.arr), errs(map_batch)
+    cells = touched_cells(b_out.plan, b_out.total_lines)
+    want = fp64_oracle_cells(list(zip(xps, tods_in)), cells, ny, nx, False)
+    pe = rel_errs(rect_cells(map_plain.arr, cells, ny, nx), want)
+    be = rel_errs(rect_cells(map_batch, cells, ny, nx), want)
     return {
         "workload": f"64 TODs, nsamp lognormal (median 2^20, sigma 1.0, clipped [2^16, 2^24]), total {total} samples, "
                     "rotated rasters, 3x4096x8192 map",
@@ -370,9 +406,116 @@ def batch_study(reps=3):
         "batched_gsamples_s": round(total / (batch_ms * 1e-3) / 1e9, 3),
         "speedup": round(plain_ms / batch_ms, 3),
         "map2tod_bitwise_equal": bool(map2tod_equal),
-        "tod2map_vs_fp64": {"plain": {"max_rel_err": pe[0], "rms_rel_err": pe[1]},
-                            "batched": {"max_rel_err": be[0], "rms_rel_err": be[1]}},
+        "tod2map_vs_fp64": {"plain": pe, "batched": be, "cells": len(cells)},
         "autotune": {"best": list(best), "candidates_ms": cand_ms},
+    }
+
+
+def serving_study(rate=200.0, duration_s=2.5, ntod_pool=128, seed=5):
+    """Poisson arrivals at 'rate' req/s for 'duration_s' (seeded): 40% plan build, 30% map2tod, 30%
+    tod2map, on TODs drawn uniformly from a pool of 'ntod_pool' TODs sized as the batched workload,
+    against a resident 3x8192x32768 map; plan cache budget 120 GB.  (a) PointingServer (continuous
+    batching) and (b) sequential plain calls (one request at a time, plans cached the same way) serve
+    the same request stream at the same arrival times; latency = completion - arrival.  Then both
+    serve the same requests all at once (saturated): sustained Gsamples/s = samples processed /
+    (last completion - first arrival).  Results: map2tod of every request compared bitwise between
+    (a) and (b); the tod2map output maps against the FP64 oracle."""
+    import threading
+    import numpy as np
+    import torch
+    import oracle
+    import gpu_mm_b200 as g
+    from gpu_mm_b200 import synthetic
+    ny, nx = 8192, 32768
+    xps = synthetic.config4_tods(device="cuda", ntod=ntod_pool, seed=2000, ny=ny, nx=nx)
+    pool = dict(enumerate(xps))
+    lp = g.LocalPixelization.make_rectangle(ny, nx, False)
+    gen = torch.Generator(device="cuda").manual_seed(55)
+    in_map = torch.randn(3 * lp.npix, generator=gen, device="cuda")
+    tods = {i: torch.randn(x.shape[1], generator=gen, device="cuda") for i, x in pool.items()}
+    rng = np.random.default_rng(seed)
+    t, reqs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration_s:
+            break
+        u = rng.random()
+        kind = "plan" if u < 0.4 else ("map2tod" if u < 0.7 else "tod2map")
+        reqs.append((t, kind, int(rng.integers(0, ntod_pool))))
+    torch.cuda.synchronize()
+
+    def served(times):
+        out_map = torch.zeros(3 * lp.npix, device="cuda")
+        srv = g.PointingServer(pool, in_map, out_map, lp, hbm_budget_bytes=120 << 30)
+        futs, t0 = [], time.perf_counter()
+        for (ta, kind, i) in times:
+            dt = t0 + ta - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            futs.append((kind, i, srv.submit(kind, i, tod=tods[i] if kind == "tod2map" else None)))
+        srv.drain(timeout=120)
+        t_end = time.perf_counter()
+        res = [(kind, i, f.result(timeout=60)) for kind, i, f in futs]
+        srv.check()
+        st = srv.stats()
+        srv.close()
+        return res, out_map, st, t_end - t0
+
+    def sequential(times):
+        out_map = torch.zeros(3 * lp.npix, device="cuda")
+        lmap_in = g.LocalMap(lp, in_map)
+        lmap_out = g.LocalMap(lp, out_map)
+        plans, res, lat = {}, [], []
+        t0 = time.perf_counter()
+        for (ta, kind, i) in times:
+            dt = t0 + ta - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            xp = pool[i]
+            if kind == "plan" or i not in plans:
+                plans[i] = g.PointingPlan(g.PointingPrePlan(xp, ny, nx, periodic_xcoord=False), xp)
+            r = None
+            if kind == "map2tod":
+                r = torch.empty(xp.shape[1], device="cuda")
+                g.map2tod(r, lmap_in, xp, plans[i])
+            elif kind == "tod2map":
+                g.tod2map(lmap_out, tods[i], xp, plans[i])
+            torch.cuda.synchronize()
+            lat.append(time.perf_counter() - (t0 + ta))
+            res.append((kind, i, r))
+        return res, out_map, lat, time.perf_counter() - t0
+
+    def pct(v):
+        a = np.asarray(v) * 1e3
+        return {"p50_ms": round(float(np.percentile(a, 50)), 3), "p99_ms": round(float(np.percentile(a, 99)), 3)}
+
+    samples = sum(pool[i].shape[1] for _, _, i in reqs)
+    res_a, map_a, st_a, _ = served(reqs)
+    res_b, map_b, lat_b, _ = sequential(reqs)
+    burst = [(0.0, k, i) for _, k, i in reqs]
+    _, _, st_burst, wall_a = served(burst)
+    _, _, _, wall_b = sequential(burst)
+    m2t_equal = all(torch.equal(ra[2], rb[2]) for ra, rb in zip(res_a, res_b) if ra[0] == "map2tod")
+    t2m = [(pool[i], tods[i]) for _, kind, i in reqs if kind == "tod2map"]
+    probe = g.TodBatch([x for x, _ in t2m], [t for _, t in t2m], lp)
+    probe.build_plan()
+    cells = touched_cells(probe.plan, probe.total_lines)
+    del probe
+    want = fp64_oracle_cells(t2m, cells, ny, nx, False)
+    return {
+        "workload": f"Poisson {rate:g} req/s for {duration_s:g} s: {len(reqs)} requests (40% plan, 30% map2tod, "
+                    f"30% tod2map) over a pool of {ntod_pool} TODs (nsamp lognormal, median 2^20), "
+                    f"{samples} samples; resident 3x8192x32768 map; plan cache budget 120 GB",
+        "served": {"latency": {k: v for k, v in st_a.items() if isinstance(v, dict) and "p50_ms" in v},
+                   "launches": st_a["launches"]},
+        "sequential_plain": {"latency": {"all": pct(lat_b)}},
+        "saturated": {"served_gsamples_s": round(samples / wall_a / 1e9, 3),
+                      "sequential_gsamples_s": round(samples / wall_b / 1e9, 3),
+                      "speedup": round(wall_b / wall_a, 3), "served_wall_s": round(wall_a, 4),
+                      "sequential_wall_s": round(wall_b, 4), "served_iterations": st_burst.get("iterations")},
+        "map2tod_bitwise_equal": bool(m2t_equal),
+        "tod2map_vs_fp64": {"served": rel_errs(rect_cells(map_a, cells, ny, nx), want),
+                            "sequential_plain": rel_errs(rect_cells(map_b, cells, ny, nx), want), "cells": len(cells)},
     }
 
 
@@ -569,12 +712,17 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.ndet_rows)
-    precision = None
-    if rank == 0 and world == 1 and not args.no_precision:
-        precision = precision_study()
-    batched = None
-    if rank == 0 and world == 1 and not args.no_batch:
-        batched = batch_study()
+    def study(name, skip, fn):
+        if rank != 0 or world != 1 or skip:
+            return None
+        t0 = time.perf_counter()
+        r = fn()
+        print(f"[bench] {name} study: {time.perf_counter() - t0:.1f} s", file=sys.stderr, flush=True)
+        return r
+
+    precision = study("precision", args.no_precision, precision_study)
+    batched = study("batched", args.no_batch, batch_study)
+    served = study("serving", args.no_serve, serving_study)
 
     if rank == 0:
         value = world * nsamp / (ms_step * 1e-3) / 1e9
@@ -594,7 +742,7 @@ def main():
                            "first_plan_build_s": round(first_plan_s, 3)},
             "plan": {"nmt": int(pp.plan_nmt), "overhead": round(pp.overhead, 4), "sort_digit_bits": pp.sort_digit_bits},
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks.summary(), "precision": precision,
-            "batched": batched,
+            "batched": batched, "served": served,
             "gpu_launches": args.steps * (int(do_m2t) + int(do_t2m)),
         }
         print(json.dumps(line), flush=True)

@@ -49,10 +49,25 @@ def _check_pair(i, xp, tod):
     return nsamp
 
 
-class TodBatch:
-    """A batch of TODs against one LocalPixelization (see the module docstring)."""
+class SinglePlan:
+    """The plan of one TOD as a batch of one (owner list + cell bitmap), built by
+    TodBatch.build_plans_each(); TodBatch.merge_plans() combines such plans."""
 
-    def __init__(self, xpointings, tods, local_pixelization, tuning=None):
+    def __init__(self, nsamp, lpix, tuning, stream=None):
+        self.ntod = 1
+        self.nsamp = int(nsamp)
+        self.total_lines = self.nsamp // 32
+        pn, _ = _m.batch_plan_nbytes(self.total_lines, lpix.nypix_global, lpix.nxpix_global, tuning)
+        self.plan = torch.empty(pn, dtype=torch.uint8, device="cuda")
+
+
+class TodBatch:
+    """A batch of TODs against one LocalPixelization (see the module docstring).  With 'upload_stream'
+    the descriptor table is copied to the device asynchronously on that stream (the batch must then
+    be used on that stream); otherwise the copy completes before the constructor returns.
+    plan_buffers=False skips the batch plan's buffers (for build_plans_each only)."""
+
+    def __init__(self, xpointings, tods, local_pixelization, tuning=None, upload_stream=None, plan_buffers=True):
         if not isinstance(local_pixelization, LocalPixelization):
             raise RuntimeError("TodBatch: expected a LocalPixelization")
         if len(xpointings) != len(tods) or not (1 <= len(xpointings) <= 65535):
@@ -65,9 +80,10 @@ class TodBatch:
         self.total_lines = self.total_samples // 32
         self.tuning = tuple(tuning) if tuning is not None else tuple(_m.batch_tuning_default())
         self.err = torch.zeros(3, dtype=torch.int32, device="cuda")   # build, map2tod, tod2map
-        self._plan_owner = None
+        self._upload_stream = upload_stream
         self._set_tods(tods)
-        self._alloc()
+        if plan_buffers:            # not needed when the batch only builds single-TOD plans
+            self._alloc()
 
     def _set_tods(self, tods):
         self.tods = list(tods)
@@ -76,7 +92,14 @@ class TodBatch:
         d["tod"] = [t.data_ptr() for t in self.tods]
         d["nsamp"] = self.nsamps
         d["line0"] = np.concatenate([[0], np.cumsum(np.asarray(self.nsamps, np.int64) // 32)[:-1]])
-        self.descs = torch.from_numpy(d.view(np.uint8).copy()).cuda()
+        host = torch.from_numpy(d.view(np.uint8).copy())
+        if self._upload_stream is None:
+            self.descs = host.cuda()
+            torch.cuda.current_stream().synchronize()
+        else:
+            self._descs_host = host.pin_memory()          # alive until the batch is dropped
+            with torch.cuda.stream(self._upload_stream):
+                self.descs = self._descs_host.cuda(non_blocking=True)
 
     def _alloc(self):
         pn, tn = _m.batch_plan_nbytes(self.total_lines, self.lpix.nypix_global, self.lpix.nxpix_global, self.tuning)
@@ -116,6 +139,24 @@ class TodBatch:
                             self.total_lines, self.lpix.nypix_global, self.lpix.nxpix_global, self.plan.data_ptr(),
                             self.plan.numel(), self.tmp.data_ptr(), self.tmp.numel(), self.tuning,
                             _stream_handle(stream))
+
+    def build_plans_each(self, stream=None):
+        """The single-TOD plan of every TOD of the batch (a SinglePlan each), built together: one
+        owner pass over all TODs, one sort by (TOD, cell), one scatter (at most 4096 TODs)."""
+        lp = self.lpix
+        st = self._upload_stream if stream is None and self._upload_stream is not None else stream
+        with torch.cuda.stream(st if isinstance(st, torch.cuda.Stream) else torch.cuda.current_stream()):
+            singles = [SinglePlan(n, lp, self.tuning) for n in self.nsamps]
+            ptrs = torch.tensor([sp.plan.data_ptr() for sp in singles], dtype=torch.int64).pin_memory()
+            self._each_host = ptrs
+            self._each_ptrs = ptrs.cuda(non_blocking=True)
+            tn = _m.batch_plan_each_tmp_nbytes(self.total_lines, self.ntod, lp.nypix_global, lp.nxpix_global,
+                                               self.tuning)
+            self._each_tmp = torch.empty(tn, dtype=torch.uint8, device="cuda")
+        _m.batch_plan_build_each(self.descs.data_ptr(), self.ntod, self.total_lines, lp.nypix_global, lp.nxpix_global,
+                                 bool(lp.periodic_xcoord), self._each_ptrs.data_ptr(), self._each_tmp.data_ptr(),
+                                 self._each_tmp.numel(), self.tuning, self.err.data_ptr(), _stream_handle(st))
+        return singles
 
     def set_tuning(self, tuning):
         """Launch/sort parameters (sort_digit_bits, ctas_per_sm, min_lines_per_cta); the plan must be

@@ -603,8 +603,8 @@ int gmm_batch_plan_build(const gmm_tod_desc *descs, int32_t ntod, int64_t total_
     if (e == cudaSuccess)
         e = cudaMemsetAsync(cellmap, 0, kCellmapBytes, stream);
     if (e == cudaSuccess)
-        e = launch_batch_owner(descs, ntod, total_lines, ny, nx, periodic != 0, even ? owner : alt, cellmap, errword,
-                               stream);
+        e = launch_batch_owner(descs, ntod, total_lines, ny, nx, periodic != 0, even ? owner : alt, cellmap, nullptr,
+                               errword, stream);
     if (e == cudaSuccess)
         e = radix_sort_mt(even ? owner : alt, even ? alt : owner, total_lines, nyc, nxc, dbits, passes, hist, stream);
     return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
@@ -640,6 +640,62 @@ int gmm_batch_plan_merge(const void *const *plans, const int64_t *nlines, int32_
         e = launch_batch_merge(plans, nlines, ntod, total_lines, even ? owner : alt, cellmap, stream);
     if (e == cudaSuccess)
         e = radix_sort_mt(even ? owner : alt, even ? alt : owner, total_lines, nyc, nxc, dbits, passes, hist, stream);
+    return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
+}
+
+static int each_tod_bits(int32_t ntod)
+{
+    int b = 0;
+    while ((1 << b) < ntod) b++;
+    return b;
+}
+
+int gmm_batch_plan_each_tmp_nbytes(int64_t total_lines, int32_t ntod, int32_t ny, int32_t nx,
+                                   const gmm_batch_tuning *tuning, int64_t *tmp_nbytes)
+{
+    const char *where = "batch_plan_each_tmp_nbytes";
+    if (int rc = check_npix(ny, nx, where)) return rc;
+    if (int rc = check_tuning(tuning, where)) return rc;
+    if (int rc = check_ptr(tmp_nbytes, where, "tmp_nbytes")) return rc;
+    if ((ntod < 1) || (ntod > 4096) || (total_lines < ntod))
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": need 1 <= ntod <= 4096 and total_lines >= ntod");
+    int dbits = 0;
+    sort_passes((ny + 63) / 64, (nx + 63) / 64, tuning ? tuning->sort_digit_bits : g_sort_max_digit_bits, &dbits,
+                each_tod_bits(ntod));
+    *tmp_nbytes = 2 * align128(8 * total_lines) + std::max<int64_t>(sort_scratch_nbytes(dbits, kSortGridMax), 128);
+    return 0;
+}
+
+int gmm_batch_plan_build_each(const gmm_tod_desc *descs, int32_t ntod, int64_t total_lines, int32_t ny, int32_t nx,
+                              int32_t periodic, void *const *plans_gpu, void *tmp, int64_t tmp_nbytes,
+                              const gmm_batch_tuning *tuning, uint32_t *errword, cudaStream_t stream)
+{
+    const char *where = "batch_plan_build_each";
+    if (int rc = check_batch(descs, ntod, total_lines, where)) return rc;
+    if (ntod > 4096)
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": at most 4096 TODs per call");
+    if (int rc = check_npix(ny, nx, where)) return rc;
+    if (int rc = check_tuning(tuning, where)) return rc;
+    if (int rc = check_ptr(plans_gpu, where, "plans")) return rc;
+    if (int rc = check_ptr(tmp, where, "tmp")) return rc;
+    if (int rc = check_ptr(errword, where, "errword")) return rc;
+    if (((uintptr_t) tmp) & 127)
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": 'tmp' must be 128-byte aligned");
+    int64_t need = 0;
+    if (int rc = gmm_batch_plan_each_tmp_nbytes(total_lines, ntod, ny, nx, tuning, &need)) return rc;
+    if (tmp_nbytes < need)
+        return fail(GMM_ERR_BUFFER_TOO_SMALL, std::string(where) + ": 'tmp' too small");
+    const int tb = each_tod_bits(ntod);
+    int dbits = 0;
+    const int passes = sort_passes((ny + 63) / 64, (nx + 63) / 64,
+                                   tuning ? tuning->sort_digit_bits : g_sort_max_digit_bits, &dbits, tb);
+    char *t = (char *) tmp;
+    uint64_t *a = (uint64_t *) t, *b = (uint64_t *) (t + align128(8 * total_lines));
+    uint32_t *hist = (uint32_t *) (t + 2 * align128(8 * total_lines));
+    cudaError_t e = cudaMemsetAsync(errword, 0, sizeof(uint32_t), stream);
+    if (e == cudaSuccess)
+        e = launch_plans_each(descs, ntod, total_lines, ny, nx, periodic != 0, plans_gpu, a, b, hist, dbits, passes, tb,
+                              errword, stream);
     return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
 }
 

@@ -17,11 +17,12 @@ namespace gmm {
 int device_sm_count();
 
 // ---- plan construction (plan_kernels.cu) ----
-int sort_passes(int nycells_max, int nxcells_max, int max_digit_bits, int *digit_bits);
+// Radix sort of plan words by cell (and, with tod_bits > 0, by TOD index above the cell).
+int sort_passes(int nycells_max, int nxcells_max, int max_digit_bits, int *digit_bits, int tod_bits = 0);
 int64_t sort_scratch_nbytes(int digit_bits, int grid);
 int sort_grid_for(int64_t n);
 cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, int nxcells_max, int digit_bits,
-                          int npasses, uint32_t *hist, cudaStream_t stream);
+                          int npasses, uint32_t *hist, cudaStream_t stream, int tod_bits = 0);
 cudaError_t launch_preplan(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
                            int nblocks, uint32_t *nmt, uint32_t *err, cudaStream_t stream);
 cudaError_t launch_plan_emit(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
@@ -98,7 +99,11 @@ cudaError_t launch_fold_compensation(float *lmap, float *comp, int64_t n, cudaSt
 // Batches of TODs.
 constexpr int kBatchTodShift = 48;
 cudaError_t launch_batch_owner(const gmm_tod_desc *descs, int ntod, int64_t total_lines, int ny, int nx, bool periodic,
-                               uint64_t *owner_out, uint32_t *cellmap, uint32_t *errword, cudaStream_t stream);
+                               uint64_t *owner_out, uint32_t *cellmap, void *const *plans_each, uint32_t *errword,
+                               cudaStream_t stream);
+cudaError_t launch_plans_each(const gmm_tod_desc *descs, int ntod, int64_t total_lines, int ny, int nx, bool periodic,
+                              void *const *plans, uint64_t *a, uint64_t *b, uint32_t *hist, int digit_bits,
+                              int npasses, int tod_bits, uint32_t *errword, cudaStream_t stream);
 cudaError_t launch_batch_merge(const void *const *plans, const int64_t *nlines, int ntod, int64_t total_lines,
                                uint64_t *owner_out, uint32_t *cellmap, cudaStream_t stream);
 cudaError_t launch_batch_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,

@@ -291,15 +291,20 @@ struct DigitSpec {
     int xbits;       // bits of the ixcell part
     uint32_t xmask;  // (1 << xbits) - 1
     uint32_t ymask;  // mask of the iycell part
+    int ybits;       // bits of the iycell part
+    uint32_t tmask;  // mask of the TOD index (bits 48+ of batch words) above the cell; 0: cell only
     int shift;       // first compound bit of this pass
     int dbits;       // digit width of this pass
 };
 
+// Compound sort key of a word: ixcell | iycell << xbits | tod << (xbits + ybits), of which this pass
+// takes 'dbits' bits from bit 'shift'.
 __device__ __forceinline__ uint32_t key_digit(uint64_t w, const DigitSpec &ds)
 {
     uint32_t c = (uint32_t) w;
     uint32_t ix = c & 0x3ffu, iy = (c >> 10) & 0x3ffu;
-    uint32_t comp = (ix & ds.xmask) | ((iy & ds.ymask) << ds.xbits);
+    uint32_t comp = (ix & ds.xmask) | ((iy & ds.ymask) << ds.xbits) |
+                    (((uint32_t) (w >> 48) & ds.tmask) << (ds.xbits + ds.ybits));
     return (comp >> ds.shift) & ((1u << ds.dbits) - 1u);
 }
 
@@ -500,9 +505,9 @@ static int bits_for(int64_t n)   // bits needed for values in [0, n)
     return b;
 }
 
-int sort_passes(int nycells_max, int nxcells_max, int max_digit_bits, int *digit_bits)
+int sort_passes(int nycells_max, int nxcells_max, int max_digit_bits, int *digit_bits, int tod_bits)
 {
-    const int cb = bits_for(nxcells_max) + bits_for(nycells_max);
+    const int cb = bits_for(nxcells_max) + bits_for(nycells_max) + tod_bits;
     if (cb == 0) {
         *digit_bits = 0;
         return 0;
@@ -532,11 +537,12 @@ int sort_grid_for(int64_t n) { return sort_grid(n, device_sm_count()); }
 // Sorts 'n' mt words by cell.  The input is in 'a'; the result ends in 'a' if npasses is even and in
 // 'b' if it is odd (callers place the input accordingly).
 cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, int nxcells_max, int digit_bits,
-                          int npasses, uint32_t *hist, cudaStream_t stream)
+                          int npasses, uint32_t *hist, cudaStream_t stream, int tod_bits)
 {
     if ((n <= 0) || (npasses == 0))
         return cudaSuccess;
     const int xbits = bits_for(nxcells_max), ybits = bits_for(nycells_max);
+    const int kbits = xbits + ybits + tod_bits;
     const int G = sort_grid_for(n);
     const int64_t chunk = (((n + G - 1) / G) + 255) / 256 * 256;
     constexpr int K = 8;
@@ -552,8 +558,10 @@ cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, 
         ds.xbits = xbits;
         ds.xmask = (1u << xbits) - 1u;
         ds.ymask = (1u << ybits) - 1u;
+        ds.ybits = ybits;
+        ds.tmask = (1u << tod_bits) - 1u;
         ds.shift = p * digit_bits;
-        ds.dbits = min(digit_bits, xbits + ybits - p * digit_bits);
+        ds.dbits = min(digit_bits, kbits - p * digit_bits);
         const int ndp = 1 << ds.dbits;
         sort_upsweep_kernel<<<G, 256, ndp * sizeof(uint32_t), stream>>>(src, n, chunk, ds, hist);
         sort_scan_kernel<<<1, 1024, 0, stream>>>(hist, (int64_t) ndp * G);
@@ -583,16 +591,23 @@ __device__ __forceinline__ int batch_tod_of_line(const gmm_tod_desc *__restrict_
 
 // Marks 'cell' in the cell bitmap unless it is in this warp's cache of recently marked cells (one
 // entry per lane 0..7, round robin); 'cell' is warp-uniform.
-__device__ __forceinline__ void mark_cell(uint32_t cell, uint32_t *cellmap, uint32_t &cache, int &next)
+__device__ __forceinline__ void mark_cell(uint32_t cell, uint32_t tag, uint32_t *cellmap, uint32_t &cache, int &next)
 {
     const int lane = threadIdx.x & 31;
-    if (__ballot_sync(kFullMask, (lane < 8) && (cache == cell)) != 0u)
+    const uint32_t key = cell | tag;   // 'tag' distinguishes per-TOD bitmaps (0 for one shared bitmap)
+    if (__ballot_sync(kFullMask, (lane < 8) && (cache == key)) != 0u)
         return;
     if (lane == 0)
         atomicOr(cellmap + (cell >> 5), 1u << (cell & 31));
     if (lane == next)
-        cache = cell;
+        cache = key;
     next = (next + 1) & 7;
+}
+
+// Cell bitmap of a single-TOD batch plan buffer: after its nlines owner words, 128-byte aligned.
+__device__ __forceinline__ uint32_t *single_plan_cellmap(void *plan, int64_t nlines)
+{
+    return (uint32_t *) ((char *) plan + ((8 * nlines + 127) & ~127ll));
 }
 
 // One warp per cache line (lane = sample).  Each CTA takes a contiguous range of the batch's lines
@@ -604,8 +619,10 @@ __device__ __forceinline__ void mark_cell(uint32_t cell, uint32_t *cellmap, uint
 __global__ void __launch_bounds__(256)
 batch_owner_kernel(const gmm_tod_desc *__restrict__ descs, int ntod, int64_t total_lines, int ny, int nx,
                    bool periodic, uint64_t *__restrict__ owner_out, uint32_t *__restrict__ cellmap,
-                   uint32_t *__restrict__ errword)
+                   void *const *__restrict__ plans_each, uint32_t *__restrict__ errword)
 {
+    // plans_each (optional): per-TOD single-TOD plan buffers whose own cell bitmaps are marked
+    // instead of the shared 'cellmap'.
     __shared__ uint32_t s_err[8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int64_t l0 = (total_lines * (int64_t) blockIdx.x) / gridDim.x;
@@ -640,7 +657,13 @@ batch_owner_kernel(const gmm_tod_desc *__restrict__ descs, int ntod, int64_t tot
         if (lane == 0)
             owner_out[gl] = (uint64_t) owner | ((uint64_t) line << 20) | ((uint64_t) multi << 46) |
                             ((uint64_t) tod << kBatchTodShift);
-        mark_cell(owner, cellmap, cache, next);
+        uint32_t *cm = cellmap;
+        uint32_t tag = 0;
+        if (plans_each) {
+            cm = single_plan_cellmap(plans_each[tod], nsamp >> 5);
+            tag = ((uint32_t) tod & 0xfffu) << 20;
+        }
+        mark_cell(owner, tag, cm, cache, next);
         if (multi) {
             // The line's other cells: one representative lane per distinct value of each corner.
 #pragma unroll
@@ -650,7 +673,7 @@ batch_owner_kernel(const gmm_tod_desc *__restrict__ descs, int ntod, int64_t tot
                 while (lead) {
                     const int src = __ffs(lead) - 1;
                     lead &= lead - 1;
-                    mark_cell(__shfl_sync(kFullMask, c[k], src), cellmap, cache, next);
+                    mark_cell(__shfl_sync(kFullMask, c[k], src), tag, cm, cache, next);
                 }
             }
         }
@@ -709,14 +732,61 @@ cudaError_t launch_batch_merge(const void *const *plans, const int64_t *nlines, 
 }
 
 cudaError_t launch_batch_owner(const gmm_tod_desc *descs, int ntod, int64_t total_lines, int ny, int nx, bool periodic,
-                               uint64_t *owner_out, uint32_t *cellmap, uint32_t *errword, cudaStream_t stream)
+                               uint64_t *owner_out, uint32_t *cellmap, void *const *plans_each, uint32_t *errword,
+                               cudaStream_t stream)
 {
     if (total_lines <= 0)
         return cudaSuccess;
     // Contiguous ranges of >= 256 lines per CTA (8 warps).
     const int64_t g = std::max<int64_t>(1, std::min<int64_t>((total_lines + 255) / 256, 8 * (int64_t) device_sm_count()));
     batch_owner_kernel<<<(unsigned) g, 256, 0, stream>>>(descs, ntod, total_lines, ny, nx, periodic, owner_out, cellmap,
-                                                         errword);
+                                                         plans_each, errword);
+    return cudaGetLastError();
+}
+
+// Building many single-TOD plans at once: clear their cell bitmaps, then (after the owner kernel and
+// a sort by (TOD, cell)) copy TOD i's segment [line0_i, line0_i + nlines_i) into its own buffer.
+__global__ void __launch_bounds__(256)
+clear_cellmaps_kernel(const gmm_tod_desc *__restrict__ descs, int ntod, void *const *__restrict__ plans)
+{
+    const int tod = blockIdx.x % ntod, part = blockIdx.x / ntod, nparts = gridDim.x / ntod;
+    uint32_t *cm = single_plan_cellmap(plans[tod], __ldg(&descs[tod].nsamp) >> 5);
+    for (int w = part * blockDim.x + threadIdx.x; w < (1 << 15); w += nparts * blockDim.x)
+        cm[w] = 0u;
+}
+
+__global__ void __launch_bounds__(256)
+scatter_each_kernel(const gmm_tod_desc *__restrict__ descs, const uint64_t *__restrict__ sorted, int64_t total_lines,
+                    void *const *__restrict__ plans)
+{
+    for (int64_t p = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; p < total_lines;
+         p += (int64_t) gridDim.x * blockDim.x) {
+        const uint64_t w = sorted[p];
+        const int tod = (int) (w >> kBatchTodShift);
+        // With consistent descriptors TOD i's entries are exactly [line0_i, line0_i + nlines_i);
+        // anything else (already flagged by the owner kernel) is not written.
+        const int64_t k = p - __ldg(&descs[tod].line0);
+        if ((k >= 0) && (k < (__ldg(&descs[tod].nsamp) >> 5)))
+            ((uint64_t *) plans[tod])[k] = w & ((1ull << kBatchTodShift) - 1);
+    }
+}
+
+cudaError_t launch_plans_each(const gmm_tod_desc *descs, int ntod, int64_t total_lines, int ny, int nx, bool periodic,
+                              void *const *plans, uint64_t *a, uint64_t *b, uint32_t *hist, int digit_bits,
+                              int npasses, int tod_bits, uint32_t *errword, cudaStream_t stream)
+{
+    if (total_lines <= 0)
+        return cudaSuccess;
+    const int nyc = (ny + 63) / 64, nxc = (nx + 63) / 64;
+    clear_cellmaps_kernel<<<(unsigned) (ntod * 4), 256, 0, stream>>>(descs, ntod, plans);
+    cudaError_t e = launch_batch_owner(descs, ntod, total_lines, ny, nx, periodic, a, nullptr, plans, errword, stream);
+    if (e == cudaSuccess)
+        e = radix_sort_mt(a, b, total_lines, nyc, nxc, digit_bits, npasses, hist, stream, tod_bits);
+    if (e != cudaSuccess)
+        return e;
+    const uint64_t *sorted = (npasses % 2 == 0) ? a : b;
+    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((total_lines + 255) / 256, 8 * (int64_t) device_sm_count()));
+    scatter_each_kernel<<<(unsigned) g, 256, 0, stream>>>(descs, sorted, total_lines, plans);
     return cudaGetLastError();
 }
 

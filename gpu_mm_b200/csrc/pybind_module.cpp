@@ -141,6 +141,25 @@ PYBIND11_MODULE(gpu_mm_pybind11, m)
           py::arg("descs"), py::arg("ntod"), py::arg("total_lines"), py::arg("nypix_global"), py::arg("nxpix_global"),
           py::arg("periodic_xcoord"), py::arg("plan"), py::arg("plan_nbytes"), py::arg("tmp"), py::arg("tmp_nbytes"),
           py::arg("tuning"), py::arg("errword"), py::arg("stream") = 0);
+    m.def("batch_plan_each_tmp_nbytes", [tuning_of](long total_lines, int ntod, int ny, int nx, py::object tuning) {
+        gmm_batch_tuning bt = tuning_of(tuning);
+        int64_t tn = 0;
+        throw_on_error(gmm_batch_plan_each_tmp_nbytes(total_lines, ntod, ny, nx, &bt, &tn));
+        return tn;
+    }, py::arg("total_lines"), py::arg("ntod"), py::arg("nypix_global"), py::arg("nxpix_global"),
+       py::arg("tuning") = py::none());
+    m.def("batch_plan_build_each",
+          [tuning_of](uintptr_t descs, int ntod, long total_lines, int ny, int nx, bool periodic, uintptr_t plans,
+                      uintptr_t tmp, long tmp_nbytes, py::object tuning, uintptr_t errword, uintptr_t stream) {
+              gmm_batch_tuning bt = tuning_of(tuning);
+              py::gil_scoped_release rel;
+              throw_on_error(gmm_batch_plan_build_each((const gmm_tod_desc *) descs, ntod, total_lines, ny, nx,
+                                                       periodic, (void *const *) plans, (void *) tmp, tmp_nbytes, &bt,
+                                                       (uint32_t *) errword, (cudaStream_t) stream));
+          },
+          py::arg("descs"), py::arg("ntod"), py::arg("total_lines"), py::arg("nypix_global"), py::arg("nxpix_global"),
+          py::arg("periodic_xcoord"), py::arg("plans"), py::arg("tmp"), py::arg("tmp_nbytes"), py::arg("tuning"),
+          py::arg("errword"), py::arg("stream") = 0);
     m.def("batch_plan_merge",
           [tuning_of](uintptr_t plans, uintptr_t nlines, int ntod, long total_lines, int ny, int nx, uintptr_t plan,
                       long plan_nbytes, uintptr_t tmp, long tmp_nbytes, py::object tuning, uintptr_t stream) {

@@ -12,10 +12,11 @@ A worker thread runs the loop.  Every iteration it
   1. takes the newly submitted requests and admits them in arrival order while their device memory
      (plans, output TODs, batch plans) fits the HBM budget, evicting least-recently-used plans that no
      admitted request needs; requests that do not fit wait and are admitted as memory frees up;
-  2. launches the admitted work on one of several CUDA streams: plan builds (one single-TOD batch plan
-     each), then all admitted map2tod requests as one TodBatch whose plan is merged from the cached
-     single-TOD plans, then all admitted tod2map requests likewise -- so requests that arrive while
-     others are on the GPU join the next launch, and launches of successive iterations overlap;
+  2. launches the admitted work on one of several CUDA streams: the plans it needs (plan requests,
+     and operator requests whose plan is not cached), all built together into single-TOD plans; then
+     all admitted map2tod requests as one TodBatch whose plan is merged from the cached single-TOD
+     plans, then all admitted tod2map requests likewise -- so requests that arrive while others are
+     on the GPU join the next launch, and launches of successive iterations overlap;
   3. completes the requests whose launches have finished (CUDA events) and releases their memory.
 
 Results do not depend on the mix: map2tod evaluates every sample with the same rounded operations as
@@ -58,6 +59,7 @@ class PointingServer:
         self.samples_done = 0
         self.launches = 0
         self.evictions = 0
+        self.iterations = []                               # (requests launched, host seconds)
         self.errors = []
         self._errwords = []
         self._thread = threading.Thread(target=self._run, daemon=True)
@@ -107,6 +109,11 @@ class PointingServer:
                           "p99_ms": round(float(np.percentile(a, 99)), 3)}
         out["launches"] = self.launches
         out["evictions"] = self.evictions
+        if self.iterations:
+            it = np.asarray(self.iterations, dtype=np.float64)
+            out["iterations"] = {"n": len(it), "mean_requests": round(float(it[:, 0].mean()), 2),
+                                 "host_ms_mean": round(1e3 * float(it[:, 1].mean()), 3),
+                                 "host_ms_max": round(1e3 * float(it[:, 1].max()), 3)}
         out["plan_cache"] = {"plans": len(self._plans), "bytes": self._used}
         return out
 
@@ -140,24 +147,6 @@ class PointingServer:
         self._next_stream = (self._next_stream + 1) % len(self.streams)
         return s
 
-    def _ensure_plan(self, tod_id, stream, rebuild=False):
-        if tod_id in self._plans and not rebuild:
-            self._plans.move_to_end(tod_id)
-            return self._plans[tod_id]
-        xp = self.xpointings[tod_id]
-        # A plan needs no TOD array; the y row stands in for it (never read or written by a build).
-        single = TodBatch([xp], [xp[0]], self.lpix, tuning=self.tuning)
-        # Charged at the admission estimate, which bounds the plan and its sort scratch.
-        nb = max(self._plan_nbytes(tod_id), single.plan.numel() + single.tmp.numel())
-        if tod_id in self._plans:
-            self._used -= self._plans.pop(tod_id)[2]
-        single.build_plan(stream)
-        ev = torch.cuda.Event()
-        ev.record(stream)
-        self._plans[tod_id] = (single, ev, nb)
-        self._used += nb
-        return self._plans[tod_id]
-
     def _run(self):
         while not self._stop:
             with self._lock:
@@ -183,7 +172,8 @@ class PointingServer:
                 t1 = time.perf_counter()
                 for r in reqs:
                     self.latencies[r["kind"]].append(t1 - r["t0"])
-                    r["fut"].set_result(r.get("result"))
+                    if not r["fut"].done():
+                        r["fut"].set_result(r.get("result"))
                 self._used -= nb
                 done = True
             else:
@@ -204,19 +194,54 @@ class PointingServer:
             self._used += self._request_nbytes(r)
         if not admitted:
             return False
+        try:
+            t0 = time.perf_counter()
+            ok = self._launch_admitted(admitted)
+            self.iterations.append((len(admitted), time.perf_counter() - t0))
+            return ok
+        except Exception as e:
+            # The admitted requests are no longer queued: fail them here so no client waits forever.
+            for r in admitted:
+                if not r["fut"].done():
+                    r["fut"].set_exception(e)
+                self._used -= self._request_nbytes(r)
+            raise
+
+    def _launch_admitted(self, admitted):
         stream = self._stream()
+        keep = []
         # Everything below is allocated and launched on 'stream', so allocations, copies and kernels
         # of one iteration are ordered, and iterations on different streams overlap.
         with torch.cuda.stream(stream):
+            # Plans to (re)build: plan requests, and operator requests whose plan is not cached --
+            # all built together (one owner pass, one sort, one scatter).
+            need = []
             for r in admitted:
-                self._ensure_plan(r["id"], stream, rebuild=(r["kind"] == "plan"))
-            batches = []
+                if (r["kind"] == "plan" or r["id"] not in self._plans) and r["id"] not in need:
+                    need.append(r["id"])
+            if need:
+                xps = [self.xpointings[i] for i in need]
+                builder = TodBatch(xps, [x[0] for x in xps], self.lpix, tuning=self.tuning, upload_stream=stream,
+                                   plan_buffers=False)
+                singles = builder.build_plans_each(stream)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                for i, sp in zip(need, singles):
+                    if i in self._plans:
+                        self._used -= self._plans.pop(i)[2]
+                    nb = max(self._plan_nbytes(i), sp.plan.numel())
+                    self._plans[i] = (sp, ev, nb)
+                    self._used += nb
+                self._errwords.append(builder.err)
+                keep.append(builder)
+            for r in admitted:
+                self._plans.move_to_end(r["id"])
             for kind in ("map2tod", "tod2map"):
                 reqs = [r for r in admitted if r["kind"] == kind]
                 if not reqs:
                     continue
-                singles = [self._plans[r["id"]] for r in reqs]
-                for _, ev, _ in singles:
+                plans = [self._plans[r["id"]] for r in reqs]
+                for ev in {id(p[1]): p[1] for p in plans}.values():
                     stream.wait_event(ev)
                 xps = [self.xpointings[r["id"]] for r in reqs]
                 if kind == "map2tod":
@@ -225,27 +250,25 @@ class PointingServer:
                         r["result"] = t
                 else:
                     tods = [r["tod"] for r in reqs]
-                b = TodBatch(xps, tods, self.lpix, tuning=self.tuning)
-                b.merge_plans([sg for sg, _, _ in singles], stream)
+                b = TodBatch(xps, tods, self.lpix, tuning=self.tuning, upload_stream=stream)
+                b.merge_plans([p[0] for p in plans], stream)
                 if kind == "map2tod":
                     b.map2tod(self.in_map, stream=stream)
                 else:
                     b.tod2map(self.out_map, stream=stream)
                 self.samples_done += b.total_samples
                 self.launches += 1
-                batches.append(b)
+                keep.append(b)
                 self._errwords.append(b.err)
             ev = torch.cuda.Event()
             ev.record(stream)
         nb = sum(self._request_nbytes(r) for r in admitted)
-        self._inflight.append((ev, admitted, nb, batches))
+        self._inflight.append((ev, admitted, nb, keep))
         return True
 
     def check(self):
         """Raises if any plan build or launch reported device error bits (waits for the GPU)."""
         torch.cuda.synchronize()
-        for single, _, _ in self._plans.values():
-            single.check()
         words = [int(w) for e in self._errwords for w in e.cpu().tolist()]
         if any(words):
             raise RuntimeError(f"PointingServer: device error bits {sorted(set(w for w in words if w))}")

@@ -191,6 +191,17 @@ int gmm_batch_plan_build(const gmm_tod_desc *descs_gpu, int32_t ntod, int64_t to
                          int32_t nxpix_global, int32_t periodic_xcoord, void *plan_buf, int64_t plan_nbytes, void *tmp,
                          int64_t tmp_nbytes, const gmm_batch_tuning *tuning, uint32_t *errword_gpu, cudaStream_t stream);
 
+/* Builds the single-TOD plans of up to 4096 TODs at once: plans_gpu[i] (device array of ntod
+ * pointers) receives TOD i's plan, laid out as gmm_batch_plan_build with ntod = 1 lays it out (sized
+ * by gmm_batch_plan_nbytes(nsamp_i/32, ...), 128-byte aligned).  One owner pass over all the TODs,
+ * one sort by (TOD, cell), one scatter; 'tmp' sized by gmm_batch_plan_each_tmp_nbytes. */
+int gmm_batch_plan_each_tmp_nbytes(int64_t total_lines, int32_t ntod, int32_t nypix_global, int32_t nxpix_global,
+                                   const gmm_batch_tuning *tuning, int64_t *tmp_nbytes);
+int gmm_batch_plan_build_each(const gmm_tod_desc *descs_gpu, int32_t ntod, int64_t total_lines, int32_t nypix_global,
+                              int32_t nxpix_global, int32_t periodic_xcoord, void *const *plans_gpu, void *tmp,
+                              int64_t tmp_nbytes, const gmm_batch_tuning *tuning, uint32_t *errword_gpu,
+                              cudaStream_t stream);
+
 /* Merges single-TOD batch plans (each built by gmm_batch_plan_build with ntod = 1) into the plan of
  * a batch whose TOD i has plans_gpu[i]: the owner words are copied with their TOD index set to i,
  * the cell bitmaps OR-ed, and the list sorted by cell (stable: the order gmm_batch_plan_build gives

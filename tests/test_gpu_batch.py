@@ -196,3 +196,30 @@ def test_autotune_small(g):
         pp = g.PointingPrePlan(x, ny, nx)
         g.map2tod(single, lmap, x, g.PointingPlan(pp, x))
         assert torch.equal(single, outs[i])
+
+
+def test_build_plans_each_matches_single_builds(g):
+    """build_plans_each (one owner pass, one sort by (TOD, cell), one scatter) gives each TOD the plan
+    a batch of that one TOD builds, and merging those plans gives the batch's own plan."""
+    import torch
+    ny, nx = 256, 512
+    rng, xps, tods = make_batch_inputs(61, ny, nx, True, ntod=7)
+    xg = [cuda(x) for x in xps]
+    tg = [cuda(t) for t in tods]
+    lp = g.LocalPixelization.make_rectangle(ny, nx, True)
+    builder = g.TodBatch(xg, tg, lp, plan_buffers=False)
+    singles = builder.build_plans_each()
+    builder.check()
+    for x, t, sp in zip(xg, tg, singles):
+        one = g.TodBatch([x], [t], lp)
+        one.build_plan()
+        one.check()
+        n = one.total_lines
+        np.testing.assert_array_equal(sp.plan[:8 * n].cpu().numpy(), one.plan[:8 * n].cpu().numpy())
+        np.testing.assert_array_equal(cellmap_bits(sp), cellmap_bits(one))
+    b = g.TodBatch(xg, tg, lp)
+    b.build_plan()
+    want = owner_words(b)
+    b.merge_plans(singles)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(owner_words(b), want)
