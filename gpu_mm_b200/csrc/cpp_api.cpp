@@ -829,10 +829,19 @@ uint expand_dynamic_map2(Array<uint> &global_ncells, LocalPixelization &lpix, co
 template<typename T>
 void local_map_to_global(const LocalPixelization &lp, Array<T> &dst, const Array<T> &src)
 {
-    // local_map_to_global.cu:11-45 (host arrays)
+    // local_map_to_global.cu:11-45.  Host arrays: the reference's loop (dst is zeroed by the caller).
+    // Device arrays (float): gmm_local_map_to_global, which also zeroes the pixels of absent cells.
     const long ny = lp.nypix_global, nx = lp.nxpix_global;
     GMM_ASSERT(dst.ndim == 3 && dst.shape[0] == 3 && dst.shape[1] == ny && dst.shape[2] == nx, "local_map_to_global");
-    GMM_ASSERT(dst.on_host() && src.on_host(), "local_map_to_global");
+    GMM_ASSERT(dst.is_fully_contiguous(), "local_map_to_global");
+    if (dst.gpu || src.gpu) {
+        GMM_ASSERT(dst.gpu && src.gpu && (sizeof(T) == sizeof(float)), "local_map_to_global");
+        check_local_map(src, lp, "local_map_to_global", true);
+        gmm_lpix v = lp.device_view();
+        throw_on_error(gmm_local_map_to_global((float *) dst.data, (const float *) src.data, &v, 0));
+        cuda_check(cudaStreamSynchronize(0), "local_map_to_global");
+        return;
+    }
     check_local_map(src, lp, "local_map_to_global", false);
     for (long iyc = 0; iyc < lp.nycells; iyc++)
         for (long ixc = 0; ixc < lp.nxcells; ixc++) {
@@ -846,6 +855,177 @@ void local_map_to_global(const LocalPixelization &lp, Array<T> &dst, const Array
                     for (long ix = 0; ix < nxx; ix++)
                         dst.data[p * ny * nx + (y0 + iy) * nx + x0 + ix] = src.data[off + p * lp.polstride + iy * lp.ystride + ix];
         }
+}
+
+// cell_broadcast.cu:17-36 / cell_reduce.cu:17-41: cell-major buffers (3*64*64 values per cell).
+// Host arrays: the reference's loops and checks.  Device arrays (float): gmm_cell_broadcast /
+// gmm_cell_reduce, after the same checks on a host copy of index_map.
+static constexpr long kCellN = 3 * 64 * 64;
+
+template<typename T>
+static void check_cell_args(const Array<T> &dst, const Array<T> &src, const Array<long> &index_map, const char *where)
+{
+    GMM_ASSERT(dst.ndim == 1 && dst.is_fully_contiguous(), where);
+    GMM_ASSERT(src.ndim == 1 && src.is_fully_contiguous(), where);
+    GMM_ASSERT(index_map.ndim == 1 && index_map.is_fully_contiguous(), where);
+    GMM_ASSERT((dst.gpu == src.gpu) && (dst.gpu == index_map.gpu), where);
+    GMM_ASSERT(!dst.gpu || (sizeof(T) == sizeof(float)), where);
+}
+
+static std::vector<long> host_index_map(const Array<long> &index_map)
+{
+    if (!index_map.gpu)
+        return std::vector<long>(index_map.data, index_map.data + index_map.size);
+    std::vector<long> h(index_map.size);
+    if (index_map.size > 0)
+        cuda_check(cudaMemcpy(h.data(), index_map.data, index_map.size * sizeof(long), cudaMemcpyDeviceToHost),
+                   "cell index_map");
+    return h;
+}
+
+template<typename T>
+void cell_broadcast(Array<T> &dst, const Array<T> &src, const Array<long> &index_map)
+{
+    check_cell_args(dst, src, index_map, "cell_broadcast");
+    const long ncells = index_map.size, nsrc = src.size;
+    GMM_ASSERT(dst.size == ncells * kCellN, "cell_broadcast");
+    const std::vector<long> im = host_index_map(index_map);
+    for (long i = 0; i < ncells; i++)
+        GMM_ASSERT((im[i] >= 0) && (im[i] * kCellN + kCellN <= nsrc), "cell_broadcast");
+    if (dst.gpu) {
+        Array<uint> err = Array<uint>::alloc_gpu({1}, true);
+        throw_on_error(gmm_cell_broadcast((float *) dst.data, (const float *) src.data, nsrc, index_map.data, ncells,
+                                          (uint32_t *) err.data, 0));
+        check_errword(err.data, 0, 0);
+        return;
+    }
+    for (long i = 0; i < ncells; i++)
+        std::memcpy(dst.data + i * kCellN, src.data + im[i] * kCellN, kCellN * sizeof(T));
+}
+
+template<typename T>
+void cell_reduce(Array<T> &dst, const Array<T> &src, const Array<long> &index_map)
+{
+    check_cell_args(dst, src, index_map, "cell_reduce");
+    const long ncells = index_map.size, ndst = dst.size;
+    GMM_ASSERT(src.size == ncells * kCellN, "cell_reduce");
+    const std::vector<long> im = host_index_map(index_map);
+    for (long i = 0; i < ncells; i++)
+        GMM_ASSERT((im[i] >= 0) && (im[i] * kCellN + kCellN <= ndst), "cell_reduce");
+    if (dst.gpu) {
+        Array<uint> err = Array<uint>::alloc_gpu({1}, true);
+        throw_on_error(gmm_cell_reduce((float *) dst.data, ndst, (const float *) src.data, index_map.data, ncells,
+                                       (uint32_t *) err.data, 0));
+        check_errword(err.data, 0, 0);
+        return;
+    }
+    std::memset(dst.data, 0, ndst * sizeof(T));
+    for (long i = 0; i < ncells; i++) {
+        T *d = dst.data + im[i] * kCellN;
+        const T *q = src.data + i * kCellN;
+        for (long j = 0; j < kCellN; j++)
+            d[j] += q[j];
+    }
+}
+
+template void cell_broadcast<float>(Array<float> &, const Array<float> &, const Array<long> &);
+template void cell_broadcast<double>(Array<double> &, const Array<double> &, const Array<long> &);
+template void cell_reduce<float>(Array<float> &, const Array<float> &, const Array<long> &);
+template void cell_reduce<double>(Array<double> &, const Array<double> &, const Array<long> &);
+
+// ---- TOD preprocessing (deglitching.cu, cuts.cu, misc.cu): device arrays; index-map entries out of
+// range raise after the call.
+
+static void check_range_word(const Array<uint> &w, const char *where)
+{
+    uint h = 0;
+    cuda_check(cudaMemcpy(&h, w.data, sizeof(uint), cudaMemcpyDeviceToHost), where);
+    if (h)
+        throw std::runtime_error(std::string(where) + ": index map entries out of range");
+}
+
+static void check_dev(bool gpu_contig, const char *where, const char *name)
+{
+    if (!gpu_contig)
+        throw std::runtime_error(std::string(where) + ": '" + name + "' must be a contiguous device array");
+}
+
+void get_border_means(Array<float> &out, const Array<float> &signal, const Array<int> &index_map)
+{
+    const char *where = "get_border_means";
+    check_dev(out.gpu && out.is_fully_contiguous(), where, "out");
+    check_dev(signal.gpu && signal.is_fully_contiguous(), where, "signal");
+    check_dev(index_map.gpu && index_map.is_fully_contiguous(), where, "index_map");
+    GMM_ASSERT(out.ndim == 2 && out.shape[1] == 2 && signal.ndim == 2, where);
+    GMM_ASSERT(index_map.ndim == 2 && index_map.shape[1] == 5 && index_map.shape[0] == out.shape[0], where);
+    Array<uint> w = Array<uint>::alloc_gpu({1}, true);
+    throw_on_error(gmm_get_border_means(out.data, signal.data, signal.shape[0], signal.shape[1], index_map.data,
+                                        out.shape[0], (uint32_t *) w.data, 0));
+    check_range_word(w, where);
+}
+
+void deglitch(Array<float> &signal, const Array<float> &bvals, const Array<int> &index_map2)
+{
+    const char *where = "deglitch";
+    check_dev(signal.gpu && signal.is_fully_contiguous(), where, "signal");
+    check_dev(bvals.gpu && bvals.is_fully_contiguous(), where, "bvals");
+    check_dev(index_map2.gpu && index_map2.is_fully_contiguous(), where, "index_map2");
+    GMM_ASSERT(signal.ndim == 2 && bvals.ndim == 2 && bvals.shape[1] == 2, where);
+    GMM_ASSERT(index_map2.ndim == 2 && index_map2.shape[1] == 4 && index_map2.shape[0] == bvals.shape[0], where);
+    Array<float> cumj = Array<float>::alloc_gpu({std::max<long>(bvals.shape[0], 1)});
+    Array<uint> w = Array<uint>::alloc_gpu({1}, true);
+    throw_on_error(gmm_deglitch(signal.data, signal.shape[0], signal.shape[1], bvals.data, index_map2.data,
+                                bvals.shape[0], cumj.data, (uint32_t *) w.data, 0));
+    check_range_word(w, where);
+}
+
+void deglitch(Array<float> &signal, const Array<float> &bvals, const Array<float> &cumj, const Array<int> &index_map2)
+{
+    const char *where = "deglitch";
+    check_dev(signal.gpu && signal.is_fully_contiguous(), where, "signal");
+    check_dev(bvals.gpu && bvals.is_fully_contiguous(), where, "bvals");
+    check_dev(cumj.gpu && cumj.is_fully_contiguous(), where, "cumj");
+    check_dev(index_map2.gpu && index_map2.is_fully_contiguous(), where, "index_map2");
+    GMM_ASSERT(signal.ndim == 2 && bvals.ndim == 2 && bvals.shape[1] == 2 && cumj.ndim == 1, where);
+    GMM_ASSERT(cumj.shape[0] == bvals.shape[0], where);
+    GMM_ASSERT(index_map2.ndim == 2 && index_map2.shape[1] == 4 && index_map2.shape[0] == bvals.shape[0], where);
+    Array<uint> w = Array<uint>::alloc_gpu({1}, true);
+    throw_on_error(gmm_deglitch_cumj(signal.data, signal.shape[0], signal.shape[1], bvals.data, cumj.data,
+                                     index_map2.data, bvals.shape[0], (uint32_t *) w.data, 0));
+    check_range_word(w, where);
+}
+
+void tod_ranges(int mode, Array<float> &tod, Array<float> &rdata, const Array<int> &ostart, const Array<int> &det,
+                const Array<int> &istart, const Array<int> &len)
+{
+    const char *where = (mode == 0) ? "extract_ranges" : (mode == 1) ? "insert_ranges" : "clear_ranges";
+    check_dev(tod.gpu && tod.is_fully_contiguous() && tod.ndim == 2, where, "tod");
+    check_dev(det.gpu && istart.gpu && len.gpu, where, "dets/starts/lens");
+    GMM_ASSERT(det.size == istart.size && det.size == len.size, where);
+    if (mode != 2) {
+        check_dev(rdata.gpu && rdata.is_fully_contiguous(), where, "junk");
+        check_dev(ostart.gpu && ostart.size == det.size, where, "offs");
+    }
+    Array<uint> w = Array<uint>::alloc_gpu({1}, true);
+    int rc;
+    if (mode == 0)
+        rc = gmm_extract_ranges(tod.data, tod.shape[0], tod.shape[1], rdata.data, rdata.size, ostart.data, det.data,
+                                istart.data, len.data, det.size, (uint32_t *) w.data, 0);
+    else if (mode == 1)
+        rc = gmm_insert_ranges(tod.data, tod.shape[0], tod.shape[1], rdata.data, rdata.size, ostart.data, det.data,
+                               istart.data, len.data, det.size, (uint32_t *) w.data, 0);
+    else
+        rc = gmm_clear_ranges(tod.data, tod.shape[0], tod.shape[1], det.data, istart.data, len.data, det.size,
+                              (uint32_t *) w.data, 0);
+    throw_on_error(rc);
+    check_range_word(w, where);
+}
+
+void clip(Array<float> &arr, float vmin, float vmax)
+{
+    check_dev(arr.gpu && arr.is_fully_contiguous(), "clip", "arr");
+    throw_on_error(gmm_clip(arr.data, arr.size, vmin, vmax, 0));
+    cuda_check(cudaStreamSynchronize(0), "clip");
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -20,6 +20,7 @@ namespace {
 template<typename T> struct TypeCodes;
 template<> struct TypeCodes<float> { static bool ok(const std::string &t) { return t == "<f4" || t == "=f4"; } };
 template<> struct TypeCodes<double> { static bool ok(const std::string &t) { return t == "<f8" || t == "=f8"; } };
+template<> struct TypeCodes<int> { static bool ok(const std::string &t) { return t == "<i4" || t == "=i4"; } };
 template<> struct TypeCodes<long> { static bool ok(const std::string &t) { return t == "<i8" || t == "=i8"; } };
 template<> struct TypeCodes<uint> {
     static bool ok(const std::string &t) { return t == "<u4" || t == "<i4" || t == "=u4" || t == "=i4"; }
@@ -520,4 +521,62 @@ PYBIND11_MODULE(gpu_mm_pybind11, m)
               local_map_to_global<float>(lpix, d, s);
           },
           py::arg("local_pixelization"), py::arg("dst"), py::arg("src"));
+
+    // TOD preprocessing on device arrays (gpu_mm_pybind11.cu get_border_means / deglitch and the
+    // ctypes entry points extract_ranges / insert_ranges / clear_ranges / clip of gpu_mm.py:1579-1607).
+    m.def("get_border_means", [](py::object out, py::object signal, py::object index_map) {
+        Array<float> o = to_array<float>(out, "out"), sg = to_array<float>(signal, "signal");
+        Array<int> im = to_array<int>(index_map, "index_map");
+        py::gil_scoped_release rel;
+        get_border_means(o, sg, im);
+    }, py::arg("out"), py::arg("signal"), py::arg("index_map"));
+    // deglitch(signal, bvals, cumj, index_map2) as in the reference; cumj=None computes it on the device.
+    m.def("deglitch", [](py::object signal, py::object bvals, py::object cumj, py::object index_map2) {
+        Array<float> sg = to_array<float>(signal, "signal"), bv = to_array<float>(bvals, "bvals"), cj;
+        Array<int> im = to_array<int>(index_map2, "index_map2");
+        const bool given = !cumj.is_none();
+        if (given)
+            cj = to_array<float>(cumj, "cumj");
+        py::gil_scoped_release rel;
+        if (given)
+            deglitch(sg, bv, cj, im);
+        else
+            deglitch(sg, bv, im);
+    }, py::arg("signal"), py::arg("bvals"), py::arg("cumj"), py::arg("index_map2"));
+    m.def("_ranges", [](int mode, py::object tod, py::object rdata, py::object ostart, py::object det,
+                        py::object istart, py::object len) {
+        Array<float> t = to_array<float>(tod, "tod"), r;
+        Array<int> o, d = to_array<int>(det, "dets"), s0 = to_array<int>(istart, "starts"), n = to_array<int>(len, "lens");
+        if (mode != 2) {
+            r = to_array<float>(rdata, "junk");
+            o = to_array<int>(ostart, "offs");
+        }
+        py::gil_scoped_release rel;
+        tod_ranges(mode, t, r, o, d, s0, n);
+    });
+    m.def("clip", [](py::object arr, float vmin, float vmax) {
+        Array<float> a = to_array<float>(arr, "arr");
+        py::gil_scoped_release rel;
+        clip(a, vmin, vmax);
+    }, py::arg("arr"), py::arg("vmin"), py::arg("vmax"));
+
+    // gpu_mm_pybind11.cu:195-200 (float32 maps): host (numpy) or device (CUDA) cell-major buffers.
+    m.def("cell_broadcast",
+          [](py::object dst, py::object src, py::object index_map) {
+              Array<float> d = to_array<float>(dst, "dst");
+              Array<float> s = to_array<float>(src, "src");
+              Array<long> im = to_array<long>(index_map, "index_map");
+              py::gil_scoped_release rel;
+              cell_broadcast<float>(d, s, im);
+          },
+          py::arg("dst"), py::arg("src"), py::arg("index_map"));
+    m.def("cell_reduce",
+          [](py::object dst, py::object src, py::object index_map) {
+              Array<float> d = to_array<float>(dst, "dst");
+              Array<float> s = to_array<float>(src, "src");
+              Array<long> im = to_array<long>(index_map, "index_map");
+              py::gil_scoped_release rel;
+              cell_reduce<float>(d, s, im);
+          },
+          py::arg("dst"), py::arg("src"), py::arg("index_map"));
 }

@@ -152,6 +152,73 @@ def tod2map_f64(map64, local_pixelization, tod, xpointing, plan, partial_pixeliz
 
 
 ####################################################################################################
+#
+# TOD preprocessing (gpu_mm.py:1420-1607 of the reference): deglitching, cut ranges, clip.
+# Device arrays are torch CUDA tensors (float32 data, int32 index maps).
+
+
+def get_border_means(out, signal, index_map):
+    """Deglitching means on the GPU (gpu_mm.py:1423-1458): out[r] = (mean of signal[di, b00:b01],
+    mean of signal[di, b10:b11]) for index_map[r] = (di, b00, b01, b10, b11); an empty range takes
+    the other range's mean.  out (R,2) float32, signal (ndet,nt) float32, index_map (R,5) int32."""
+    gpu_mm_pybind11.get_border_means(out, signal, index_map)
+
+
+def deglitch(signal, bvals, index_map2):
+    """Subtracts deglitching offsets on the GPU (gpu_mm.py:1461-1501), in place: with
+    cumj = cumsum(bvals[:,1] - bvals[:,0]) and index_map2[r] = (di, r0, t1, t2),
+    signal[di,t1:t2] = bvals[r,1] - dc and signal[di,t2:t3] -= dc, dc = cumj[r] - cumj[r0-1], t3 the
+    next range's t1 if it has the same detector, else ntod."""
+    gpu_mm_pybind11.deglitch(signal, bvals, None, index_map2)
+
+
+def reference_get_border_means(signal, index_map):
+    """CPU restatement of get_border_means() for testing (gpu_mm.py:1504-1529)."""
+    R = len(index_map)
+    bvals = np.zeros((R, 2), signal.dtype)
+    for ri in range(R):
+        di, b00, b01, b10, b11 = (int(v) for v in index_map[ri])
+        a, b = signal[di, b00:b01], signal[di, b10:b11]
+        v1 = np.mean(a) if a.size else 0.0
+        v2 = np.mean(b) if b.size else 0.0
+        bvals[ri] = (v1 if a.size else v2, v2 if b.size else v1)
+    return bvals
+
+
+def reference_deglitch(signal, bvals, index_map2):
+    """CPU restatement of deglitch() for testing (gpu_mm.py:1532-1563); modifies 'signal'."""
+    R, nsamp = len(index_map2), signal.shape[1]
+    cumj = np.cumsum(bvals[:, 1] - bvals[:, 0])
+    for ri in range(R):
+        di, r0, t1, t2 = (int(v) for v in index_map2[ri])
+        dcumj = cumj[ri] - (cumj[r0 - 1] if r0 > 0 else 0)
+        last = not ((ri < R - 1) and (index_map2[ri + 1, 0] == di))
+        t3 = nsamp if last else int(index_map2[ri + 1, 2])
+        signal[di, t1:t2] = bvals[ri, 1] - dcumj
+        signal[di, t2:t3] -= dcumj
+
+
+def extract_ranges(tod, junk, offs, dets, starts, lens):
+    """junk[offs[r] : offs[r]+lens[r]] = tod[dets[r], starts[r] : starts[r]+lens[r]] (gpu_mm.py:1593)."""
+    gpu_mm_pybind11._ranges(0, tod, junk, offs, dets, starts, lens)
+
+
+def insert_ranges(tod, junk, offs, dets, starts, lens):
+    """tod[dets[r], starts[r] : starts[r]+lens[r]] = junk[offs[r] : offs[r]+lens[r]] (gpu_mm.py:1590)."""
+    gpu_mm_pybind11._ranges(1, tod, junk, offs, dets, starts, lens)
+
+
+def clear_ranges(tod, dets, starts, lens):
+    """tod[dets[r], starts[r] : starts[r]+lens[r]] = 0 (gpu_mm.py:1596)."""
+    gpu_mm_pybind11._ranges(2, tod, None, None, dets, starts, lens)
+
+
+def clip(arr, vmin, vmax):
+    """In-place clip of a float32 CUDA array (gpu_mm.py:1602-1607)."""
+    gpu_mm_pybind11.clip(arr, float(vmin), float(vmax))
+
+
+####################################################################################################
 
 
 def _to_numpy_int64(a):
@@ -249,9 +316,16 @@ class LocalMap:
         self.dtype = np.float32
         self.arr = arr
 
-    def to_global(self):
+    def to_global(self, on_device=False):
         """The map as a numpy array of shape (3, nypix_global, nxpix_global); pixels outside the
-        local map are zero (gpu_mm.py:565-580)."""
+        local map are zero (gpu_mm.py:565-580).  on_device=True (GPU maps): a CUDA tensor, built by a
+        kernel without a round trip through the host."""
+        if on_device:
+            if not (isinstance(self.arr, torch.Tensor) and self.arr.is_cuda):
+                raise RuntimeError("LocalMap.to_global(on_device=True): the map is not on the GPU")
+            dst = torch.empty((3, self.nypix_global, self.nxpix_global), dtype=torch.float32, device="cuda")
+            gpu_mm_pybind11.local_map_to_global(self.pixelization, dst, self.arr)
+            return dst
         src = self.arr.detach().cpu().numpy() if isinstance(self.arr, torch.Tensor) else self.arr
         src = np.ascontiguousarray(src.reshape(-1))
         dst = np.zeros((3, self.nypix_global, self.nxpix_global), dtype=np.float32)

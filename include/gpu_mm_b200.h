@@ -152,6 +152,53 @@ int gmm_planned_tod2map(float *local_map, const float *tod, const float *xpointi
                         const gmm_preplan_info *info, const void *plan_buf, int32_t partial_pixelization,
                         uint32_t *errword_gpu, cudaStream_t stream);
 
+/* Replaces local_map_to_global (gpu_mm.hpp:226-228, local_map_to_global.cu:12-44) for device arrays:
+ * dst is the dense (3, nypix_global, nxpix_global) global map (zeroed outside the local cells). */
+int gmm_local_map_to_global(float *dst, const float *src, const gmm_lpix *lpix, cudaStream_t stream);
+
+/* Replace cell_broadcast / cell_reduce (gpu_mm.hpp:230-236, cell_broadcast.cu, cell_reduce.cu) for
+ * device arrays of cell-major buffers (3*64*64 floats per cell): broadcast dst cell i = src cell
+ * index_map[i]; reduce dst = 0, then dst cell index_map[i] += src cell i.  index_map is a device
+ * int64 array of ncells entries; out-of-range entries are skipped and set bit 1 of the error word. */
+int gmm_cell_broadcast(float *dst, const float *src, int64_t nsrc, const int64_t *index_map_gpu, int64_t ncells,
+                       uint32_t *errword_gpu, cudaStream_t stream);
+int gmm_cell_reduce(float *dst, int64_t ndst, const float *src, const int64_t *index_map_gpu, int64_t ncells,
+                    uint32_t *errword_gpu, cudaStream_t stream);
+
+/* ---- TOD preprocessing (the reference's deglitching.cu, cuts.cu, misc.cu), device arrays.
+ * Every index read from an index map is checked against the arrays' extents; entries out of range
+ * are skipped and set bit 1 of the error word (zeroed by each call). */
+
+/* get_border_means (deglitching.cu:99-141): out[r] = (mean signal[di, b00:b01], mean signal[di, b10:b11])
+ * for index_map[r] = (di, b00, b01, b10, b11); an empty range takes the other's mean.  signal is
+ * (ndet, nt), out (R, 2), index_map (R, 5) int32. */
+int gmm_get_border_means(float *out, const float *signal, int64_t ndet, int64_t nt, const int32_t *index_map,
+                         int64_t R, uint32_t *errword_gpu, cudaStream_t stream);
+
+/* deglitch (deglitching.cu:180-210, gpu_mm.py:1461-1501): cumj = cumsum(bvals[:,1] - bvals[:,0]) into
+ * the caller's scratch 'cumj' (R floats), then per range r = (di, r0, t1, t2) of index_map2 (R, 4):
+ * signal[di, t1:t2] = bvals[r,1] - dc and signal[di, t2:t3] -= dc, with dc = cumj[r] - cumj[r0-1]. */
+int gmm_deglitch(float *signal, int64_t ndet, int64_t nt, const float *bvals, const int32_t *index_map2, int64_t R,
+                 float *cumj, uint32_t *errword_gpu, cudaStream_t stream);
+/* deglitch with the jump cumsum given by the caller (the reference's pybind deglitch(signal, bvals,
+   cumj, index_map2), deglitching.cu:180-210): cumj (R,) float32 on the device. */
+int gmm_deglitch_cumj(float *signal, int64_t ndet, int64_t nt, const float *bvals, const float *cumj,
+                      const int32_t *index_map2, int64_t R, uint32_t *errword, cudaStream_t stream);
+
+/* extract_ranges / insert_ranges / clear_ranges (cuts.cu:38-55): range r is
+ * tod[det[r], istart[r] : istart[r] + len[r]] of a (ndet, nsamp) TOD, kept in rdata[ostart[r]:]. */
+int gmm_extract_ranges(const float *tod, int64_t ndet, int64_t nsamp, float *rdata, int64_t nrdata,
+                       const int32_t *ostart, const int32_t *det, const int32_t *istart, const int32_t *len,
+                       int64_t nrange, uint32_t *errword_gpu, cudaStream_t stream);
+int gmm_insert_ranges(float *tod, int64_t ndet, int64_t nsamp, const float *rdata, int64_t nrdata,
+                      const int32_t *ostart, const int32_t *det, const int32_t *istart, const int32_t *len,
+                      int64_t nrange, uint32_t *errword_gpu, cudaStream_t stream);
+int gmm_clear_ranges(float *tod, int64_t ndet, int64_t nsamp, const int32_t *det, const int32_t *istart,
+                     const int32_t *len, int64_t nrange, uint32_t *errword_gpu, cudaStream_t stream);
+
+/* clip (misc.cu:8-19): arr = max(vmin, min(vmax, arr)) in place. */
+int gmm_clip(float *arr, int64_t n, float vmin, float vmax, cudaStream_t stream);
+
 /* ---- Batches of TODs (no counterpart in the reference, which plans and applies one TOD per call).
  *
  * A batch is up to 65535 TODs, each with its own xpointing [3][nsamp] and TOD [nsamp] (16-byte

@@ -228,6 +228,22 @@ uint expand_dynamic_map2(Array<uint> &global_ncells, LocalPixelization &local_pi
 template<typename T>
 void local_map_to_global(const LocalPixelization &local_pixelization, Array<T> &dst, const Array<T> &src);
 
+// TOD preprocessing on device arrays (deglitching.cu:99-210, cuts.cu:38-55, misc.cu:8-19); index
+// maps are int32.  deglitch without 'cumj' computes the jump cumsum on the device.  tod_ranges mode: 0 extract (rdata <- tod), 1 insert (tod <- rdata), 2 clear.
+void get_border_means(Array<float> &out, const Array<float> &signal, const Array<int> &index_map);
+void deglitch(Array<float> &signal, const Array<float> &bvals, const Array<int> &index_map2);
+void deglitch(Array<float> &signal, const Array<float> &bvals, const Array<float> &cumj, const Array<int> &index_map2);
+void tod_ranges(int mode, Array<float> &tod, Array<float> &rdata, const Array<int> &ostart, const Array<int> &det,
+                const Array<int> &istart, const Array<int> &len);
+void clip(Array<float> &arr, float vmin, float vmax);
+
+// Cell-major buffer exchange (cell_broadcast.cu, cell_reduce.cu): dst cell i = src cell index_map[i];
+// dst cell index_map[i] += src cell i (dst zeroed first).  Host arrays, or device arrays (float).
+template<typename T>
+void cell_broadcast(Array<T> &dst, const Array<T> &src, const Array<long> &index_map);
+template<typename T>
+void cell_reduce(Array<T> &dst, const Array<T> &src, const Array<long> &index_map);
+
 // Argument checks (check_arguments.cu).
 void check_nsamp(long nsamp, const char *where);
 void check_nypix_global(long nypix_global, const char *where);
