@@ -27,6 +27,7 @@ from .gpu_mm import (map2tod, tod2map, LocalPixelization, LocalMap, DynamicMap, 
 from .batch import TodBatch  # noqa: E402,F401
 from . import autotune  # noqa: E402,F401
 from .serving import PointingServer  # noqa: E402,F401
+from .host_pipeline import HostPipeline  # noqa: E402,F401
 
 __all__ = ["map2tod", "tod2map", "LocalPixelization", "LocalMap", "DynamicMap", "PointingPrePlan",
            "PointingPlan", "read_xpointing_npzfile", "mm_dtype", "gpu_mm_pybind11", "tod2map_compensated",
