@@ -522,6 +522,20 @@ def serving_study(rate=200.0, duration_s=2.5, ntod_pool=128, seed=5):
 # ------------------------------------------------------------------------------------------------
 
 
+def replica_throughput(local_ms, nsamp_per_rank, world, device):
+    """Whole-job throughput of N independent replicas: every rank processed nsamp_per_rank samples,
+    and the job took as long as its slowest rank (the max of the ranks' device-timed milliseconds,
+    taken with one all-reduce).  Returns (max ms, Gsamples/s)."""
+    import torch
+    import torch.distributed as dist
+    ms = float(local_ms)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, world * nsamp_per_rank / (ms * 1e-3) / 1e9
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -545,11 +559,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replica_throughput(x, 0, world, "cuda")[0]
 
     import gpu_mm_b200 as g
     from gpu_mm_b200 import synthetic
