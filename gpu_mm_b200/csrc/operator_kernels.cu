@@ -20,6 +20,10 @@
 //  * tod2map accumulates into the tile with shared-memory atomics.  Adjacent samples usually hit
 //    the same pixel, so lane i adds T, Q and U in an order rotated by i mod 3: in one atomic
 //    instruction, neighbouring lanes then target different words.
+//  * With the plain float flush, only the upper row of a sample's 2x2 footprint goes into the tile;
+//    the lower row is added straight into the map with fire-and-forget reductions, which the L2
+//    executes.  Shared-memory float atomics are compare-and-swap loops on this GPU and were the
+//    bound; splitting the footprint puts half of the work on each unit, which run in parallel.
 //  * xpointing and TOD are streamed with evict-first loads/stores so that the map and plan stay in
 //    L2; each warp keeps UNR cache lines in flight.
 #include <algorithm>
@@ -325,13 +329,18 @@ __device__ __forceinline__ float m2t_sample(const OpArgs &a, const float *tile, 
     return bilinear(L.dy, L.dx, e00, e01, e10, e11);
 }
 
-// One sample of tod2map: exact locate with error bits, then 12 shared-memory atomics into the staged
+// One sample of tod2map: exact locate with error bits, then shared-memory atomics into the staged
 // tile or, if the footprint is not inside it, global atomics.  o0..o2 are this lane's polarisation
 // plane offsets in rotated order and 'rot' selects the matching rotation of (t, q, u): in one atomic
 // instruction, lanes on the same pixel then target different words.
+//
+// Flush mode kFlushF32 splits the footprint: its upper row (6 atomics) goes into the tile, its lower
+// row (6 reductions) straight into the map at the offsets of the tile's offset table 'tab'.  The
+// other flush modes keep every partial in the tile, because their flush is what adds precision.
 template<bool RESP, bool PERIODIC, int FLUSH = kFlushF32>
-__device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const Tile &T, float y, float x, float al,
-                                           float tv, uint32_t s, int rot, int o0, int o1, int o2, uint32_t &err)
+__device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const int64_t *tab, const Tile &T, float y,
+                                           float x, float al, float tv, uint32_t s, int rot, int o0, int o1, int o2,
+                                           uint32_t &err)
 {
     Located L;
     err |= locate(y, x, a.ny, a.nx, PERIODIC, L);
@@ -364,6 +373,27 @@ __device__ __forceinline__ void t2m_sample(const OpArgs &a, float *tile, const T
         atomicAdd(p0 + 1, w01 * v0);
         atomicAdd(p1 + 1, w01 * v1);
         atomicAdd(p2 + 1, w01 * v2);
+        if constexpr (FLUSH == kFlushF32) {
+            // Lower row: tile row ry + 1 (inside the tile), its two columns' map offsets from 'tab'.
+            // An absent cell (offset -1) is skipped, as the flush skips it.
+            const int64_t *tb = tab + ((ry + 1) >> 6) * TX + rx;
+            const int64_t roff = (int64_t) ((ry + 1) & 63) * a.ystride;
+            const int64_t b0 = tb[0], b1 = tb[1];
+            const int64_t ps = a.polstride;
+            if (b0 >= 0) {
+                float *g = a.out + b0 + roff;
+                atomicAdd(g, w10 * t);
+                atomicAdd(g + ps, w10 * q);
+                atomicAdd(g + 2 * ps, w10 * u);
+            }
+            if (b1 >= 0) {
+                float *g = a.out + b1 + roff;
+                atomicAdd(g, w11 * t);
+                atomicAdd(g + ps, w11 * q);
+                atomicAdd(g + 2 * ps, w11 * u);
+            }
+            return;
+        }
         atomicAdd(p0 + TS, w10 * v0);
         atomicAdd(p1 + TS, w10 * v1);
         atomicAdd(p2 + TS, w10 * v2);
@@ -559,11 +589,12 @@ planned_kernel(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner, 
                 for (int u = 0; u < UNR; u++) {
                     if (!ok[u])
                         continue;
-                    // tod2map runs the general path for every sample: its time goes to the shared
+                    // tod2map runs the general path for every sample: its time goes to the
                     // atomics, and the vote below would keep the compiler from overlapping one
                     // sample's arithmetic with the previous sample's atomics (measured slower).
                     if constexpr (TOD2MAP) {
-                        t2m_sample<RESP, PERIODIC, FLUSH>(a, tile, T, y[u], x[u], al[u], tv[u], s[u], rot, o0, o1, o2, err);
+                        t2m_sample<RESP, PERIODIC, FLUSH>(a, tile, s_tab, T, y[u], x[u], al[u], tv[u], s[u], rot, o0, o1, o2,
+                                                          err);
                     } else {
                         // map2tod: fast path when every lane's sample passes tile_sample (the line
                         // is warp-uniform), else the general path.
