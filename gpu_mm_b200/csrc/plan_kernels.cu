@@ -42,6 +42,11 @@ __device__ __forceinline__ void analyse_line(float y, float x, int ny, int nx, b
     line_slot_masks(ls.slots, ls.amask);
 }
 
+// Each planner block is counted by kPreplanSplit CTAs (a contiguous quarter of its lines each), which
+// add their counts into the block's word: up to 1024 planner blocks would otherwise fill the GPU
+// unevenly (about 1.4 waves).  nmt_out and err_out must be zero on entry.
+constexpr int kPreplanSplit = 4;
+
 __global__ void __launch_bounds__(kPlanWarps * 32)
 preplan_count_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bool periodic,
                      int64_t nclpb, uint32_t *__restrict__ nmt_out, uint32_t *__restrict__ err_out)
@@ -50,8 +55,11 @@ preplan_count_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx
     __shared__ uint32_t s_e[kPlanWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t ncl = nsamp >> 5;
-    const int64_t l0 = blockIdx.x * nclpb;
-    const int64_t l1 = min(ncl, l0 + nclpb);
+    const int64_t pb = blockIdx.x / kPreplanSplit, part = blockIdx.x % kPreplanSplit;
+    const int64_t b0 = pb * nclpb, b1 = min(ncl, b0 + nclpb);
+    const int64_t chunk = (nclpb + kPreplanSplit - 1) / kPreplanSplit;
+    const int64_t l0 = b0 + part * chunk;
+    const int64_t l1 = min(b1, l0 + chunk);
     uint32_t n = 0, err = 0;
 
     for (int64_t lb = l0 + warp * kLinesPerWarp; lb < l1; lb += kRoundLines) {
@@ -86,8 +94,10 @@ preplan_count_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx
         nn = __reduce_add_sync(kFullMask, nn);
         ee = __reduce_or_sync(kFullMask, ee);
         if (lane == 0) {
-            nmt_out[blockIdx.x] = nn;
-            err_out[blockIdx.x] = ee;
+            if (nn)
+                atomicAdd(nmt_out + pb, nn);
+            if (ee)
+                atomicOr(err_out + pb, ee);
         }
     }
 }
@@ -141,7 +151,7 @@ preplan_finalize_kernel(uint32_t *__restrict__ nmt, uint32_t *__restrict__ err, 
 // Plan emit: deterministic, cache-line-major mt words per planner block, plus one owner word per
 // cache line (the line's lowest cell), which the operators use to visit each line exactly once.
 
-__global__ void __launch_bounds__(kPlanWarps * 32)
+__global__ void __launch_bounds__(kPlanWarps * 32, 4)
 plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
                  const uint32_t *__restrict__ nmt_cumsum, uint64_t *__restrict__ mt_out,
                  uint64_t *__restrict__ owner_out, uint32_t *__restrict__ errflags)
@@ -151,6 +161,9 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
     __shared__ int s_fill[kRoundLines];
     __shared__ int s_ring[4];
     __shared__ int64_t s_base;
+    // Slot analysis of each line of the round, kept here between the phases instead of in registers.
+    __shared__ int s_slots[kRoundLines][6][32];
+    __shared__ unsigned s_amask[kRoundLines][6];
     __shared__ uint32_t s_err[kPlanWarps];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -171,7 +184,6 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
 
     for (int64_t r0 = l0; r0 < l1; r0 += kRoundLines) {
         // Phase 1: analyse this warp's lines of the round.
-        LineSlots ls[kLinesPerWarp];
         float y[kLinesPerWarp], x[kLinesPerWarp];
         const int64_t lw = r0 + warp * kLinesPerWarp;
 #pragma unroll
@@ -183,20 +195,29 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
 #pragma unroll
         for (int j = 0; j < kLinesPerWarp; j++) {
             int cnt = 0;
+            LineSlots ls;
             if (lw + j < l1) {
-                analyse_line(y[j], x[j], ny, nx, periodic, ls[j], err);
+                analyse_line(y[j], x[j], ny, nx, periodic, ls, err);
 #pragma unroll
                 for (int k = 0; k < 6; k++)
-                    cnt += __popc(ls[j].amask[k]);
+                    cnt += __popc(ls.amask[k]);
             } else {
 #pragma unroll
                 for (int k = 0; k < 6; k++) {
-                    ls[j].amask[k] = 0;
-                    ls[j].slots[k] = -1;
+                    ls.amask[k] = 0;
+                    ls.slots[k] = -1;
                 }
             }
-            if (lane == 0)
-                s_cnt[warp * kLinesPerWarp + j] = cnt;
+            const int li = warp * kLinesPerWarp + j;
+#pragma unroll
+            for (int k = 0; k < 6; k++)
+                s_slots[li][k][lane] = ls.slots[k];
+            if (lane == 0) {
+#pragma unroll
+                for (int k = 0; k < 6; k++)
+                    s_amask[li][k] = ls.amask[k];
+                s_cnt[li] = cnt;
+            }
         }
         __syncthreads();
 
@@ -243,15 +264,16 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
             unsigned minc = 0xffffffffu;
 #pragma unroll
             for (int k = 0; k < 6; k++) {
-                const unsigned am = ls[j].amask[k];
+                const unsigned am = s_amask[li][k];
                 if ((am >> lane) & 1u) {
                     const int rank = __popc(am & lt);
                     const int64_t p = base + pos + rank;
                     const bool zflag = mflag && (rank == 0) && (fill + pos < 32);
-                    const uint64_t word = (uint64_t) (unsigned) ls[j].slots[k] | hi | (zflag ? kZflag : 0ull);
+                    const int slot = s_slots[li][k][lane];
+                    const uint64_t word = (uint64_t) (unsigned) slot | hi | (zflag ? kZflag : 0ull);
                     if (p < nmax)
                         out[p] = word;
-                    minc = min(minc, (unsigned) ls[j].slots[k]);
+                    minc = min(minc, (unsigned) slot);
                 }
                 pos += __popc(am);
             }
@@ -793,7 +815,13 @@ cudaError_t launch_plans_each(const gmm_tod_desc *descs, int ntod, int64_t total
 cudaError_t launch_preplan(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
                            int nblocks, uint32_t *nmt, uint32_t *err, cudaStream_t stream)
 {
-    preplan_count_kernel<<<nblocks, kPlanWarps * 32, 0, stream>>>(xp, nsamp, ny, nx, periodic, nclpb, nmt, err);
+    cudaError_t e = cudaMemsetAsync(nmt, 0, (size_t) nblocks * sizeof(uint32_t), stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(err, 0, (size_t) nblocks * sizeof(uint32_t), stream);
+    if (e != cudaSuccess)
+        return e;
+    preplan_count_kernel<<<(unsigned) nblocks * kPreplanSplit, kPlanWarps * 32, 0, stream>>>(xp, nsamp, ny, nx,
+                                                                                           periodic, nclpb, nmt, err);
     preplan_finalize_kernel<<<1, 1024, 0, stream>>>(nmt, err, nblocks);
     return cudaGetLastError();
 }
