@@ -753,6 +753,77 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
 // Unplanned operators (map2tod_unplanned.cu:17-71, tod2map_unplanned.cu:17-66): one pass over the
 // samples, map accesses straight to global memory.  Four consecutive samples per thread with
 // 16-byte loads when the arrays are aligned.
+//
+// tod2map accumulates a thread's consecutive samples in a window of two adjacent map columns (rows
+// iy, iy+1, planes T, Q, U) held in registers; a column goes to the map (one global reduction per
+// pixel and plane) when the window moves past it.  A scan crosses a column every 1/speed samples,
+// so the L2 performs about half the reductions of one per sample and neighbour, which bound this
+// kernel.  Every pixel a sample touches is flushed once, so the not-in-pixelization check is the
+// per-sample one.
+
+struct ColumnWindow {
+    int iy, cx;             // rows iy, iy + 1 and columns cx, cx + 1; cx < 0: empty
+    float c0[6], c1[6];     // column cx and cx + 1: [row * 3 + plane]
+};
+
+__device__ __forceinline__ void window_flush(const OpArgs &a, int iy, int ix, float *v, uint32_t &err)
+{
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int64_t off = global_pixel_offset(iy + r, ix, a);
+        if (off >= 0) {
+            atomicAdd(a.out + off, v[3 * r]);
+            atomicAdd(a.out + off + a.polstride, v[3 * r + 1]);
+            atomicAdd(a.out + off + 2 * a.polstride, v[3 * r + 2]);
+        } else {
+            err |= a.partial ? 0u : kErrNotInPixelization;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+        v[k] = 0.0f;
+}
+
+// Adds one located sample (t, q, u = its T, Q, U factors) into the window, moving or restarting
+// the window as needed; samples whose x neighbours wrap around the map go straight to the map.
+__device__ __forceinline__ void window_add(const OpArgs &a, ColumnWindow &W, const Located &L, float t, float q,
+                                           float u, uint32_t &err)
+{
+    const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
+    const float w00 = wy0 * wx0, w01 = wy0 * L.dx, w10 = L.dy * wx0, w11 = L.dy * L.dx;
+    if (L.ix1 != L.ix0 + 1) {
+        global_accum(a, a.out, L.iy0, L.ix0, t, q, u, w00, err);
+        global_accum(a, a.out, L.iy0, L.ix1, t, q, u, w01, err);
+        global_accum(a, a.out, L.iy1, L.ix0, t, q, u, w10, err);
+        global_accum(a, a.out, L.iy1, L.ix1, t, q, u, w11, err);
+        return;
+    }
+    const bool same_row = (W.cx >= 0) && (L.iy0 == W.iy);
+    if (same_row && (L.ix0 == W.cx + 1)) {
+        window_flush(a, W.iy, W.cx, W.c0, err);
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            W.c0[k] = W.c1[k];
+            W.c1[k] = 0.0f;
+        }
+        W.cx += 1;
+    } else if (!(same_row && (L.ix0 == W.cx))) {
+        if (W.cx >= 0) {
+            window_flush(a, W.iy, W.cx, W.c0, err);
+            window_flush(a, W.iy, W.cx + 1, W.c1, err);
+        }
+        W.iy = L.iy0;
+        W.cx = L.ix0;
+    }
+    const float f[3] = {t, q, u};
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+        W.c0[p] += w00 * f[p];
+        W.c1[p] += w01 * f[p];
+        W.c0[3 + p] += w10 * f[p];
+        W.c1[3 + p] += w11 * f[p];
+    }
+}
 
 template<bool TOD2MAP, int V>
 __global__ void __launch_bounds__(256)
@@ -765,19 +836,23 @@ unplanned_kernel(OpArgs a)
     for (int64_t v = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; v < nvec; v += stride) {
         const int64_t s0 = v * V;
         float y[V], x[V], al[V], tv[V], r[V];
-        if constexpr (V == 4) {
-            const float4 yy = __ldcs(reinterpret_cast<const float4 *>(a.xp + s0));
-            const float4 xx = __ldcs(reinterpret_cast<const float4 *>(a.xp + a.nsamp + s0));
-            const float4 aa = __ldcs(reinterpret_cast<const float4 *>(a.xp + 2 * a.nsamp + s0));
-            y[0] = yy.x; y[1] = yy.y; y[2] = yy.z; y[3] = yy.w;
-            x[0] = xx.x; x[1] = xx.y; x[2] = xx.z; x[3] = xx.w;
-            al[0] = aa.x; al[1] = aa.y; al[2] = aa.z; al[3] = aa.w;
-            if (TOD2MAP || a.accum) {
-                const float4 tt = TOD2MAP ? __ldcs(reinterpret_cast<const float4 *>(a.in + s0))
-                                          : *reinterpret_cast<const float4 *>(a.out + s0);
-                tv[0] = tt.x; tv[1] = tt.y; tv[2] = tt.z; tv[3] = tt.w;
-            } else {
-                tv[0] = tv[1] = tv[2] = tv[3] = 0.0f;
+        if constexpr (V >= 4) {
+#pragma unroll
+            for (int h = 0; h < V / 4; h++) {
+                const int64_t sh = s0 + 4 * h;
+                const float4 yy = __ldcs(reinterpret_cast<const float4 *>(a.xp + sh));
+                const float4 xx = __ldcs(reinterpret_cast<const float4 *>(a.xp + a.nsamp + sh));
+                const float4 aa = __ldcs(reinterpret_cast<const float4 *>(a.xp + 2 * a.nsamp + sh));
+                y[4 * h] = yy.x; y[4 * h + 1] = yy.y; y[4 * h + 2] = yy.z; y[4 * h + 3] = yy.w;
+                x[4 * h] = xx.x; x[4 * h + 1] = xx.y; x[4 * h + 2] = xx.z; x[4 * h + 3] = xx.w;
+                al[4 * h] = aa.x; al[4 * h + 1] = aa.y; al[4 * h + 2] = aa.z; al[4 * h + 3] = aa.w;
+                if (TOD2MAP || a.accum) {
+                    const float4 tt = TOD2MAP ? __ldcs(reinterpret_cast<const float4 *>(a.in + sh))
+                                              : *reinterpret_cast<const float4 *>(a.out + sh);
+                    tv[4 * h] = tt.x; tv[4 * h + 1] = tt.y; tv[4 * h + 2] = tt.z; tv[4 * h + 3] = tt.w;
+                } else {
+                    tv[4 * h] = tv[4 * h + 1] = tv[4 * h + 2] = tv[4 * h + 3] = 0.0f;
+                }
             }
         } else {
             y[0] = __ldcs(a.xp + s0);
@@ -785,6 +860,12 @@ unplanned_kernel(OpArgs a)
             al[0] = __ldcs(a.xp + 2 * a.nsamp + s0);
             tv[0] = TOD2MAP ? __ldcs(a.in + s0) : (a.accum ? a.out[s0] : 0.0f);
         }
+        ColumnWindow W;
+        W.iy = 0;
+        W.cx = -1;
+#pragma unroll
+        for (int k = 0; k < 6; k++)
+            W.c0[k] = W.c1[k] = 0.0f;
 #pragma unroll
         for (int k = 0; k < V; k++) {
             Located L;
@@ -794,10 +875,7 @@ unplanned_kernel(OpArgs a)
             const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
             if constexpr (TOD2MAP) {
                 const float t = tv[k], q = t * cs, u = t * sn;
-                global_accum(a, a.out, L.iy0, L.ix0, t, q, u, wy0 * wx0, err);
-                global_accum(a, a.out, L.iy0, L.ix1, t, q, u, wy0 * L.dx, err);
-                global_accum(a, a.out, L.iy1, L.ix0, t, q, u, L.dy * wx0, err);
-                global_accum(a, a.out, L.iy1, L.ix1, t, q, u, L.dy * L.dx, err);
+                window_add(a, W, L, t, q, u, err);
             } else {
                 const float e00 = global_eval(a, a.in, L.iy0, L.ix0, 1.0f, cs, sn, err);
                 const float e01 = global_eval(a, a.in, L.iy0, L.ix1, 1.0f, cs, sn, err);
@@ -807,11 +885,20 @@ unplanned_kernel(OpArgs a)
                 r[k] = a.accum ? (tv[k] + rr) : rr;
             }
         }
-        if constexpr (!TOD2MAP) {
-            if constexpr (V == 4)
-                __stcs(reinterpret_cast<float4 *>(a.out + s0), make_float4(r[0], r[1], r[2], r[3]));
-            else
+        if constexpr (TOD2MAP) {
+            if (W.cx >= 0) {
+                window_flush(a, W.iy, W.cx, W.c0, err);
+                window_flush(a, W.iy, W.cx + 1, W.c1, err);
+            }
+        } else {
+            if constexpr (V >= 4) {
+#pragma unroll
+                for (int h = 0; h < V / 4; h++)
+                    __stcs(reinterpret_cast<float4 *>(a.out + s0 + 4 * h),
+                           make_float4(r[4 * h], r[4 * h + 1], r[4 * h + 2], r[4 * h + 3]));
+            } else {
                 __stcs(a.out + s0, r[0]);
+            }
         }
     }
     block_publish_err(err, s_err, a.errword);
