@@ -205,6 +205,11 @@ int check_plan_vs_lpix(const gmm_lpix *lp, const gmm_preplan_info *info, const c
 
 }  // namespace
 
+int gmm::report_err_bits(uint32_t err, const char *where, uint32_t ignore)
+{
+    return err_bits(err, where, ignore);
+}
+
 extern "C" {
 
 const char *gmm_last_error(void) { return g_last_error.c_str(); }

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <sstream>
+#include <type_traits>
 
 #include <cuda_runtime.h>
 
@@ -482,6 +483,10 @@ void launch_planned_map2tod(Array<T> &tod, const Array<T> &local_map, const Arra
                             const LocalPixelization &lpix, const PointingPlan &plan, bool partial, bool debug, bool accum)
 {
     (void) debug;
+    if constexpr (!std::is_same_v<T, float>)
+        throw std::runtime_error(std::string("launch_map2tod") + ": planned operators are float32 only (the reference instantiates "
+                                 "the double kernels but cannot launch them: they need 96 KB of shared memory without "
+                                 "the opt-in); use the unplanned operators for double");
     check_tod(tod, plan.nsamp, "launch_map2tod", true);
     check_local_map(local_map, lpix, "launch_map2tod", true);
     check_xpointing(xpointing, plan.nsamp, "launch_map2tod", true);
@@ -496,6 +501,10 @@ void launch_planned_tod2map(Array<T> &local_map, const Array<T> &tod, const Arra
                             const LocalPixelization &lpix, const PointingPlan &plan, bool partial, bool debug)
 {
     (void) debug;
+    if constexpr (!std::is_same_v<T, float>)
+        throw std::runtime_error(std::string("launch_tod2map") + ": planned operators are float32 only (the reference instantiates "
+                                 "the double kernels but cannot launch them: they need 96 KB of shared memory without "
+                                 "the opt-in); use the unplanned operators for double");
     check_tod(tod, plan.nsamp, "launch_tod2map", true);
     check_local_map(local_map, lpix, "launch_tod2map", true);
     check_xpointing(xpointing, plan.nsamp, "launch_tod2map", true);
@@ -562,6 +571,10 @@ void launch_response_map2tod(Array<T> &tod, const Array<T> &local_map, const Arr
                              const LocalPixelization &lpix, const PointingPlan &plan, bool partial, bool debug, bool accum)
 {
     (void) debug;
+    if constexpr (!std::is_same_v<T, float>)
+        throw std::runtime_error(std::string("launch_response_map2tod") + ": planned operators are float32 only (the reference instantiates "
+                                 "the double kernels but cannot launch them: they need 96 KB of shared memory without "
+                                 "the opt-in); use the unplanned operators for double");
     const char *where = "launch_response_map2tod";
     check_tod(tod, plan.nsamp, where, true);
     check_local_map(local_map, lpix, where, true);
@@ -579,6 +592,10 @@ void launch_response_tod2map(Array<T> &local_map, const Array<T> &tod, const Arr
                              const LocalPixelization &lpix, const PointingPlan &plan, bool partial, bool debug)
 {
     (void) debug;
+    if constexpr (!std::is_same_v<T, float>)
+        throw std::runtime_error(std::string("launch_response_tod2map") + ": planned operators are float32 only (the reference instantiates "
+                                 "the double kernels but cannot launch them: they need 96 KB of shared memory without "
+                                 "the opt-in); use the unplanned operators for double");
     const char *where = "launch_response_tod2map";
     check_tod(tod, plan.nsamp, where, true);
     check_local_map(local_map, lpix, where, true);
@@ -610,8 +627,12 @@ void launch_unplanned_map2tod(Array<T> &tod, const Array<T> &local_map, const Ar
     check_xpointing(xpointing, nsamp, where, true);
     check_errflags_arr(errflags, where);
     gmm_lpix v = lpix.device_view();
-    throw_on_error(gmm_unplanned_map2tod((float *) tod.data, (const float *) local_map.data, (const float *) xpointing.data,
-                                         nsamp, &v, (uint32_t *) errflags.data, errflags.size, partial, accum, 1, 0));
+    if constexpr (std::is_same_v<T, double>)
+        throw_on_error(gmm_unplanned_map2tod_f64(tod.data, local_map.data, xpointing.data, nsamp, &v,
+                                                 (uint32_t *) errflags.data, errflags.size, partial, accum, 1, 0));
+    else
+        throw_on_error(gmm_unplanned_map2tod(tod.data, local_map.data, xpointing.data, nsamp, &v,
+                                             (uint32_t *) errflags.data, errflags.size, partial, accum, 1, 0));
 }
 
 template<typename T>
@@ -625,8 +646,12 @@ void launch_unplanned_tod2map(Array<T> &local_map, const Array<T> &tod, const Ar
     check_xpointing(xpointing, nsamp, where, true);
     check_errflags_arr(errflags, where);
     gmm_lpix v = lpix.device_view();
-    throw_on_error(gmm_unplanned_tod2map((float *) local_map.data, (const float *) tod.data, (const float *) xpointing.data,
-                                         nsamp, &v, (uint32_t *) errflags.data, errflags.size, partial, 1, 0));
+    if constexpr (std::is_same_v<T, double>)
+        throw_on_error(gmm_unplanned_tod2map_f64(local_map.data, tod.data, xpointing.data, nsamp, &v,
+                                                 (uint32_t *) errflags.data, errflags.size, partial, 1, 0));
+    else
+        throw_on_error(gmm_unplanned_tod2map(local_map.data, tod.data, xpointing.data, nsamp, &v,
+                                             (uint32_t *) errflags.data, errflags.size, partial, 1, 0));
 }
 
 void launch_planned_map2tod_async(Array<float> &tod, const Array<float> &local_map, const Array<float> &xpointing,
@@ -1054,6 +1079,22 @@ template void launch_unplanned_map2tod<float>(Array<float> &, const Array<float>
                                               const LocalPixelization &, Array<uint> &, bool, bool);
 template void launch_unplanned_tod2map<float>(Array<float> &, const Array<float> &, const Array<float> &,
                                               const LocalPixelization &, Array<uint> &, bool);
+// Double: the unplanned operators run (f64_kernels.cu); the planned and response ones raise, as the
+// reference's cannot launch.
+template void launch_planned_map2tod<double>(Array<double> &, const Array<double> &, const Array<double> &,
+                                             const LocalPixelization &, const PointingPlan &, bool, bool, bool);
+template void launch_planned_tod2map<double>(Array<double> &, const Array<double> &, const Array<double> &,
+                                             const LocalPixelization &, const PointingPlan &, bool, bool);
+template void launch_response_map2tod<double>(Array<double> &, const Array<double> &, const Array<double> &,
+                                              const Array<double> &, const LocalPixelization &, const PointingPlan &,
+                                              bool, bool, bool);
+template void launch_response_tod2map<double>(Array<double> &, const Array<double> &, const Array<double> &,
+                                              const Array<double> &, const LocalPixelization &, const PointingPlan &,
+                                              bool, bool);
+template void launch_unplanned_map2tod<double>(Array<double> &, const Array<double> &, const Array<double> &,
+                                               const LocalPixelization &, Array<uint> &, bool, bool);
+template void launch_unplanned_tod2map<double>(Array<double> &, const Array<double> &, const Array<double> &,
+                                               const LocalPixelization &, Array<uint> &, bool);
 template void reference_map2tod<float>(Array<float> &, const Array<float> &, const Array<float> &,
                                        const LocalPixelization &, bool, bool);
 template void reference_map2tod<double>(Array<double> &, const Array<double> &, const Array<double> &,

@@ -15,6 +15,9 @@ namespace gmm {
 
 // Number of SMs of the current device (cached per device).
 int device_sm_count();
+// Turns device error bits into the reference's exception text (check_arguments.cu:42-58) as the
+// last-error message and returns the status code (0 if no bit outside 'ignore' is set).
+int report_err_bits(uint32_t err, const char *where, uint32_t ignore);
 
 // ---- plan construction (plan_kernels.cu) ----
 // Radix sort of plan words by cell (and, with tod_bits > 0, by TOD index above the cell).

@@ -309,6 +309,16 @@ int gmm_unplanned_tod2map(float *local_map, const float *tod, const float *xpoin
                           const gmm_lpix *lpix, uint32_t *errflags_gpu, int64_t errflags_len,
                           int32_t partial_pixelization, int32_t sync_check, cudaStream_t stream);
 
+/* Double-precision unplanned operators: replace launch_unplanned_map2tod<double> and
+ * launch_unplanned_tod2map<double> (gpu_mm.hpp:204-224, map2tod_unplanned.cu:130-141,
+ * tod2map_unplanned.cu:124-134).  Arguments as in the float entry points, with double arrays. */
+int gmm_unplanned_map2tod_f64(double *tod, const double *local_map, const double *xpointing, int64_t nsamp,
+                              const gmm_lpix *lpix, uint32_t *errflags_gpu, int64_t errflags_len,
+                              int32_t partial_pixelization, int32_t accum, int32_t sync_check, cudaStream_t stream);
+int gmm_unplanned_tod2map_f64(double *local_map, const double *tod, const double *xpointing, int64_t nsamp,
+                              const gmm_lpix *lpix, uint32_t *errflags_gpu, int64_t errflags_len,
+                              int32_t partial_pixelization, int32_t sync_check, cudaStream_t stream);
+
 /* Deferred error check: reads the device error word (after 'stream' completes), masks the bits in
  * 'ignore' and returns the rest (check_gpu_errflags, check_arguments.cu:69-74). */
 int gmm_errword_read(const uint32_t *errword_gpu, uint32_t ignore, cudaStream_t stream);
