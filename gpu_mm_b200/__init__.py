@@ -21,7 +21,7 @@ except ImportError as _e:   # pragma: no cover - exercised only on unbuilt trees
 
 from .gpu_mm import *            # noqa: F401,F403
 from .gpu_mm import (map2tod, tod2map, LocalPixelization, LocalMap, DynamicMap, PointingPrePlan,  # noqa: F401
-                     PointingPlan, read_xpointing_npzfile, mm_dtype, tod2map_compensated, fold_compensation,
+                     PointingPlan, read_xpointing_npzfile, mm_dtype, ToyPointing, PointingPlanTester, tod2map_compensated, fold_compensation,
                      tod2map_f64)
 
 from .batch import TodBatch  # noqa: E402,F401

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 
-CU_SOURCES = ["plan_kernels.cu", "operator_kernels.cu", "cell_kernels.cu", "tod_kernels.cu", "f64_kernels.cu", "capi.cu", "noalloc.cu", "cpp_api.cpp"]
+CU_SOURCES = ["plan_kernels.cu", "operator_kernels.cu", "cell_kernels.cu", "tod_kernels.cu", "f64_kernels.cu", "quantize_kernels.cu", "capi.cu", "noalloc.cu", "cpp_api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(HERE, "libgpu_mm_b200.so")
 

@@ -5,6 +5,7 @@
 // exceptions, same synchronous error-flag semantics.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <sstream>
 #include <type_traits>
@@ -957,6 +958,156 @@ template void cell_broadcast<float>(Array<float> &, const Array<float> &, const 
 template void cell_broadcast<double>(Array<double> &, const Array<double> &, const Array<long> &);
 template void cell_reduce<float>(Array<float> &, const Array<float> &, const Array<long> &);
 template void cell_reduce<double>(Array<double> &, const Array<double> &, const Array<long> &);
+
+// ---- Test utilities: ToyPointing, PointingPlanTester -------------------------------------------
+
+template<typename T>
+static Array<T> toy_xpointing(long ndet, long nt, bool gpu)
+{
+    if ((nt <= 0) || ((ndet > 0) && (ndet * nt <= 0)))
+        throw std::runtime_error("ToyPointing constructor: bad (ndet, nt)");
+    std::vector<long> shape = (ndet <= 0) ? std::vector<long>{3, nt} : std::vector<long>{3, ndet, nt};
+    return gpu ? Array<T>::alloc_gpu(shape) : Array<T>::alloc_host(shape);
+}
+
+template<typename T>
+ToyPointing<T>::ToyPointing(long ndet, long nt, long ny, long nx, double speed, double drift, bool noisy)
+    : ToyPointing(ny, nx, speed, drift, toy_xpointing<T>(ndet, nt, false), toy_xpointing<T>(ndet, nt, true), noisy)
+{
+}
+
+// The raster of ToyPointing.cu:63-108: y bounces between 1.1*speed and ny-2-1.1*speed at 'speed'
+// pixels per sample, x moves by the same step plus the drift and wraps into [0, nx]; alpha = 1.
+// Accumulated in double, as there, and stored as T.
+template<typename T>
+ToyPointing<T>::ToyPointing(long ny, long nx, double speed, double drift, const Array<T> &xp_cpu, const Array<T> &xp_gpu,
+                            bool noisy)
+    : nypix_global(ny), nxpix_global(nx), scan_speed(speed), total_drift(drift),
+      drift_speed(drift / (3.0 * (double) xp_cpu.size)), xpointing_cpu(xp_cpu), xpointing_gpu(xp_gpu)
+{
+    const char *where = "ToyPointing constructor";
+    long nsamp;
+    check_xpointing_and_init_nsamp(xpointing_cpu, nsamp, where, false);
+    check_xpointing(xpointing_gpu, nsamp, where, true);
+    GMM_ASSERT(xpointing_cpu.is_fully_contiguous() && xpointing_gpu.is_fully_contiguous(), where);
+    GMM_ASSERT((ny >= 2) && (ny <= (1 << 16)) && (nx >= 2) && (nx <= (1 << 16)), where);
+    GMM_ASSERT((scan_speed > 0.0) && (scan_speed <= 1.0), where);
+    GMM_ASSERT((drift_speed > 0.0) && (drift_speed <= 1.0), where);
+    if (noisy)
+        std::printf("%s: constructor called\n", str().c_str());
+    T *yp = xpointing_cpu.data, *xp = yp + nsamp, *ap = yp + 2 * nsamp;
+    const double ylo = 1.1 * speed, yhi = (double) (ny - 2) - 1.1 * speed;
+    double y = 1.0, x = 1.0, vel = speed;
+    for (long s = 0; s < nsamp; s++) {
+        yp[s] = (T) y;
+        xp[s] = (T) x;
+        ap[s] = (T) 1.0;
+        if ((vel > 0) && (y > yhi))
+            vel = -speed;
+        if ((vel < 0) && (y < ylo))
+            vel = speed;
+        y += vel;
+        x += vel + drift_speed;
+        if (x < 0.0)
+            x += (double) nx;
+        if (x > (double) nx)
+            x -= (double) nx;
+    }
+    cuda_check(cudaMemcpy(xpointing_gpu.data, xpointing_cpu.data, 3 * nsamp * sizeof(T), cudaMemcpyHostToDevice), where);
+    if (noisy)
+        std::printf("%s: constructor done\n", str().c_str());
+}
+
+template<typename T>
+std::string ToyPointing<T>::str() const
+{
+    std::ostringstream ss;
+    ss << "ToyPointing(tod_shape=(";
+    for (int i = 1; i < xpointing_cpu.ndim; i++)
+        ss << (i > 1 ? "," : "") << xpointing_cpu.shape[i];
+    ss << "), nypix_global=" << nypix_global << ", nxpix_global=" << nxpix_global << ", scan_speed=" << scan_speed
+       << ", total_drift=" << total_drift << ")";
+    return ss.str();
+}
+
+template struct ToyPointing<float>;
+template struct ToyPointing<double>;
+
+long PointingPlanTester::get_constructor_tmp_nbytes(const PointingPrePlan &pp)
+{
+    // The reference's size (PointingPlanTester.cu:172-178): two int arrays and one error word per block.
+    const long nblocks = (pp.nsamp + nsamp_per_block - 1) / nsamp_per_block;
+    return (2 * pp.nsamp + nblocks) * (long) sizeof(int);
+}
+
+PointingPlanTester::PointingPlanTester(const PointingPrePlan &pp, const Array<float> &xp)
+    : PointingPlanTester(pp, xp, Array<unsigned char>::alloc_gpu({get_constructor_tmp_nbytes(pp)}))
+{
+}
+
+PointingPlanTester::PointingPlanTester(const PointingPrePlan &pp, const Array<float> &xp, const Array<unsigned char> &tmp)
+    : nsamp(pp.nsamp), nypix_global(pp.nypix_global), nxpix_global(pp.nxpix_global), periodic_xcoord(pp.periodic_xcoord),
+      plan_nmt(pp.plan_nmt), ncl_per_threadblock(pp.ncl_per_threadblock), planner_nblocks(pp.planner_nblocks)
+{
+    const char *where = "PointingPlanTester constructor";
+    check_xpointing(xp, nsamp, where, true);
+    GMM_ASSERT(tmp.on_gpu() && tmp.is_fully_contiguous() && (tmp.size >= get_constructor_tmp_nbytes(pp)), where);
+    GMM_ASSERT((nsamp > (planner_nblocks - 1) * ncl_per_threadblock * 32) &&
+               (nsamp <= planner_nblocks * ncl_per_threadblock * 32), where);
+
+    int32_t *iy_gpu = (int32_t *) tmp.data;
+    int32_t *ix_gpu = iy_gpu + nsamp;
+    uint32_t *err_gpu = (uint32_t *) (ix_gpu + nsamp);
+    throw_on_error(gmm_quantize_pointing(xp.data, nsamp, (int32_t) nypix_global, (int32_t) nxpix_global,
+                                         periodic_xcoord, iy_gpu, ix_gpu, err_gpu, 0));
+    throw_on_error(gmm_errword_read(err_gpu, 0, 0));
+    iypix_arr = Array<int>::alloc_host({nsamp});
+    ixpix_arr = Array<int>::alloc_host({nsamp});
+    cuda_check(cudaMemcpy(iypix_arr.data, iy_gpu, nsamp * sizeof(int), cudaMemcpyDeviceToHost), where);
+    cuda_check(cudaMemcpy(ixpix_arr.data, ix_gpu, nsamp * sizeof(int), cudaMemcpyDeviceToHost), where);
+
+    // Per cache line: the distinct cells of the four neighbours of its samples, ascending, as mt words
+    // cell | line << 20 (PointingPlanTester.cu:126-160; x+1 wraps to 0 at the last column).
+    nmt_cumsum = Array<uint>::alloc_host({planner_nblocks});
+    sorted_mt = Array<ulong>::alloc_host({std::max<long>(plan_nmt, 1)});
+    std::vector<int> cells;
+    long n = 0;
+    for (long b = 0; b < planner_nblocks; b++) {
+        const long l1 = std::min(nsamp, (b + 1) * ncl_per_threadblock * 32) >> 5;
+        for (long l = b * ncl_per_threadblock; l < l1; l++) {
+            cells.clear();
+            for (long s = 32 * l; s < 32 * l + 32; s++) {
+                const int iy = iypix_arr.data[s], ix = ixpix_arr.data[s];
+                const int ix1 = (ix < nxpix_global - 1) ? (ix + 1) : 0;
+                for (int dy = 0; dy < 2; dy++)
+                    for (int c = 0; c < 2; c++) {
+                        const int cell = (((iy + dy) >> 6) << 10) | ((c ? ix1 : ix) >> 6);
+                        if (std::find(cells.begin(), cells.end(), cell) == cells.end())
+                            cells.push_back(cell);
+                    }
+            }
+            std::sort(cells.begin(), cells.end());
+            for (int cell : cells) {
+                if (n >= plan_nmt)
+                    throw std::runtime_error(std::string(where) + ": more (cell, cache line) pairs than the preplan's nmt");
+                sorted_mt.data[n++] = (ulong) cell | ((ulong) l << 20);
+            }
+        }
+        nmt_cumsum.data[b] = (uint) n;
+    }
+    if (n != plan_nmt)
+        throw std::runtime_error(std::string(where) + ": (cell, cache line) count differs from the preplan's nmt");
+    std::sort(sorted_mt.data, sorted_mt.data + n);
+    sorted_mt.shape[0] = sorted_mt.size = n;
+}
+
+std::string PointingPlanTester::str() const
+{
+    std::ostringstream ss;
+    ss << "PointingPlanTester(nsamp=" << nsamp << ", nypix_global=" << nypix_global << ", nxpix_global=" << nxpix_global
+       << ", plan_nmt=" << plan_nmt << ")";
+    return ss.str();
+}
 
 // ---- TOD preprocessing (deglitching.cu, cuts.cu, misc.cu): device arrays; index-map entries out of
 // range raise after the call.

@@ -296,6 +296,48 @@ PYBIND11_MODULE(gpu_mm_pybind11, m)
              "One word per cache line (cell | line << 20), sorted by the line's lowest cell")
         .def("__str__", &PointingPlan::str);
 
+    // Test utilities (gpu_mm_pybind11.cu:228-262).  ToyPointing fills caller-allocated arrays.
+    py::class_<ToyPointing<float>>(m, "ToyPointing")
+        .def(py::init([](long nypix_global, long nxpix_global, double scan_speed, double total_drift,
+                         py::object xpointing_cpu, py::object xpointing_gpu, bool noisy) {
+                 Array<float> c = to_array<float>(xpointing_cpu, "xpointing_cpu");
+                 Array<float> g = to_array<float>(xpointing_gpu, "xpointing_gpu");
+                 return new ToyPointing<float>(nypix_global, nxpix_global, scan_speed, total_drift, c, g, noisy);
+             }),
+             py::arg("nypix_global"), py::arg("nxpix_global"), py::arg("scan_speed"), py::arg("total_drift"),
+             py::arg("xpointing_cpu"), py::arg("xpointing_gpu"), py::arg("noisy"))
+        .def_readonly("nypix_global", &ToyPointing<float>::nypix_global, "Number of y-pixels")
+        .def_readonly("nxpix_global", &ToyPointing<float>::nxpix_global, "Number of x-pixels")
+        .def_readonly("scan_speed", &ToyPointing<float>::scan_speed, "Scan speed in map pixels per TOD sample")
+        .def_readonly("total_drift", &ToyPointing<float>::total_drift, "Total drift over full TOD, in x-pixels")
+        .def_readonly("drift_speed", &ToyPointing<float>::drift_speed, "Drift (in x-pixels) per TOD sample")
+        .def("__str__", &ToyPointing<float>::str);
+
+    py::class_<PointingPlanTester>(m, "PointingPlanTester", "PointingPlanTester: A utility class used in unit tests")
+        .def(py::init([](const PointingPrePlan &preplan, py::object xpointing_gpu, py::object tmp) {
+                 Array<float> xp = to_array<float>(xpointing_gpu, "xpointing_gpu");
+                 Array<unsigned char> t = to_array<unsigned char>(tmp, "tmp");
+                 py::gil_scoped_release rel;
+                 return new PointingPlanTester(preplan, xp, t);
+             }),
+             py::arg("preplan"), py::arg("xpointing_gpu"), py::arg("tmp"))
+        .def_readonly("nsamp", &PointingPlanTester::nsamp, "Number of TOD samples")
+        .def_readonly("nypix_global", &PointingPlanTester::nypix_global, "Number of y-pixels")
+        .def_readonly("nxpix_global", &PointingPlanTester::nxpix_global, "Number of x-pixels")
+        .def_readonly("plan_nmt", &PointingPlanTester::plan_nmt, "Total number of mt-pairs in plan")
+        .def_readonly("ncl_per_threadblock", &PointingPlanTester::ncl_per_threadblock, "Used when launching planner/preplanner kernels")
+        .def_readonly("planner_nblocks", &PointingPlanTester::planner_nblocks, "Used when launching planner/preplanner kernels")
+        .def_property_readonly("iypix", [](const PointingPlanTester &p) { return host_to_numpy(p.iypix_arr); },
+                               "Length-nsamp array containing integer y-pixel indices")
+        .def_property_readonly("ixpix", [](const PointingPlanTester &p) { return host_to_numpy(p.ixpix_arr); },
+                               "Length-nsamp array containing integer x-pixel indices")
+        .def_property_readonly("nmt_cumsum", [](const PointingPlanTester &p) { return host_to_numpy(p.nmt_cumsum); },
+                               "Length-nblocks array containing integer cumulative counts")
+        .def_property_readonly("sorted_mt", [](const PointingPlanTester &p) { return host_to_numpy(p.sorted_mt); },
+                               "Length nmt_cumsum[-1], see PointingPlan docstring for 'mt' format")
+        .def_static("get_constructor_tmp_nbytes", &PointingPlanTester::get_constructor_tmp_nbytes, py::arg("preplan"))
+        .def("__str__", &PointingPlanTester::str);
+
     m.def("planned_map2tod",
           [](py::object tod, py::object local_map, py::object xpointing, const LocalPixelization &lpix,
              const PointingPlan &plan, bool partial_pixelization, bool debug, bool accum) {

@@ -501,6 +501,61 @@ class PointingPlan(gpu_mm_pybind11.PointingPlan):
         gpu_mm_pybind11.PointingPlan.__init__(self, preplan, xpointing_gpu, buf, tmp_buf, debug)
 
 
+class ToyPointing(gpu_mm_pybind11.ToyPointing):
+    """
+    ToyPointing(ndet, nt, nypix_global, nxpix_global, scan_speed, total_drift, noisy=True)
+    (gpu_mm.py:1332-1385): a synthetic raster for tests.  Scans go at 45 degrees and cover the
+    full y range; 'scan_speed' = map pixels per TOD sample, 'total_drift' = drift over the TOD in
+    x-pixels.  ndet=None gives (3, nt) pointing, else (3, ndet, nt).
+
+    Members: xpointing_cpu (numpy float32), xpointing_gpu (torch CUDA float32), ndet, nt, and from
+    C++ nypix_global, nxpix_global, scan_speed, total_drift, drift_speed, __str__().
+    """
+
+    def __init__(self, ndet, nt, nypix_global, nxpix_global, scan_speed, total_drift, noisy=True):
+        shape = (3, ndet, nt) if (ndet is not None) else (3, nt)
+        self.ndet, self.nt = ndet, nt
+        self.xpointing_cpu = np.zeros(shape, mm_dtype)
+        self.xpointing_gpu = torch.zeros(shape, dtype=torch.float32, device="cuda")
+        gpu_mm_pybind11.ToyPointing.__init__(self, nypix_global, nxpix_global, scan_speed, total_drift,
+                                             self.xpointing_cpu, self.xpointing_gpu, noisy)
+
+    @staticmethod
+    def make_random(nsamp_max, noisy=True):
+        """A ToyPointing of random shape and parameters (the reference's make_random): TOD shape (nt,)
+        or (ndet, nt) with at most about nsamp_max samples."""
+        assert nsamp_max >= 64 * 1024
+        if np.random.randint(0, 2):
+            ndet = None
+            nt = 32 * np.random.randint(nsamp_max // 64, nsamp_max // 32)
+        else:
+            r = np.random.randint(0, 6)
+            s = int((nsamp_max / 32.) ** 0.5)
+            ndet = 2 ** r * np.random.randint(s // 2, s + 1)
+            nt = 2 ** (5 - r) * np.random.randint(s // 2, s + 1)
+        npix_max = min(nsamp_max // 128, 16384)
+        nypix_global = np.random.randint(npix_max / 8, npix_max // 2 + 1)
+        nxpix_global = np.random.randint(nypix_global + 2, npix_max + 1)
+        scan_speed = np.random.uniform(0.1, 0.5)
+        total_drift = np.random.uniform(0.1 * (nxpix_global - nypix_global), (nxpix_global - nypix_global) - 2)
+        return ToyPointing(ndet, nt, nypix_global, nxpix_global, scan_speed, total_drift, noisy=noisy)
+
+
+class PointingPlanTester(gpu_mm_pybind11.PointingPlanTester):
+    """
+    PointingPlanTester(preplan, xpointing_gpu) (gpu_mm.py:1388-1415): the plan computed the simple way,
+    for tests.  Members: nsamp, nypix_global, nxpix_global, plan_nmt, ncl_per_threadblock,
+    planner_nblocks, iypix and ixpix (per sample, from the GPU), nmt_cumsum (per planner block) and
+    sorted_mt (all mt words, sorted), as numpy arrays.
+    """
+
+    def __init__(self, preplan, xpointing_gpu):
+        assert isinstance(preplan, PointingPrePlan)
+        tmp_nbytes = gpu_mm_pybind11.PointingPlanTester.get_constructor_tmp_nbytes(preplan)
+        tmp = torch.empty(tmp_nbytes, dtype=torch.uint8, device="cuda")
+        gpu_mm_pybind11.PointingPlanTester.__init__(self, preplan, xpointing_gpu, tmp)
+
+
 ####################################################################################################
 
 

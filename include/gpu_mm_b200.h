@@ -319,6 +319,13 @@ int gmm_unplanned_tod2map_f64(double *local_map, const double *tod, const double
                               const gmm_lpix *lpix, uint32_t *errflags_gpu, int64_t errflags_len,
                               int32_t partial_pixelization, int32_t sync_check, cudaStream_t stream);
 
+/* Per-sample pixel quantization for the PointingPlanTester test utility (PointingPlanTester.cu:22-63,
+ * quantize_kernel): iypix[s], ixpix[s] = the (iy0, ix0) that locate() gives sample s.  Asynchronous;
+ * device error bits (out-of-range pointing) go to *errword. */
+int gmm_quantize_pointing(const float *xpointing, int64_t nsamp, int32_t nypix_global, int32_t nxpix_global,
+                          int32_t periodic_xcoord, int32_t *iypix, int32_t *ixpix, uint32_t *errword,
+                          cudaStream_t stream);
+
 /* Deferred error check: reads the device error word (after 'stream' completes), masks the bits in
  * 'ignore' and returns the rest (check_gpu_errflags, check_arguments.cu:69-74). */
 int gmm_errword_read(const uint32_t *errword_gpu, uint32_t ignore, cudaStream_t stream);

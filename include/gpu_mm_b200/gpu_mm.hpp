@@ -228,6 +228,54 @@ uint expand_dynamic_map2(Array<uint> &global_ncells, LocalPixelization &local_pi
 template<typename T>
 void local_map_to_global(const LocalPixelization &local_pixelization, Array<T> &dst, const Array<T> &src);
 
+// Test utilities of the reference's public surface (gpu_mm.hpp:314-430).
+//
+// ToyPointing: a synthetic 45-degree raster over the full y range with a slow x drift
+// (ToyPointing.cu:29-117); writes xpointing_cpu, then copies it into xpointing_gpu.
+template<typename T>
+struct ToyPointing {
+    ToyPointing(long ndet, long nt, long nypix_global, long nxpix_global, double scan_speed, double total_drift,
+                bool noisy = true);
+    ToyPointing(long nypix_global, long nxpix_global, double scan_speed, double total_drift,
+                const Array<T> &xpointing_cpu, const Array<T> &xpointing_gpu, bool noisy = true);
+
+    long nypix_global = 0;
+    long nxpix_global = 0;
+    double scan_speed = 0.0;    // map pixels per sample
+    double total_drift = 0.0;   // the constructor argument
+    double drift_speed = 0.0;   // x-pixels per sample: total_drift / (3 * xpointing size), as in the reference
+    Array<T> xpointing_cpu;
+    Array<T> xpointing_gpu;
+
+    std::string str() const;
+};
+
+// PointingPlanTester: the plan computed the simple way, for tests (PointingPlanTester.cu:69-160).
+// (iypix, ixpix) per sample come from the GPU (same roundoff as the plan); per cache line the
+// distinct cells of the four neighbours, sorted, as mt words; nmt_cumsum per planner block; and all
+// words sorted.  All arrays are on the host.
+struct PointingPlanTester {
+    PointingPlanTester(const PointingPrePlan &pp, const Array<float> &xpointing_gpu);
+    PointingPlanTester(const PointingPrePlan &pp, const Array<float> &xpointing_gpu, const Array<unsigned char> &tmp);
+
+    long nsamp = 0;
+    long nypix_global = 0;
+    long nxpix_global = 0;
+    bool periodic_xcoord = true;
+    long plan_nmt = 0;
+    long ncl_per_threadblock = 0;
+    long planner_nblocks = 0;
+
+    Array<int> iypix_arr;      // length nsamp
+    Array<int> ixpix_arr;      // length nsamp
+    Array<uint> nmt_cumsum;    // length planner_nblocks
+    Array<ulong> sorted_mt;    // length plan_nmt
+
+    std::string str() const;
+    static long get_constructor_tmp_nbytes(const PointingPrePlan &pp);
+    static constexpr int nsamp_per_block = 1024;
+};
+
 // TOD preprocessing on device arrays (deglitching.cu:99-210, cuts.cu:38-55, misc.cu:8-19); index
 // maps are int32.  deglitch without 'cumj' computes the jump cumsum on the device.  tod_ranges mode: 0 extract (rdata <- tod), 1 insert (tod <- rdata), 2 clear.
 void get_border_means(Array<float> &out, const Array<float> &signal, const Array<int> &index_map);
