@@ -8,7 +8,8 @@ xpointing and TOD, build the plan, run the operators and copy the result back on
 over PCIe the copies dominate, so here they run on their own streams while the GPU works on the
 chunk before:
 
-  stream 'h2d':     chunk i's xpointing rows (and TOD) into device slot i % nslots
+  streams 'h2d':    chunk i's xpointing rows (and TOD) into device slot i % nslots, on one of two
+                    streams in turn (two copies in flight use PCIe better than one: 55 vs 49 GB/s)
   stream 'compute': chunk i's plan (a one-TOD batch plan: no host synchronisation), map2tod into the
                     slot's output TOD, tod2map from the slot's input TOD into the map
   stream 'd2h':     the slot's output TOD back into the host array
@@ -83,7 +84,8 @@ class HostPipeline:
         self._tout = [torch.empty(n, dtype=torch.float32, device="cuda") for _ in range(self.nslots)]
         self._errs = torch.zeros((len(self.chunks), 3), dtype=torch.int32, device="cuda")
         self._batches = {}                   # (slot, ndet of chunk) -> (batch over tout, batch over tin)
-        self._h2d, self._comp, self._d2h = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+        self._h2d = [torch.cuda.Stream(), torch.cuda.Stream()]
+        self._comp, self._d2h = torch.cuda.Stream(), torch.cuda.Stream()
         self._free = [torch.cuda.Event() for _ in range(self.nslots)]      # compute done reading the slot
         self._drained = [torch.cuda.Event() for _ in range(self.nslots)]   # output copied out of the slot
         self._map_dev = {}
@@ -135,7 +137,7 @@ class HostPipeline:
                 raise RuntimeError("HostPipeline.run: tod2map needs map_out")
         self._partial = bool(partial_pixelization)
         cur = torch.cuda.current_stream()
-        for s in (self._h2d, self._comp, self._d2h):
+        for s in (*self._h2d, self._comp, self._d2h):
             s.wait_stream(cur)               # inputs written on the caller's stream come first
 
         # Maps: host maps are copied in on the h2d stream before the first chunk.
@@ -147,7 +149,7 @@ class HostPipeline:
             else:
                 _host(m, "map_in", tuple(m.shape))
                 min_d = self._device_map("in", m)
-                with torch.cuda.stream(self._h2d):
+                with torch.cuda.stream(self._h2d[0]):
                     min_d.copy_(m, non_blocking=True)
         if do_t2m:
             m = _map_tensor(map_out, "map_out")
@@ -157,10 +159,10 @@ class HostPipeline:
                 _host(m, "map_out", tuple(m.shape))
                 mout_h = m
                 mout_d = self._device_map("out", m)
-                with torch.cuda.stream(self._h2d):
+                with torch.cuda.stream(self._h2d[0]):
                     mout_d.copy_(m, non_blocking=True)
         maps_in = torch.cuda.Event()
-        maps_in.record(self._h2d)
+        maps_in.record(self._h2d[0])
         self._comp.wait_event(maps_in)
 
         for i, (d0, d1) in enumerate(self.chunks):
@@ -169,15 +171,16 @@ class HostPipeline:
             n = nd * nt
             b_out, b_in = self._slot_batches(k, nd)
             # h2d: overwrite the slot once the compute that last read it is done.
-            self._h2d.wait_event(self._free[k])
-            with torch.cuda.stream(self._h2d):
+            h2d = self._h2d[i % 2]
+            h2d.wait_event(self._free[k])
+            with torch.cuda.stream(h2d):
                 xv = self._xp[k][:3 * n].view(3, nd, nt)
                 for r in range(3):
                     xv[r].copy_(xpointing[r, d0:d1], non_blocking=True)
                 if do_t2m:
                     self._tin[k][:n].view(nd, nt).copy_(tod_in[d0:d1], non_blocking=True)
             arrived = torch.cuda.Event()
-            arrived.record(self._h2d)
+            arrived.record(h2d)
             # compute: wait for the inputs, and for the copy that drained the slot's last output.
             self._comp.wait_event(arrived)
             self._comp.wait_event(self._drained[k])
@@ -201,7 +204,7 @@ class HostPipeline:
             self._d2h.wait_event(done)
             with torch.cuda.stream(self._d2h):
                 mout_h.copy_(mout_d, non_blocking=True)
-        for s in (self._h2d, self._comp, self._d2h):
+        for s in (*self._h2d, self._comp, self._d2h):
             cur.wait_stream(s)
         self._pending = True
 
