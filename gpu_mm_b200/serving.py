@@ -182,21 +182,27 @@ class PointingServer:
         return done
 
     def _launch(self):
-        admitted, pinned = [], set()
+        # A plan this iteration builds is reserved when its first request is admitted, so that the
+        # admission of later requests in the same iteration sees it.
+        admitted, pinned, reserved = [], set(), {}
         while self._waiting and len(admitted) < self.max_batch:
             r = self._waiting[0]
-            need = self._request_nbytes(r) + (0 if r["id"] in self._plans else self._plan_nbytes(r["id"]))
+            new_plan = (r["id"] not in self._plans) and (r["id"] not in reserved)
+            plan_nb = self._plan_nbytes(r["id"]) if new_plan else 0
+            need = self._request_nbytes(r) + plan_nb
             pinned.add(r["id"])
             if not self._evict(need, pinned | {q["id"] for q in admitted}):
                 pinned.discard(r["id"])
                 break
             admitted.append(self._waiting.popleft())
-            self._used += self._request_nbytes(r)
+            self._used += need
+            if new_plan:
+                reserved[r["id"]] = plan_nb
         if not admitted:
             return False
         try:
             t0 = time.perf_counter()
-            ok = self._launch_admitted(admitted)
+            ok = self._launch_admitted(admitted, reserved)
             self.iterations.append((len(admitted), time.perf_counter() - t0))
             return ok
         except Exception as e:
@@ -205,9 +211,12 @@ class PointingServer:
                 if not r["fut"].done():
                     r["fut"].set_exception(e)
                 self._used -= self._request_nbytes(r)
+            for tid, nb in reserved.items():
+                if tid not in self._plans:
+                    self._used -= nb
             raise
 
-    def _launch_admitted(self, admitted):
+    def _launch_admitted(self, admitted, reserved):
         stream = self._stream()
         keep = []
         # Everything below is allocated and launched on 'stream', so allocations, copies and kernels
@@ -231,7 +240,7 @@ class PointingServer:
                         self._used -= self._plans.pop(i)[2]
                     nb = max(self._plan_nbytes(i), sp.plan.numel())
                     self._plans[i] = (sp, ev, nb)
-                    self._used += nb
+                    self._used += nb - reserved.get(i, 0)
                 self._errwords.append(builder.err)
                 keep.append(builder)
             for r in admitted:
