@@ -15,6 +15,7 @@ xpointing + TOD streamed per step is larger than L2, so no flush is needed betwe
 Other numbers on the JSON line:
   roofline     the dominant kernel's algorithmic bytes per launch / its CUDA-event duration, against
                the measured HBM copy bandwidth (MEASURED_PEAKS.json)
+  rooflines    the same for both planned kernels
   e2e          the same metric through the public API from pinned HOST buffers: H2D of xpointing,
                TOD and map, preplan + plan, map2tod, tod2map, D2H of the TOD and map results
   cpu_baseline the reference's CPU operators (oracle/_ref: the reference header; else the oracle
@@ -657,6 +658,19 @@ def main():
             td = json.load(f)
         traffic = int(td["bytes_per_sample"] * nsamp + td.get("bytes_per_pixel", 0) * npix)
 
+    # Both planned kernels against the roofline (the dominant one is 'roofline' above).
+    per_kernel = {}
+    for kname, kms, kbytes in (("planned_map2tod", m2t_ms, m2t_bytes), ("planned_tod2map", t2m_ms, t2m_bytes)):
+        kach = kbytes / (kms * 1e-3) / 1e9
+        ktr = None
+        kpath = os.path.join(ROOT, "profiles", f"{kname}_traffic.json")
+        if os.path.exists(kpath):
+            with open(kpath) as f:
+                kd = json.load(f)
+            ktr = int(kd["bytes_per_sample"] * nsamp + kd.get("bytes_per_pixel", 0) * npix)
+        per_kernel[kname] = {"ms": round(kms, 4), "achieved_gbs": round(kach, 1), "frac": round(kach / peak, 4),
+                             "algorithmic_bytes": kbytes, "traffic": ktr}
+
     # Unplanned operators (for context).
     unplanned = {}
     for name, fn in (("unplanned_map2tod_ms", lambda: m.unplanned_map2tod_async(tod_out, lmap.arr, xp, lp, False, False, err_a, 0)),
@@ -776,6 +790,7 @@ def main():
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
                          "per_unit": "16 B/sample + 12 B/hit pixel (map2tod) or 24 B/hit pixel (tod2map)"},
+            "rooflines": per_kernel,
             "kernels_ms": {"planned_map2tod": round(m2t_ms, 4), "planned_tod2map": round(t2m_ms, 4),
                            **unplanned, "plan_build": round(statistics.mean(plan_ms), 4),
                            "first_plan_build_s": round(first_plan_s, 3)},
