@@ -33,13 +33,34 @@ struct LineSlots {
     unsigned amask[6];
 };
 
-__device__ __forceinline__ void analyse_line(float y, float x, int ny, int nx, bool periodic,
-                                             LineSlots &ls, uint32_t &err)
+// Slot analysis of one cache line by the full warp; returns its number of (cell, line) pairs.
+// A line whose samples all have their four bilinear neighbours in one and the same cell (most lines:
+// a line is 32 samples, a cell 64 pixels wide) has exactly one pair, the same result the six-slot
+// analysis gives it: that cell, reported in slot 0 at lane 0.  The test is two shifts and two
+// compares per lane plus one shuffle and one vote, where the slot analysis is ALU-bound.
+__device__ __forceinline__ int analyse_line(float y, float x, int ny, int nx, bool periodic, LineSlots &ls,
+                                            uint32_t &err)
 {
     Located L;
     err |= locate(y, x, ny, nx, periodic, L);
+    const bool one = ((L.iy0 >> 6) == (L.iy1 >> 6)) && ((L.ix0 >> 6) == (L.ix1 >> 6));
+    const int c = ((L.iy0 >> 6) << 10) | (L.ix0 >> 6);
+    const int c0 = __shfl_sync(kFullMask, c, 0);
+    if (__all_sync(kFullMask, one && (c == c0))) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            ls.slots[k] = (k == 0) ? c0 : -1;
+            ls.amask[k] = (k == 0) ? 1u : 0u;
+        }
+        return 1;
+    }
     cell_slots(L, ls.slots);
     line_slot_masks(ls.slots, ls.amask);
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+        cnt += __popc(ls.amask[k]);
+    return cnt;
 }
 
 // Each planner block is counted by kPreplanSplit CTAs (a contiguous quarter of its lines each), which
@@ -75,10 +96,7 @@ preplan_count_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx
             if (lb + j >= l1)
                 break;
             LineSlots ls;
-            analyse_line(y[j], x[j], ny, nx, periodic, ls, err);
-#pragma unroll
-            for (int k = 0; k < 6; k++)
-                n += __popc(ls.amask[k]);
+            n += analyse_line(y[j], x[j], ny, nx, periodic, ls, err);
         }
     }
 
@@ -197,10 +215,7 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
             int cnt = 0;
             LineSlots ls;
             if (lw + j < l1) {
-                analyse_line(y[j], x[j], ny, nx, periodic, ls, err);
-#pragma unroll
-                for (int k = 0; k < 6; k++)
-                    cnt += __popc(ls.amask[k]);
+                cnt = analyse_line(y[j], x[j], ny, nx, periodic, ls, err);
             } else {
 #pragma unroll
                 for (int k = 0; k < 6; k++) {
