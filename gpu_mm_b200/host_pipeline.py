@@ -48,6 +48,23 @@ def _map_tensor(m, name):
     return arr
 
 
+def chunk_plan(ndet, nt, chunk_dets=None, target_samples=1 << 24):
+    """Detector ranges [(d0, d1), ...] covering range(ndet): about target_samples (or chunk_dets
+    detectors) per chunk, every chunk a multiple of 32 samples.  Raises if ndet*nt is not."""
+    ndet, nt = int(ndet), int(nt)
+    if ndet <= 0 or nt <= 0 or (ndet * nt) % 32:
+        raise RuntimeError(f"HostPipeline: ndet*nt = {ndet * nt} must be a positive multiple of 32")
+    step = 1
+    while (step * nt) % 32:
+        step += 1                            # detectors per chunk must keep chunks a multiple of 32 samples
+    cd = int(chunk_dets) if chunk_dets else max(1, target_samples // nt)
+    cd = min(ndet, max(step, (cd // step) * step))
+    chunks = [(d0, min(ndet, d0 + cd)) for d0 in range(0, ndet, cd)]
+    # The last chunk holds ndet*nt - (whole chunks)*cd*nt samples: a multiple of 32 as both terms are.
+    assert all(((d1 - d0) * nt) % 32 == 0 for d0, d1 in chunks)
+    return cd, chunks
+
+
 class HostPipeline:
     """Streams TODs of shape (ndet, nt) with pointing (3, ndet, nt) from pinned host memory through
     the planned operators against one LocalPixelization.
@@ -61,21 +78,12 @@ class HostPipeline:
         if not isinstance(local_pixelization, LocalPixelization):
             raise RuntimeError("HostPipeline: expected a LocalPixelization")
         ndet, nt = int(ndet), int(nt)
-        if ndet <= 0 or nt <= 0 or (ndet * nt) % 32:
-            raise RuntimeError(f"HostPipeline: ndet*nt = {ndet * nt} must be a positive multiple of 32")
         if nslots < 1:
             raise RuntimeError("HostPipeline: nslots must be >= 1")
         self.lpix = local_pixelization
         self.ndet, self.nt = ndet, nt
-        step = 1
-        while (step * nt) % 32:
-            step += 1                        # detectors per chunk must keep chunks a multiple of 32 samples
-        cd = int(chunk_dets) if chunk_dets else max(1, (1 << 24) // nt)
-        cd = min(ndet, max(step, (cd // step) * step))
+        cd, self.chunks = chunk_plan(ndet, nt, chunk_dets)
         self.chunk_dets = cd
-        self.chunks = [(d0, min(ndet, d0 + cd)) for d0 in range(0, ndet, cd)]
-        if (self.chunks[-1][1] - self.chunks[-1][0]) * nt % 32:
-            raise RuntimeError("HostPipeline: the last chunk would not hold a multiple of 32 samples")
         self.nslots = min(int(nslots), len(self.chunks))
         self.tuning = tuning
         n = cd * nt
