@@ -420,8 +420,9 @@ def serving_study(rate=200.0, duration_s=2.5, ntod_pool=128, seed=5):
     against a resident 3x8192x32768 map; plan cache budget 120 GB.  (a) PointingServer (continuous
     batching) and (b) sequential plain calls (one request at a time, plans cached the same way) serve
     the same request stream at the same arrival times; latency = completion - arrival.  Then both
-    serve the same requests all at once (saturated): sustained Gsamples/s = samples processed /
-    (last completion - first arrival).  Results: map2tod of every request compared bitwise between
+    serve the same requests all at once (saturated, best of three runs per arm after one untimed
+    warm-up run of each): sustained Gsamples/s = samples processed / (last completion - first
+    arrival).  Results: map2tod of every request compared bitwise between
     (a) and (b); the tod2map output maps against the FP64 oracle."""
     import threading
     import numpy as np
@@ -493,11 +494,18 @@ def serving_study(rate=200.0, duration_s=2.5, ntod_pool=128, seed=5):
         return {"p50_ms": round(float(np.percentile(a, 50)), 3), "p99_ms": round(float(np.percentile(a, 99)), 3)}
 
     samples = sum(pool[i].shape[1] for _, _, i in reqs)
+    burst = [(0.0, k, i) for _, k, i in reqs]
+    # Warm-up of both arms (untimed): first launches of each kernel, the allocator's and the pinned
+    # host allocator's caches.
+    served(burst)
+    sequential(burst)
     res_a, map_a, st_a, _ = served(reqs)
     res_b, map_b, lat_b, _ = sequential(reqs)
-    burst = [(0.0, k, i) for _, k, i in reqs]
-    _, _, st_burst, wall_a = served(burst)
-    _, _, _, wall_b = sequential(burst)
+    # Saturated: best of three for each arm (host threads and the allocator make single runs noisy).
+    runs_a = [served(burst) for _ in range(3)]
+    best_a = min(runs_a, key=lambda r: r[3])
+    st_burst, wall_a = best_a[2], best_a[3]
+    wall_b = min(sequential(burst)[3] for _ in range(3))
     m2t_equal = all(torch.equal(ra[2], rb[2]) for ra, rb in zip(res_a, res_b) if ra[0] == "map2tod")
     t2m = [(pool[i], tods[i]) for _, kind, i in reqs if kind == "tod2map"]
     probe = g.TodBatch([x for x, _ in t2m], [t for _, t in t2m], lp)

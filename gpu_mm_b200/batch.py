@@ -140,9 +140,10 @@ class TodBatch:
                             self.plan.numel(), self.tmp.data_ptr(), self.tmp.numel(), self.tuning,
                             _stream_handle(stream))
 
-    def build_plans_each(self, stream=None):
+    def build_plans_each(self, stream=None, tmp=None):
         """The single-TOD plan of every TOD of the batch (a SinglePlan each), built together: one
-        owner pass over all TODs, one sort by (TOD, cell), one scatter (at most 4096 TODs)."""
+        owner pass over all TODs, one sort by (TOD, cell), one scatter (at most 4096 TODs).  'tmp':
+        optional uint8 CUDA scratch of at least batch_plan_each_tmp_nbytes bytes, used on 'stream'."""
         lp = self.lpix
         st = self._upload_stream if stream is None and self._upload_stream is not None else stream
         with torch.cuda.stream(st if isinstance(st, torch.cuda.Stream) else torch.cuda.current_stream()):
@@ -152,11 +153,22 @@ class TodBatch:
             self._each_ptrs = ptrs.cuda(non_blocking=True)
             tn = _m.batch_plan_each_tmp_nbytes(self.total_lines, self.ntod, lp.nypix_global, lp.nxpix_global,
                                                self.tuning)
-            self._each_tmp = torch.empty(tn, dtype=torch.uint8, device="cuda")
+            if tmp is not None and tmp.numel() >= tn:
+                self._each_tmp = tmp
+            else:
+                self._each_tmp = torch.empty(tn, dtype=torch.uint8, device="cuda")
         _m.batch_plan_build_each(self.descs.data_ptr(), self.ntod, self.total_lines, lp.nypix_global, lp.nxpix_global,
                                  bool(lp.periodic_xcoord), self._each_ptrs.data_ptr(), self._each_tmp.data_ptr(),
                                  self._each_tmp.numel(), self.tuning, self.err.data_ptr(), _stream_handle(st))
         return singles
+
+    def use_buffers(self, plan, tmp):
+        """Uses caller-owned uint8 CUDA buffers (at least batch_plan_nbytes each) for the batch plan
+        and its scratch instead of allocating them; their users must be ordered (same stream)."""
+        pn, tn = _m.batch_plan_nbytes(self.total_lines, self.lpix.nypix_global, self.lpix.nxpix_global, self.tuning)
+        if plan.numel() < pn or tmp.numel() < tn:
+            raise RuntimeError("TodBatch.use_buffers: buffers too small")
+        self.plan, self.tmp = plan[:pn], tmp[:tn]
 
     def set_tuning(self, tuning):
         """Launch/sort parameters (sort_digit_bits, ctas_per_sm, min_lines_per_cta); the plan must be

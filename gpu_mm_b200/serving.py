@@ -34,7 +34,40 @@ import time
 import numpy as np
 import torch
 
+from . import gpu_mm_pybind11 as _m
 from .batch import TodBatch
+
+
+# Streams shared by every server of the process, per device: torch's caching allocator keeps freed
+# device blocks per stream, so a server on streams of its own could not reuse what an earlier one
+# freed, and each of its allocations (plans, output TODs) would go to cudaMalloc.
+_STREAM_POOL = {}
+
+
+def _server_streams(n):
+    dev = torch.cuda.current_device()
+    pool = _STREAM_POOL.setdefault(dev, [])
+    while len(pool) < n:
+        pool.append(torch.cuda.Stream())
+    return pool[:n]
+
+
+# Grow-only scratch per server stream (batch plans and their sort space, up to ~GBs for large
+# iterations): allocated once and reused by every later iteration on that stream, which stream order
+# makes safe.  Allocating them per iteration meant a cudaMalloc of that size each time (measured up to
+# 0.2 s per iteration) because the buffers of iterations still in flight cannot be reused.
+_SCRATCH = {}
+
+
+def _scratch(stream, key, nbytes):
+    d = _SCRATCH.setdefault(stream.cuda_stream, {})
+    buf = d.get(key)
+    if buf is None or buf.numel() < nbytes:
+        size = max(int(nbytes), 2 * (buf.numel() if buf is not None else 0))
+        with torch.cuda.stream(stream):
+            buf = torch.empty(size, dtype=torch.uint8, device="cuda")
+        d[key] = buf
+    return buf
 
 
 class PointingServer:
@@ -46,9 +79,10 @@ class PointingServer:
         self.budget = int(hbm_budget_bytes)
         self.tuning = tuning
         self.max_batch = max_batch
-        self.streams = [torch.cuda.Stream() for _ in range(nstreams)]
+        self.streams = _server_streams(nstreams)
         self._next_stream = 0
         self._lock = threading.Lock()
+        self._wake = threading.Condition(self._lock)   # signalled by submit() and close()
         self._submitted = collections.deque()
         self._waiting = collections.deque()
         self._inflight = []                                # (event, requests, bytes, keepalive)
@@ -77,6 +111,7 @@ class PointingServer:
         fut = concurrent.futures.Future()
         with self._lock:
             self._submitted.append({"kind": kind, "id": tod_id, "tod": tod, "t0": time.perf_counter(), "fut": fut})
+            self._wake.notify()
         return fut
 
     def drain(self, timeout=60.0):
@@ -91,7 +126,9 @@ class PointingServer:
         raise TimeoutError("PointingServer.drain: requests still pending")
 
     def close(self):
-        self._stop = True
+        with self._lock:
+            self._stop = True
+            self._wake.notify()
         self._thread.join()
         torch.cuda.synchronize()
 
@@ -162,7 +199,15 @@ class PointingServer:
                         r["fut"].set_exception(e)
                     self._waiting.clear()
             if not progressed:
-                time.sleep(0.0002)
+                if self._inflight:
+                    # Launches on the GPU: poll their events again shortly.  (A short real sleep:
+                    # waking a condition at that rate would contend for the GIL with the clients.)
+                    time.sleep(0.0001)
+                else:
+                    # Idle: sleep until a request arrives; requests waiting for memory retry soon.
+                    with self._lock:
+                        if not self._submitted and not self._stop:
+                            self._wake.wait(timeout=0.005 if self._waiting else 0.05)
 
     def _complete(self):
         done = False
@@ -232,7 +277,10 @@ class PointingServer:
                 xps = [self.xpointings[i] for i in need]
                 builder = TodBatch(xps, [x[0] for x in xps], self.lpix, tuning=self.tuning, upload_stream=stream,
                                    plan_buffers=False)
-                singles = builder.build_plans_each(stream)
+                lp = self.lpix
+                tn = _m.batch_plan_each_tmp_nbytes(builder.total_lines, builder.ntod, lp.nypix_global,
+                                                   lp.nxpix_global, builder.tuning)
+                singles = builder.build_plans_each(stream, tmp=_scratch(stream, "each_tmp", tn))
                 ev = torch.cuda.Event()
                 ev.record(stream)
                 for i, sp in zip(need, singles):
@@ -259,7 +307,10 @@ class PointingServer:
                         r["result"] = t
                 else:
                     tods = [r["tod"] for r in reqs]
-                b = TodBatch(xps, tods, self.lpix, tuning=self.tuning, upload_stream=stream)
+                b = TodBatch(xps, tods, self.lpix, tuning=self.tuning, upload_stream=stream, plan_buffers=False)
+                pn, tn = _m.batch_plan_nbytes(b.total_lines, self.lpix.nypix_global, self.lpix.nxpix_global,
+                                              b.tuning)
+                b.use_buffers(_scratch(stream, "plan_" + kind, pn), _scratch(stream, "tmp_" + kind, tn))
                 b.merge_plans([p[0] for p in plans], stream)
                 if kind == "map2tod":
                     b.map2tod(self.in_map, stream=stream)
