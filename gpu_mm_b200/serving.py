@@ -4,7 +4,8 @@ PointingServer keeps a pool of TODs' pointing, a resident input map (read by map
 map (into which tod2map accumulates) on the device, and serves three kinds of requests:
 
   * ('plan', tod_id):    build the TOD's plan and keep it in the device plan cache;
-  * ('map2tod', tod_id): the TOD's samples from the input map (a new device array per request);
+  * ('map2tod', tod_id): the TOD's samples from the input map (a new device array per request: a
+                         view into one allocation per launch);
   * ('tod2map', tod_id, tod): accumulate a TOD array into the output map.
 
 A worker thread runs the loop.  Every iteration it
@@ -131,6 +132,11 @@ class PointingServer:
             self._wake.notify()
         self._thread.join()
         torch.cuda.synchronize()
+        # Release the plan cache and the launches' buffers now rather than when the server object is
+        # collected, so that a later server's allocations can reuse the blocks.
+        self._plans.clear()
+        self._inflight = []
+        self._used = 0
 
     def stats(self):
         out = {}
@@ -302,7 +308,11 @@ class PointingServer:
                     stream.wait_event(ev)
                 xps = [self.xpointings[r["id"]] for r in reqs]
                 if kind == "map2tod":
-                    tods = [torch.empty(x.shape[1:], device="cuda") for x in xps]
+                    # One allocation per iteration, a view per request (16-byte aligned: nsamp is a
+                    # multiple of 32); the block is freed when the last of its results is dropped.
+                    sizes = [x[0].numel() for x in xps]
+                    flat = torch.empty(sum(sizes), device="cuda")
+                    tods = [v.view(x.shape[1:]) for v, x in zip(flat.split(sizes), xps)]
                     for r, t in zip(reqs, tods):
                         r["result"] = t
                 else:
