@@ -1,0 +1,104 @@
+"""GPU tests at the full size of the large raster workload: 1024 detectors (32x32, 2 px spacing) x
+2^18 samples (nsamp = 2^28), x sweep 0.7 px/sample over a periodic 3x8192x32768 map, LocalPixelization
+holding the hit cells.  The oracle would take minutes over the whole TOD, so the checks here are the
+size-independent properties of the operators:
+
+  * the plan is deterministic: a second build gives the same plan words, bit for bit;
+  * planned map2tod is the same on every call of a plan-reuse loop (ten calls);
+  * planned and unplanned map2tod agree within the float32 tolerance, and map2tod is per sample, so
+    a handful of detectors checks against the oracle exactly like a small case;
+  * planned and unplanned tod2map agree within the float32 tolerance (different atomic orders);
+  * the operators are adjoint: <t, A m> = <A^T t, m> (A = map2tod), summed in float64.
+
+Tolerances as in the parity tests: rel-L1 < 1e-6 and max|a-b| / max|b| < 1e-5; the adjoint identity
+to 1e-6 of sum |t_i (A m)_i|.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from tests._common import rel_stats
+
+pytestmark = pytest.mark.gpu
+
+RL1_TOL = 1e-6
+MAX_TOL = 1e-5
+NY, NX = 8192, 32768
+
+
+@pytest.fixture(scope="module")
+def workload():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import gpu_mm_b200 as g
+    from gpu_mm_b200 import synthetic
+    xp = synthetic.config2_xpointing(device="cuda")
+    assert xp.shape == (3, 1024, 2 ** 18)
+    pp = g.PointingPrePlan(xp, NY, NX)
+    plan = g.PointingPlan(pp, xp)
+    cells = synthetic.cells_of_plan(plan.get_plan_mt())
+    lp = g.LocalPixelization.make_cells(NY, NX, cells)
+    gen = torch.Generator(device="cuda").manual_seed(2028)
+    m = torch.randn(3 * lp.npix, generator=gen, device="cuda")
+    t = torch.randn(xp.shape[1:], generator=gen, device="cuda")
+    return g, xp, pp, plan, lp, m, t
+
+
+def gpu_rel_stats(a, b):
+    """rel-L1 and max relative difference of two CUDA arrays, in float64 on the device."""
+    a, b = a.double(), b.double()
+    d = (a - b).abs()
+    return float(d.sum() / (a.abs().sum() + b.abs().sum())), float(d.max() / b.abs().max())
+
+
+def test_plan_deterministic(workload):
+    g, xp, pp, plan, lp, m, t = workload
+    pp2 = g.PointingPrePlan(xp, NY, NX)
+    assert pp2.plan_nmt == pp.plan_nmt
+    np.testing.assert_array_equal(pp2.get_nmt_cumsum(), pp.get_nmt_cumsum())
+    plan2 = g.PointingPlan(pp2, xp)
+    np.testing.assert_array_equal(plan2.get_plan_mt(), plan.get_plan_mt())
+
+
+def test_map2tod_reuse_unplanned_and_oracle_sample(workload):
+    import torch
+    g, xp, pp, plan, lp, m, t = workload
+    lmap = g.LocalMap(lp, m)
+    first = torch.empty(xp.shape[1:], device="cuda")
+    g.map2tod(first, lmap, xp, plan)
+    tod = torch.empty_like(first)
+    for _ in range(10):
+        g.map2tod(tod, lmap, xp, plan)
+        assert torch.equal(tod, first)
+    g.map2tod(tod, lmap, xp, None)
+    rl1, mx = gpu_rel_stats(tod, first)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+
+    # A sample of detectors (first, last, and two in between) against the oracle.
+    dets = [0, 17, 611, 1023]
+    xs = np.ascontiguousarray(xp[:, dets, :].cpu().numpy())
+    lp_o = oracle.Lpix(NY, NX, lp.cell_offsets_cpu, lp.ystride, lp.polstride, True)
+    want = np.zeros(xs.shape[1:], np.float32)
+    err = oracle.map2tod(want, m.cpu().numpy(), xs, lp_o)
+    assert err == 0
+    rl1, mx = rel_stats(first[dets].cpu().numpy(), want)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+
+
+def test_tod2map_planned_unplanned_and_adjoint(workload):
+    import torch
+    g, xp, pp, plan, lp, m, t = workload
+    out_p = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+    g.tod2map(out_p, t, xp, plan)
+    out_u = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+    g.tod2map(out_u, t, xp, None)
+    rl1, mx = gpu_rel_stats(out_p.arr, out_u.arr)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+
+    am = torch.empty(xp.shape[1:], device="cuda")
+    g.map2tod(am, g.LocalMap(lp, m), xp, plan)
+    lhs = float((t.double() * am.double()).sum())
+    rhs = float((out_p.arr.double() * m.double()).sum())
+    scale = float((t.double() * am.double()).abs().sum())
+    assert abs(lhs - rhs) < 1e-6 * scale, (lhs, rhs, scale)
