@@ -420,9 +420,9 @@ def serving_study(rate=200.0, duration_s=2.5, ntod_pool=128, seed=5):
     against a resident 3x8192x32768 map; plan cache budget 120 GB.  (a) PointingServer (continuous
     batching) and (b) sequential plain calls (one request at a time, plans cached the same way) serve
     the same request stream at the same arrival times; latency = completion - arrival.  Then both
-    serve the same requests all at once (saturated, best of three runs per arm after one untimed
-    warm-up run of each): sustained Gsamples/s = samples processed / (last completion - first
-    arrival).  Results: map2tod of every request compared bitwise between
+    serve the same requests all at once (saturated, best of three runs per arm): sustained
+    Gsamples/s = samples processed / (last completion - first arrival).  Each arm first serves the
+    burst and the Poisson stream once, untimed.  Results: map2tod of every request compared bitwise between
     (a) and (b); the tod2map output maps against the FP64 oracle."""
     import threading
     import numpy as np
@@ -495,10 +495,14 @@ def serving_study(rate=200.0, duration_s=2.5, ntod_pool=128, seed=5):
 
     samples = sum(pool[i].shape[1] for _, _, i in reqs)
     burst = [(0.0, k, i) for _, k, i in reqs]
-    # Warm-up of both arms (untimed): first launches of each kernel, the allocator's and the pinned
-    # host allocator's caches.
+    # Warm-up of both arms (untimed), on the burst and on the Poisson stream: first launches of each
+    # kernel, and the device and pinned host allocators' caches (the device allocator caches blocks
+    # per stream, and the Poisson run's small launches land on the server's streams differently
+    # from the burst's).
     served(burst)
     sequential(burst)
+    served(reqs)
+    sequential(reqs)
     res_a, map_a, st_a, _ = served(reqs)
     res_b, map_b, lat_b, _ = sequential(reqs)
     # Saturated: best of three for each arm (host threads and the allocator make single runs noisy).

@@ -17,8 +17,11 @@ A worker thread runs the loop.  Every iteration it
      and operator requests whose plan is not cached), all built together into single-TOD plans; then
      all admitted map2tod requests as one TodBatch whose plan is merged from the cached single-TOD
      plans, then all admitted tod2map requests likewise -- so requests that arrive while others are
-     on the GPU join the next launch, and launches of successive iterations overlap;
-  3. completes the requests whose launches have finished (CUDA events) and releases their memory.
+     on the GPU join the next launch, and launches of successive iterations overlap (a launch of
+     one TOD uses its cached plan as is).
+
+A completion thread waits on each launch's CUDA event in launch order, completes its requests and
+returns their memory to the budget, waking the worker for requests that wait for memory.
 
 Results do not depend on the mix: map2tod evaluates every sample with the same rounded operations as
 the single-TOD operator (bit-identical), and tod2map adds the same per-sample contributions into the
@@ -86,7 +89,11 @@ class PointingServer:
         self._wake = threading.Condition(self._lock)   # signalled by submit() and close()
         self._submitted = collections.deque()
         self._waiting = collections.deque()
-        self._inflight = []                                # (event, requests, bytes, keepalive)
+        self._inflight = collections.deque()               # (event, requests, bytes, keepalive), launch order
+        self._done = threading.Condition(self._lock)       # signalled when a launch is queued, and at exit
+        self._freed = 0                                    # bytes released by completions, not yet in _used
+        self._worker_done = False
+        self._launching = False                            # admitted requests between queues (see drain)
         self._plans = collections.OrderedDict()            # tod_id -> (single TodBatch, ready event, nbytes)
         self._used = 0
         self._stop = False
@@ -98,7 +105,9 @@ class PointingServer:
         self.errors = []
         self._errwords = []
         self._thread = threading.Thread(target=self._run, daemon=True)
+        self._completer = threading.Thread(target=self._complete_loop, daemon=True)
         self._thread.start()
+        self._completer.start()
 
     # ---- client side ----
 
@@ -120,10 +129,10 @@ class PointingServer:
         t_end = time.perf_counter() + timeout
         while time.perf_counter() < t_end:
             with self._lock:
-                busy = bool(self._submitted or self._waiting or self._inflight)
+                busy = bool(self._submitted or self._waiting or self._inflight or self._launching)
             if not busy:
                 return
-            time.sleep(0.0005)
+            time.sleep(0.0002)
         raise TimeoutError("PointingServer.drain: requests still pending")
 
     def close(self):
@@ -131,11 +140,12 @@ class PointingServer:
             self._stop = True
             self._wake.notify()
         self._thread.join()
+        self._completer.join()
         torch.cuda.synchronize()
         # Release the plan cache and the launches' buffers now rather than when the server object is
         # collected, so that a later server's allocations can reuse the blocks.
         self._plans.clear()
-        self._inflight = []
+        self._inflight.clear()
         self._used = 0
 
     def stats(self):
@@ -191,46 +201,67 @@ class PointingServer:
         return s
 
     def _run(self):
-        while not self._stop:
-            with self._lock:
-                while self._submitted:
-                    self._waiting.append(self._submitted.popleft())
-            try:
-                progressed = self._complete()
-                progressed |= self._launch()
-            except Exception as e:   # surfaced to the waiting requests
-                self.errors.append(repr(e))
+        try:
+            while not self._stop:
                 with self._lock:
-                    for r in list(self._waiting):
-                        r["fut"].set_exception(e)
-                    self._waiting.clear()
-            if not progressed:
-                if self._inflight:
-                    # Launches on the GPU: poll their events again shortly.  (A short real sleep:
-                    # waking a condition at that rate would contend for the GIL with the clients.)
-                    time.sleep(0.0001)
-                else:
-                    # Idle: sleep until a request arrives; requests waiting for memory retry soon.
+                    while self._submitted:
+                        self._waiting.append(self._submitted.popleft())
+                    self._used -= self._freed
+                    self._freed = 0
+                    self._launching = bool(self._waiting)
+                try:
+                    launched = self._launch()
+                except Exception as e:   # surfaced to the waiting requests
+                    launched = False
+                    self.errors.append(repr(e))
                     with self._lock:
-                        if not self._submitted and not self._stop:
+                        for r in list(self._waiting):
+                            r["fut"].set_exception(e)
+                        self._waiting.clear()
+                finally:
+                    self._launching = False
+                if not launched:
+                    # Nothing to launch: sleep until a request arrives or a completion frees memory
+                    # (requests waiting for memory also retry after a short timeout).
+                    with self._lock:
+                        if not (self._submitted or self._freed or self._stop):
                             self._wake.wait(timeout=0.005 if self._waiting else 0.05)
+        finally:
+            with self._lock:
+                self._worker_done = True
+                self._done.notify()
 
-    def _complete(self):
-        done = False
-        keep = []
-        for ev, reqs, nb, keepalive in self._inflight:
-            if ev.query():
-                t1 = time.perf_counter()
+    def _complete_loop(self):
+        """Completion thread: waits for the oldest launch's event (the wait releases the GIL), then
+        completes its requests and hands the memory back to the worker.  Launches on different
+        streams may finish out of order; a later one is then completed right after the earlier."""
+        while True:
+            with self._lock:
+                while not self._inflight and not self._worker_done:
+                    self._done.wait(timeout=0.05)
+                if not self._inflight:
+                    return
+                ev, reqs, nb, keepalive = self._inflight[0]
+            err = None
+            try:
+                ev.synchronize()
+            except Exception as e:
+                err = e
+                self.errors.append(repr(e))
+            t1 = time.perf_counter()
+            with self._lock:
+                self._inflight.popleft()
+                self._freed += nb
                 for r in reqs:
                     self.latencies[r["kind"]].append(t1 - r["t0"])
-                    if not r["fut"].done():
+                self._wake.notify()
+            for r in reqs:
+                if not r["fut"].done():
+                    if err is None:
                         r["fut"].set_result(r.get("result"))
-                self._used -= nb
-                done = True
-            else:
-                keep.append((ev, reqs, nb, keepalive))
-        self._inflight = keep
-        return done
+                    else:
+                        r["fut"].set_exception(err)
+            del keepalive
 
     def _launch(self):
         # A plan this iteration builds is reserved when its first request is admitted, so that the
@@ -318,10 +349,16 @@ class PointingServer:
                 else:
                     tods = [r["tod"] for r in reqs]
                 b = TodBatch(xps, tods, self.lpix, tuning=self.tuning, upload_stream=stream, plan_buffers=False)
-                pn, tn = _m.batch_plan_nbytes(b.total_lines, self.lpix.nypix_global, self.lpix.nxpix_global,
-                                              b.tuning)
-                b.use_buffers(_scratch(stream, "plan_" + kind, pn), _scratch(stream, "tmp_" + kind, tn))
-                b.merge_plans([p[0] for p in plans], stream)
+                if len(plans) == 1:
+                    # One TOD: its cached plan is already the batch plan (a merge of one plan gives
+                    # the same words).  The reference keeps it alive until the launch completes.
+                    b.plan = plans[0][0].plan
+                    b._merge_refs = [plans[0][0]]
+                else:
+                    pn, tn = _m.batch_plan_nbytes(b.total_lines, self.lpix.nypix_global, self.lpix.nxpix_global,
+                                                  b.tuning)
+                    b.use_buffers(_scratch(stream, "plan_" + kind, pn), _scratch(stream, "tmp_" + kind, tn))
+                    b.merge_plans([p[0] for p in plans], stream)
                 if kind == "map2tod":
                     b.map2tod(self.in_map, stream=stream)
                 else:
@@ -333,7 +370,9 @@ class PointingServer:
             ev = torch.cuda.Event()
             ev.record(stream)
         nb = sum(self._request_nbytes(r) for r in admitted)
-        self._inflight.append((ev, admitted, nb, keep))
+        with self._lock:
+            self._inflight.append((ev, admitted, nb, keep))
+            self._done.notify()
         return True
 
     def check(self):
