@@ -129,3 +129,33 @@ def test_serving_rejects_bad_requests(g):
     with pytest.raises(ValueError):
         srv.submit("bogus", 0)
     srv.close()
+
+
+def test_serving_reports_errors_and_keeps_serving(g):
+    """Device error bits from a plan build reach check(); a request whose launch fails on the host
+    fails alone (its future raises) and the server goes on serving later requests."""
+    import torch
+    ny, nx = 256, 512
+    rng, xps, tods = pool(13, n=3)
+    xps[0] = xps[0].copy()
+    xps[0][0, 0, 7] = ny + 3.0                       # a y outside the map in TOD 0
+    lp = g.LocalPixelization.make_rectangle(ny, nx, True)
+    xg = {i: torch.from_numpy(x).cuda() for i, x in xps.items()}
+    m = torch.from_numpy(rng.standard_normal(3 * lp.npix).astype(np.float32)).cuda()
+    srv = g.PointingServer(xg, m, torch.zeros(3 * lp.npix, device="cuda"), lp, hbm_budget_bytes=1 << 30)
+    try:
+        srv.submit("plan", 0).result(timeout=30)
+        srv.drain()
+        with pytest.raises(RuntimeError, match="device error bits"):
+            srv.check()
+        bad = srv.submit("tod2map", 1, tod=torch.zeros(7, device="cuda"))    # wrong shape
+        with pytest.raises(RuntimeError, match="shape"):
+            bad.result(timeout=30)
+        assert srv.errors
+        r = srv.submit("map2tod", 1).result(timeout=30)
+        srv.drain()
+    finally:
+        srv.close()
+    alone = torch.zeros(xps[1].shape[1:], device="cuda")
+    g.map2tod(alone, g.LocalMap(lp, m), xg[1], None)
+    assert torch.equal(r, alone)
