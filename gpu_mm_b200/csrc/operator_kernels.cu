@@ -872,7 +872,6 @@ unplanned_kernel(OpArgs a)
             err |= locate(y[k], x[k], a.ny, a.nx, a.periodic, L);
             float sn, cs;
             sincos2a(al[k], &sn, &cs);
-            const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
             if constexpr (TOD2MAP) {
                 const float t = tv[k], q = t * cs, u = t * sn;
                 window_add(a, W, L, t, q, u, err);
