@@ -63,6 +63,32 @@ __device__ __forceinline__ int analyse_line(float y, float x, int ny, int nx, bo
     return cnt;
 }
 
+// Number of (cell, line) pairs of one cache line for the preplan, by the full warp.  Every cell of
+// cell_slots has its slot fixed by its own coordinates (row parity; column 0, or column parity), so
+// the line's distinct (slot, cell) pairs are its distinct cells.  A line whose neighbours all lie in
+// a 2x2 block of cells -- every line of an ordinary scan -- is counted with four warp min/max
+// reductions and one OR of a 4-bit occupancy mask; any other line takes the slot analysis.
+__device__ __forceinline__ int count_line_cells(float y, float x, int ny, int nx, bool periodic, uint32_t &err)
+{
+    Located L;
+    const uint32_t e = locate(y, x, ny, nx, periodic, L);
+    const int cy0 = L.iy0 >> 6, cy1 = L.iy1 >> 6;            // iy1 >= iy0
+    const int cx0 = L.ix0 >> 6, cx1 = L.ix1 >> 6;            // cx1 < cx0 when x wraps
+    const int rmin = __reduce_min_sync(kFullMask, cy0);
+    const int rmax = __reduce_max_sync(kFullMask, cy1);
+    const int cmin = __reduce_min_sync(kFullMask, min(cx0, cx1));
+    const int cmax = __reduce_max_sync(kFullMask, max(cx0, cx1));
+    if ((rmax - rmin <= 1) && (cmax - cmin <= 1)) {
+        err |= e;
+        const int a0 = 2 * (cy0 - rmin), a1 = 2 * (cy1 - rmin);
+        const int b0 = cx0 - cmin, b1 = cx1 - cmin;
+        const unsigned m = (1u << (a0 + b0)) | (1u << (a0 + b1)) | (1u << (a1 + b0)) | (1u << (a1 + b1));
+        return __popc(__reduce_or_sync(kFullMask, m));
+    }
+    LineSlots ls;
+    return analyse_line(y, x, ny, nx, periodic, ls, err);
+}
+
 // Each planner block is counted by kPreplanSplit CTAs (a contiguous quarter of its lines each), which
 // add their counts into the block's word: up to 1024 planner blocks would otherwise fill the GPU
 // unevenly (about 1.4 waves).  nmt_out and err_out must be zero on entry.
@@ -95,8 +121,7 @@ preplan_count_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx
         for (int j = 0; j < kLinesPerWarp; j++) {
             if (lb + j >= l1)
                 break;
-            LineSlots ls;
-            n += analyse_line(y[j], x[j], ny, nx, periodic, ls, err);
+            n += count_line_cells(y[j], x[j], ny, nx, periodic, err);
         }
     }
 
