@@ -513,3 +513,48 @@ def test_c_abi_direct(g):
     assert rc == 0
     assert L.gmm_errword_read(ctypes.c_void_p(word.data_ptr()), 0, None) == 8
     assert L.gmm_errword_read(ctypes.c_void_p(word.data_ptr()), 8, None) == 0
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_maximum_map_size(g, periodic):
+    """The largest global map the API accepts (65536 x 65536 pixels, 1024 x 1024 cells), scanned
+    next to its last row and column of cells: cell ids reach (1023, 1023), and with periodic x the
+    scan wraps from column 65535 to column 0.  The local map holds only the hit cells.  Plans bit for
+    bit, operators against the oracle."""
+    ny = nx = 65536
+    rng = np.random.default_rng(65536 + periodic)
+    ndet, nt = 8, 1024
+    t = np.arange(nt, dtype=np.float64)[None, :]
+    d = np.arange(ndet, dtype=np.float64)[:, None]
+    y = (ny - 6.0) - 0.013 * t - 2.0 * d
+    if periodic:
+        x = 65400.0 + 0.7 * t + 1.5 * d          # reaches 66126: folds onto columns 0..590
+    else:
+        x = 65533.0 - 0.7 * t - 1.5 * d          # down from the last valid column
+    al = rng.uniform(-3.0, 3.0, (ndet, nt))
+    xp = np.stack([y, x, al]).astype(np.float32)
+    xg = cuda(xp)
+    pp, plan = build_plan(g, xg, ny, nx, periodic)
+    check_plan(g, xp, ny, nx, periodic, pp, plan)
+    from gpu_mm_b200 import synthetic
+    cells = synthetic.cells_of_plan(plan.get_plan_mt())
+    assert (1023, 1023) in cells and (not periodic or (1023, 0) in cells), cells
+    lp = g.LocalPixelization.make_cells(ny, nx, cells, periodic)
+    lp_o = oracle.Lpix(ny, nx, lp.cell_offsets_cpu, lp.ystride, lp.polstride, periodic)
+    m = rng.standard_normal(3 * lp.npix).astype(np.float32)
+    want = np.zeros(xp.shape[1:], np.float32)
+    assert oracle.map2tod(want, m, xp, lp_o) == 0
+    lmap = g.LocalMap(lp, cuda(m))
+    for pl in (plan, None):
+        tod = cuda(np.zeros(xp.shape[1:], np.float32))
+        g.map2tod(tod, lmap, xg, pl)
+        rl1, mx = rel_stats(host(tod), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, (pl is None, rl1, mx)
+    tv = rng.standard_normal(xp.shape[1:]).astype(np.float32)
+    want_m = np.zeros(3 * lp.npix, np.float32)
+    oracle.tod2map(want_m, tv, xp, lp_o)
+    for pl in (plan, None):
+        out = g.LocalMap(lp, cuda(np.zeros(3 * lp.npix, np.float32)))
+        g.tod2map(out, cuda(tv), xg, pl)
+        rl1, mx = rel_stats(host(out.arr), want_m)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, (pl is None, rl1, mx)
