@@ -8,7 +8,9 @@ size-independent properties of the operators:
   * planned and unplanned map2tod agree within the float32 tolerance, and map2tod is per sample, so
     a handful of detectors checks against the oracle exactly like a small case;
   * planned and unplanned tod2map agree within the float32 tolerance (different atomic orders);
-  * the operators are adjoint: <t, A m> = <A^T t, m> (A = map2tod), summed in float64.
+  * the operators are adjoint: <t, A m> = <A^T t, m> (A = map2tod), summed in float64;
+  * at nsamp = 2^31, the largest the API accepts, planned and unplanned operators agree and the last
+    detectors match the oracle.
 
 Tolerances as in the parity tests: rel-L1 < 1e-6 and max|a-b| / max|b| < 1e-5; the adjoint identity
 to 1e-6 of sum |t_i (A m)_i|.
@@ -45,11 +47,19 @@ def workload():
     return g, xp, pp, plan, lp, m, t
 
 
-def gpu_rel_stats(a, b):
-    """rel-L1 and max relative difference of two CUDA arrays, in float64 on the device."""
-    a, b = a.double(), b.double()
-    d = (a - b).abs()
-    return float(d.sum() / (a.abs().sum() + b.abs().sum())), float(d.max() / b.abs().max())
+def gpu_rel_stats(a, b, chunk=1 << 26):
+    """rel-L1 and max relative difference of two CUDA arrays, in float64 on the device, a chunk of
+    elements at a time (so that 2^31-element arrays need no full-size float64 copies)."""
+    a, b = a.reshape(-1), b.reshape(-1)
+    dsum = asum = dmax = bmax = 0.0
+    for i in range(0, a.numel(), chunk):
+        ac, bc = a[i:i + chunk].double(), b[i:i + chunk].double()
+        d = (ac - bc).abs()
+        dsum += float(d.sum())
+        asum += float(ac.abs().sum() + bc.abs().sum())
+        dmax = max(dmax, float(d.max()))
+        bmax = max(bmax, float(bc.abs().max()))
+    return dsum / asum, dmax / bmax
 
 
 def test_plan_deterministic(workload):
@@ -102,3 +112,40 @@ def test_tod2map_planned_unplanned_and_adjoint(workload):
     rhs = float((out_p.arr.double() * m.double()).sum())
     scale = float((t.double() * am.double()).abs().sum())
     assert abs(lhs - rhs) < 1e-6 * scale, (lhs, rhs, scale)
+
+
+def test_largest_nsamp():
+    """nsamp = 2^31, the largest the API accepts (8192 detectors x 2^18 samples, the same raster
+    construction; a periodic 3x8192x32768 rectangle map): the last samples sit at the top of the
+    32-bit sample index range.  Planned and unplanned operators agree, and the last two detectors'
+    map2tod matches the oracle."""
+    import torch
+    import gpu_mm_b200 as g
+    from gpu_mm_b200 import synthetic
+    xp = synthetic.raster_xpointing(256, 32, 2 ** 18, 2.0, 0.7, NX, 100.0, 2.0e-4, device="cuda")
+    assert xp[0].numel() == 2 ** 31
+    plan = g.PointingPlan(g.PointingPrePlan(xp, NY, NX), xp)
+    lp = g.LocalPixelization.make_rectangle(NY, NX, True)
+    gen = torch.Generator(device="cuda").manual_seed(2031)
+    m = torch.randn(3 * lp.npix, generator=gen, device="cuda")
+    lmap = g.LocalMap(lp, m)
+    tod_p = torch.empty(xp.shape[1:], device="cuda")
+    g.map2tod(tod_p, lmap, xp, plan)
+    tod_u = torch.empty_like(tod_p)
+    g.map2tod(tod_u, lmap, xp, None)
+    rl1, mx = gpu_rel_stats(tod_p, tod_u)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+    del tod_u
+    xs = np.ascontiguousarray(xp[:, -2:, :].cpu().numpy())
+    want = np.zeros(xs.shape[1:], np.float32)
+    assert oracle.map2tod(want, m.cpu().numpy(), xs, oracle.Lpix.rectangle(NY, NX, True)) == 0
+    rl1, mx = rel_stats(tod_p[-2:].cpu().numpy(), want)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+    t = tod_p
+    t.normal_(generator=gen)
+    out_p = torch.zeros(3 * lp.npix, device="cuda")
+    g.tod2map(g.LocalMap(lp, out_p), t, xp, plan)
+    out_u = torch.zeros(3 * lp.npix, device="cuda")
+    g.tod2map(g.LocalMap(lp, out_u), t, xp, None)
+    rl1, mx = gpu_rel_stats(out_p, out_u)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
