@@ -103,6 +103,13 @@ def test_invalid_arguments_rejected_before_device_work(lib):
                          ctypes.c_void_p(16), 0, None, ctypes.byref(info))
     assert rc == 0x100
     assert b"multiple of 32" in lib.gmm_last_error()
+    # empty and oversized TODs: nsamp must be in [32, 2^31]
+    for nsamp in (0, -32, (1 << 31) + 32):
+        rc = lib.gmm_preplan(ctypes.c_void_p(16), ctypes.c_int64(nsamp), 100, 100, 1, ctypes.c_void_p(16),
+                             ctypes.c_void_p(16), 0, None, ctypes.byref(info))
+        assert rc == 0x100 and b"nsamp" in lib.gmm_last_error(), nsamp
+    assert lib.gmm_preplan_info_init(ctypes.c_int64(1 << 31), 100, 100, 1, ctypes.c_int64(1 << 26),
+                                     ctypes.byref(info)) == 0
     # map too large (check_arguments.cu:28-39)
     rc = lib.gmm_preplan(ctypes.c_void_p(16), ctypes.c_int64(64), 70000, 100, 1, ctypes.c_void_p(16),
                          ctypes.c_void_p(16), 0, None, ctypes.byref(info))
