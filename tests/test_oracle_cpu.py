@@ -198,3 +198,42 @@ def test_errors_reported():
     offs[0, 0] = -1
     lp2 = oracle.Lpix(50, 80, offs, lp.ystride, lp.polstride, False)
     assert oracle.map2tod(t, m, xp, lp2) & oracle.ERR_NOT_IN_PIXELIZATION
+
+
+@pytest.mark.parametrize("ny,nx,periodic", [(300, 400, True), (300, 400, False), (130, 64, True), (200, 128, True),
+                                            (65536, 65536, True)])
+def test_line_count_is_distinct_cells(ny, nx, periodic):
+    """A cache line's number of (cell, line) pairs -- distinct valid (slot, cell) values over its 32
+    samples' six cell_enumerator slots -- equals its number of distinct cells among the samples'
+    bilinear neighbours: each cell's slot is fixed by its own coordinates (row parity; column 0 or
+    column parity).  The preplan's warp-reduction count relies on this.  Lines: scans near cell
+    corners, the x wrap, and scattered samples."""
+    rng = np.random.default_rng(ny + nx + periodic)
+    nl = 96
+    xp = np.zeros((3, nl, 32), dtype=np.float64)
+    t = np.arange(32)
+    for i in range(nl):
+        kind = i % 3
+        y0 = rng.uniform(0, ny - 2)
+        x0 = rng.uniform(-nx if periodic else 0, (2 * nx if periodic else nx - 1))
+        if kind == 0:       # a scan through a cell corner
+            cy, cx = 64 * rng.integers(1, max(2, ny // 64)), 64 * rng.integers(0, max(1, nx // 64))
+            y0, x0 = cy - rng.uniform(0, 1.5), cx - rng.uniform(0, 20)
+        if kind == 2:       # scattered samples
+            xp[0, i] = rng.uniform(0, ny - 1, 32)
+            xp[1, i] = rng.uniform(-nx if periodic else 0, (2 * nx if periodic else nx - 1), 32)
+            continue
+        sp = rng.choice([-1.0, 1.0]) * rng.uniform(0.2, 1.2)
+        xp[0, i] = np.clip(y0 + 0.01 * t, 0, ny - 1)
+        x = x0 + sp * t
+        xp[1, i] = x if periodic else np.clip(x, 0, nx - 1)
+    xp = xp.astype(np.float32)
+    counts = oracle.line_counts(xp, ny, nx, periodic)
+    located = _locate_all(xp, ny, nx, periodic)
+    for line in range(nl):
+        cells = set()
+        for (iy0, iy1, ix0, ix1) in located[32 * line: 32 * line + 32]:
+            for iy in (iy0, iy1):
+                for ix in (ix0, ix1):
+                    cells.add((iy >> 6, ix >> 6))
+        assert counts[line] == len(cells), (line, counts[line], sorted(cells))
