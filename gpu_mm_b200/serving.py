@@ -74,6 +74,14 @@ def _scratch(stream, key, nbytes):
     return buf
 
 
+def release_scratch():
+    """Frees the scratch buffers that servers share (batch plans and their sort space, kept per
+    stream between servers).  Call it only while no PointingServer is running; later servers
+    allocate the buffers again."""
+    torch.cuda.synchronize()
+    _SCRATCH.clear()
+
+
 class PointingServer:
     def __init__(self, xpointings, in_map, out_map, local_pixelization, hbm_budget_bytes, nstreams=3,
                  max_batch=256, tuning=None):
