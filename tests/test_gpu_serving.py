@@ -159,3 +159,5 @@ def test_serving_reports_errors_and_keeps_serving(g):
     alone = torch.zeros(xps[1].shape[1:], device="cuda")
     g.map2tod(alone, g.LocalMap(lp, m), xg[1], None)
     assert torch.equal(r, alone)
+    g.serving.release_scratch()          # no server running: the shared scratch can go
+    assert not g.serving._SCRATCH
