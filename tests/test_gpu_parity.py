@@ -6,7 +6,6 @@ Tolerances (float32 operators): rel-L1 = sum|a-b| / (sum|a|+sum|b|) < 1e-6, the 
 """
 
 import ctypes
-import os
 
 import numpy as np
 import pytest
