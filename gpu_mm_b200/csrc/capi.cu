@@ -36,7 +36,7 @@ namespace {
 
 thread_local std::string g_last_error;
 
-// Maximum radix digit width used by the plan sort; chosen by the autotuner (tuning.py) via
+// Maximum radix digit width used by the plan sort; chosen by the autotuner (autotune.py) via
 // gmm_set_sort_digit_bits, default 8.
 int g_sort_max_digit_bits = 8;
 
@@ -229,6 +229,24 @@ int gmm_set_sort_digit_bits(int32_t bits)
 
 int gmm_get_sort_digit_bits(void) { return g_sort_max_digit_bits; }
 
+int gmm_set_planned_tod2map_kernel(int32_t which)
+{
+    if ((which != GMM_TOD2MAP_BANDS) && (which != GMM_TOD2MAP_TILES))
+        return fail(GMM_ERR_INVALID_ARGUMENT, "gmm_set_planned_tod2map_kernel: expected GMM_TOD2MAP_BANDS or GMM_TOD2MAP_TILES");
+    g_tod2map_kernel = which;
+    return 0;
+}
+
+int gmm_get_planned_tod2map_kernel(void) { return g_tod2map_kernel; }
+
+// Passes and digit width of the owner-list sort of a single-TOD plan: by (cell, row band), kBandBits
+// more key bits than the plan-word sort, with digits at most max(cell_dbits, kBandBits) wide (the sort
+// scratch of gmm_preplan_info_init is sized for the wider of the two sorts).
+static int owner_sort_passes(int nyc, int nxc, int cell_dbits, int *obits)
+{
+    return sort_passes(nyc, nxc, std::max(cell_dbits, kBandBits), obits, kBandBits);
+}
+
 int gmm_preplan_info_init(int64_t nsamp, int32_t ny, int32_t nx, int32_t periodic, int64_t nmt, gmm_preplan_info *info)
 {
     const char *where = "PointingPrePlan constructor";
@@ -255,10 +273,11 @@ int gmm_preplan_info_init(int64_t nsamp, int32_t ny, int32_t nx, int32_t periodi
     info->pointing_nblocks = (nmt + nmt_per_tb - 1) / nmt_per_tb;
     info->overhead = 32 * nmt / double(nsamp) - 1.0;
 
-    int dbits = 0;
+    int dbits = 0, obits = 0;
     sort_passes((ny + 63) / 64, (nx + 63) / 64, g_sort_max_digit_bits, &dbits);
+    owner_sort_passes((ny + 63) / 64, (nx + 63) / 64, dbits, &obits);
     info->sort_digit_bits = dbits;
-    info->sort_nbytes = sort_scratch_nbytes(dbits, kSortGridMax);
+    info->sort_nbytes = sort_scratch_nbytes(std::max(dbits, obits), kSortGridMax);
 
     const int64_t ncl = nsamp / 32;
     const int64_t max_nblocks = std::max(info->planner_nblocks, info->pointing_nblocks);
@@ -347,17 +366,21 @@ int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum, con
     if (dbits > info->sort_digit_bits && info->sort_digit_bits > 0)
         return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": preplan sort digit width mismatch");
     const bool even = (passes % 2) == 0;
+    int obits = 0;
+    const int opasses = owner_sort_passes(nyc, nxc, dbits, &obits);
+    const bool oeven = (opasses % 2) == 0;
 
     const int64_t err_nbytes = lay.owner_offset - lay.err_offset;
     cudaError_t e = cudaMemsetAsync(errflags, 0, err_nbytes, stream);
     if (e == cudaSuccess)
         e = launch_plan_emit(xp, info->nsamp, info->nypix_global, info->nxpix_global, info->periodic_xcoord != 0,
                              info->ncl_per_threadblock, (int) info->planner_nblocks, nmt_cumsum,
-                             even ? plan_mt : mt_alt, even ? owner : owner_alt, errflags, stream);
+                             even ? plan_mt : mt_alt, oeven ? owner : owner_alt, errflags, stream);
     if (e == cudaSuccess)
         e = radix_sort_mt(even ? plan_mt : mt_alt, even ? mt_alt : plan_mt, nmt, nyc, nxc, dbits, passes, hist, stream);
     if (e == cudaSuccess)
-        e = radix_sort_mt(even ? owner : owner_alt, even ? owner_alt : owner, ncl, nyc, nxc, dbits, passes, hist, stream);
+        e = radix_sort_mt(oeven ? owner : owner_alt, oeven ? owner_alt : owner, ncl, nyc, nxc, obits, opasses, hist,
+                          stream, 0, kBandBits);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(cellmap, 0, kCellmapBytes, stream);
     if (e == cudaSuccess)

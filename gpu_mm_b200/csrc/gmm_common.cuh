@@ -23,6 +23,13 @@ constexpr uint64_t kClMask = (1ull << 26) - 1;
 constexpr uint64_t kMflag = 1ull << 46;
 constexpr uint64_t kZflag = 1ull << 47;
 
+// Owner words of single-TOD plans (one per cache line: its lowest cell | line << 20 | mflag << 46)
+// carry the line's row band in bits 48-53: the row of its first sample's upper bilinear neighbours,
+// relative to the owner cell's first row, clamped to [0, 63].  The owner list is sorted by
+// (cell, band, line).
+constexpr int kBandShift = 48;
+constexpr int kBandBits = 6;
+
 struct Located {
     int iy0, iy1, ix0, ix1;
     float dy, dx;

@@ -20,12 +20,13 @@ int device_sm_count();
 int report_err_bits(uint32_t err, const char *where, uint32_t ignore);
 
 // ---- plan construction (plan_kernels.cu) ----
-// Radix sort of plan words by cell (and, with tod_bits > 0, by TOD index above the cell).
+// Radix sort of plan words by cell (and, with tod_bits > 0, by TOD index above the cell; the owner
+// words of single-TOD plans by (cell, row band), kBandBits more key bits, passed as tod_bits here).
 int sort_passes(int nycells_max, int nxcells_max, int max_digit_bits, int *digit_bits, int tod_bits = 0);
 int64_t sort_scratch_nbytes(int digit_bits, int grid);
 int sort_grid_for(int64_t n);
 cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, int nxcells_max, int digit_bits,
-                          int npasses, uint32_t *hist, cudaStream_t stream, int tod_bits = 0);
+                          int npasses, uint32_t *hist, cudaStream_t stream, int tod_bits = 0, int band_bits = 0);
 cudaError_t launch_preplan(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
                            int nblocks, uint32_t *nmt, uint32_t *err, cudaStream_t stream);
 cudaError_t launch_plan_emit(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
@@ -93,6 +94,9 @@ cudaError_t set_smem_limit(Kernel k, size_t nbytes, std::atomic<uint64_t> &done)
         done.fetch_or(bit, std::memory_order_release);
     return e;
 }
+
+// Kernel of the plain planned tod2map of single-TOD plans (gmm_set_planned_tod2map_kernel).
+extern int g_tod2map_kernel;
 
 cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                    cudaStream_t stream);

@@ -32,6 +32,8 @@
 
 namespace gmm {
 
+int g_tod2map_kernel = GMM_TOD2MAP_BANDS;
+
 namespace {
 
 constexpr int HX = 32;                 // halo columns on each side
@@ -750,6 +752,325 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
 }
 
 // ------------------------------------------------------------------------------------------------
+// Planned tod2map by row bands (single-TOD plans, float flush).
+//
+// The owner list of a single-TOD plan is sorted by (cell, row band, line); the band is the row of a
+// line's first sample within its owner cell.  Each warp walks a contiguous range of the list.  While
+// the (cell, band) stays the same, it accumulates in registers: rows R0 = 64 iycell + band and R0 + 1,
+// columns x0 .. x0 + 95 (x0 = 64 ixcell, unwrapped), planes T, Q, U; lane L holds the columns
+// congruent to L mod 32 (three slots of six values).  A line whose samples all lie in those rows and
+// move by at most one column per sample in one direction (a raster scan slower than 1 px/sample,
+// except at its turnarounds) is added with shuffles instead of atomics: each sample's contribution
+// is split between its two columns, the samples of one column are summed at the last lane of their
+// run, and every lane pulls the totals of the column it holds.  When the (cell, band) changes, the
+// accumulator goes into the map with one L2 reduction per pixel and plane (zeros skipped).  Other
+// lines go sample by sample straight into the map (twelve reductions each), and so do precision
+// modes and batches, which use planned_kernel.
+
+constexpr int BW = 16;                 // warps per CTA
+constexpr int BNT = BW * 32;
+constexpr int BUNR = 2;                // cache lines loaded together per warp
+constexpr uint32_t kNoKey = 0xffffffffu;
+
+struct BandState {
+    float acc[3][6];    // [slot][row * 3 + plane]; slot s holds column 32 s + lane
+    uint32_t key;       // cell | band << 20 of the accumulated lines, or kNoKey
+    int R0, x0;         // rows R0, R0 + 1; columns x0 + [0, 96) (unwrapped; mod nx with PERIODIC)
+};
+
+// Bit n of 'm', or 0 outside [0, 32).
+__device__ __forceinline__ bool bit_at(unsigned m, int n)
+{
+    return (n >= 0) && (n < 32) && ((m >> n) & 1u);
+}
+
+// Adds the accumulator into the map (one reduction per non-zero pixel and plane) and clears it.
+// Rows and columns outside the map, and absent cells, only ever hold zeros: every line the band path
+// takes has its footprint inside the map (absent cells are reported through the plan's cell bitmap).
+template<bool PERIODIC>
+__device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int sl = 0; sl < 3; sl++) {
+        int gx = B.x0 + 32 * sl + lane;
+        bool xin = true;
+        if constexpr (PERIODIC)
+            gx %= a.nx;
+        else
+            xin = gx < a.nx;
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const float t = B.acc[sl][3 * r], q = B.acc[sl][3 * r + 1], u = B.acc[sl][3 * r + 2];
+            const bool nz = (t != 0.0f) || (q != 0.0f) || (u != 0.0f);
+            if (__any_sync(kFullMask, nz) && nz && xin) {
+                const int64_t off = global_pixel_offset(B.R0 + r, gx, a);
+                if (off >= 0) {
+                    if (t != 0.0f) atomicAdd(a.out + off, t);
+                    if (q != 0.0f) atomicAdd(a.out + off + a.polstride, q);
+                    if (u != 0.0f) atomicAdd(a.out + off + 2 * a.polstride, u);
+                }
+            }
+            B.acc[sl][3 * r] = 0.0f;
+            B.acc[sl][3 * r + 1] = 0.0f;
+            B.acc[sl][3 * r + 2] = 0.0f;
+        }
+    }
+}
+
+// One cache line (lane = sample) on the band path.  Returns false, having added nothing, unless every
+// sample is valid and needs no clamp or x = nx wrap (as tile_sample), has its upper neighbours in row
+// R0, has |2a| <= 1024 and column k = ix0 - x0 (mod nx with PERIODIC) in [0, 94], and unless k moves
+// along the line in one direction by 0 or 1 per sample, stays in one column for at most four
+// consecutive samples, and repeats at least once (so that the line covers at most 32 columns and
+// some lane holds no column total).  'tab' is the warp's 32-entry table.
+template<bool RESP, bool PERIODIC>
+__device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint16_t *tab, float y, float x, float al,
+                                          float tv, uint32_t s)
+{
+    const int lane = threadIdx.x & 31;
+    bool ok = (y >= 0.0f) && (y < (float) (a.ny - 1));
+    const int iy0 = __float2int_rz(y);
+    const float dy = y - (float) iy0;
+    int ix0;
+    float dx;
+    if constexpr (PERIODIC) {
+        const float fnx = (float) a.nx;
+        float xf = (x >= 0.0f) ? x : (x + fnx);
+        xf = (xf <= fnx) ? xf : (xf - fnx);
+        ok = ok && (xf >= 0.0f) && (xf < fnx);
+        ix0 = __float2int_rz(xf);
+        dx = xf - (float) ix0;
+    } else {
+        ok = ok && (x >= 0.0f) && (x < (float) (a.nx - 2));
+        ix0 = __float2int_rz(x);
+        dx = x - (float) ix0;
+    }
+    int k = ix0 - B.x0;
+    if constexpr (PERIODIC)
+        k += (k < 0) ? a.nx : 0;
+    const float th = 2.0f * al;
+    ok = ok && (iy0 == B.R0) && ((unsigned) k <= 94u) && (fabsf(th) <= 1024.0f);
+    const int dk = k - __shfl_up_sync(kFullMask, k, 1);
+    const unsigned su = __ballot_sync(kFullMask, (lane > 0) && (dk == 0));   // bit i: k[i] == k[i-1]
+    const bool all_ok = __all_sync(kFullMask, ok);
+    const bool inc = __all_sync(kFullMask, (lane == 0) || (dk == 0) || (dk == 1));
+    const bool dec = __all_sync(kFullMask, (lane == 0) || (dk == 0) || (dk == -1));
+    const unsigned r3 = su & (su >> 1);      // runs of three or more samples in one column
+    const unsigned r5 = r3 & (r3 >> 2);      // runs of five or more
+    if (!(all_ok && (inc || dec) && (su != 0u) && (r5 == 0u)))
+        return false;
+
+    // Lanes in scan order ("virtual" order): lane order if x increases, reversed if it decreases.
+    const int dir = inc ? 1 : -1;
+    float sn, cs;
+    sincos_reduced(th, &sn, &cs);
+    float ft, fq, fu;
+    if constexpr (RESP) {
+        float tr, pr;
+        sample_response(a, s, tr, pr);
+        ft = tr * tv;
+        fq = pr * tv * cs;
+        fu = pr * tv * sn;
+    } else {
+        ft = tv;
+        fq = tv * cs;
+        fu = tv * sn;
+    }
+    const float wy0 = 1.0f - dy;
+    const float V[6] = {wy0 * ft, wy0 * fq, wy0 * fu, dy * ft, dy * fq, dy * fu};
+    // The previous sample in scan order (lane - dir); unused where it does not exist.
+    const int src = (lane - dir) & 31;
+    float Vp[6];
+#pragma unroll
+    for (int p = 0; p < 6; p++)
+        Vp[p] = __shfl_sync(kFullMask, V[p], src);
+    const float dxp = __shfl_sync(kFullMask, dx, src);
+    // Same column as the previous / next sample in scan order.
+    const bool sprev = inc ? bit_at(su, lane) : bit_at(su, lane + 1);
+    const bool snext = inc ? bit_at(su, lane + 1) : bit_at(su, lane);
+    const bool last = !snext;   // the last sample of its column holds the column's totals
+    float SA[6], SB[6];         // totals of this lane's column (weights 1 - dx) and the next (dx)
+    if (r3 == 0u) {
+        // At most two samples per column: the last one adds the previous one's share.
+        const bool lp = last && sprev;
+        const float wa = last ? 1.0f - dx : 0.0f, wb = last ? dx : 0.0f;
+        const float wap = lp ? 1.0f - dxp : 0.0f, wbp = lp ? dxp : 0.0f;
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+            SA[p] = fmaf(wap, Vp[p], wa * V[p]);
+            SB[p] = fmaf(wbp, Vp[p], wb * V[p]);
+        }
+    } else {
+        // Up to four: pairs first, then the pair two samples back if it is in the same column.
+        const float wap = sprev ? 1.0f - dxp : 0.0f, wbp = sprev ? dxp : 0.0f;
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+            SA[p] = fmaf(wap, Vp[p], (1.0f - dx) * V[p]);
+            SB[p] = fmaf(wbp, Vp[p], dx * V[p]);
+        }
+        const int src2 = (lane - 2 * dir) & 31;
+        const bool sprev2 = sprev && (inc ? bit_at(su, lane - 1) : bit_at(su, lane + 2));
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+            const float a2 = __shfl_sync(kFullMask, SA[p], src2);
+            const float b2 = __shfl_sync(kFullMask, SB[p], src2);
+            SA[p] = last ? (sprev2 ? SA[p] + a2 : SA[p]) : 0.0f;
+            SB[p] = last ? (sprev2 ? SB[p] + b2 : SB[p]) : 0.0f;
+        }
+    }
+    // Column n (in scan order) of the line is kmin + n.  tab[n] = (lane holding column n's own
+    // totals) | (lane holding column n-1's, whose dx share falls on column n) << 8.
+    const unsigned lm = __ballot_sync(kFullMask, last);
+    const unsigned lt = (1u << lane) - 1u;
+    const int n = __popc(lm & (inc ? lt : ~(lt | (1u << lane))));
+    const int ncol = __popc(lm);
+    uint8_t *tb = reinterpret_cast<uint8_t *>(tab);
+    __syncwarp();   // the previous line's reads of the table are done
+    if (last) {
+        tb[2 * n] = (uint8_t) lane;
+        tb[2 * (n + 1) + 1] = (uint8_t) lane;
+    }
+    __syncwarp();
+    const int kmin = (int) __reduce_min_sync(kFullMask, (unsigned) k);
+    const int nA = (lane - kmin) & 31;   // this lane's column kmin + nA is congruent to lane mod 32
+    const uint16_t e = tab[nA];
+    const int zl = __ffs(~lm) - 1;       // a lane whose totals are zero
+    const int srcA = (nA < ncol) ? (int) (e & 0xffu) : zl;
+    const int srcB = ((nA >= 1) && (nA <= ncol)) ? (int) (e >> 8) : zl;
+    float C[6];
+#pragma unroll
+    for (int p = 0; p < 6; p++)
+        C[p] = __shfl_sync(kFullMask, SA[p], srcA) + __shfl_sync(kFullMask, SB[p], srcB);
+    // The line spans at most 32 columns, so at most two slots: the one of kmin and the next.
+    const int slo = kmin >> 5;
+    const bool hi = ((kmin + nA) >> 5) != slo;
+    if (slo == 0) {
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+            if (hi) B.acc[1][p] += C[p];
+            else B.acc[0][p] += C[p];
+        }
+    } else if (slo == 1) {
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+            if (hi) B.acc[2][p] += C[p];
+            else B.acc[1][p] += C[p];
+        }
+    } else if (!hi) {
+#pragma unroll
+        for (int p = 0; p < 6; p++)
+            B.acc[2][p] += C[p];
+    }
+    return true;
+}
+
+// One sample of a line that the band path does not take: exact locate with error bits, then the
+// four neighbours straight into the map.
+template<bool RESP, bool PERIODIC>
+__device__ __forceinline__ void band_general_sample(const OpArgs &a, float y, float x, float al, float tv, uint32_t s,
+                                                    uint32_t &err)
+{
+    Located L;
+    err |= locate(y, x, a.ny, a.nx, PERIODIC, L);
+    float sn, cs;
+    sincos2a(al, &sn, &cs);
+    float t, q, u;
+    if constexpr (RESP) {
+        float tr, pr;
+        sample_response(a, s, tr, pr);
+        t = tr * tv;
+        q = pr * tv * cs;
+        u = pr * tv * sn;
+    } else {
+        t = tv;
+        q = tv * cs;
+        u = tv * sn;
+    }
+    const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
+    uint32_t unused = 0;
+    global_accum(a, a.out, L.iy0, L.ix0, t, q, u, wy0 * wx0, unused);
+    global_accum(a, a.out, L.iy0, L.ix1, t, q, u, wy0 * L.dx, unused);
+    global_accum(a, a.out, L.iy1, L.ix0, t, q, u, L.dy * wx0, unused);
+    global_accum(a, a.out, L.iy1, L.ix1, t, q, u, L.dy * L.dx, unused);
+}
+
+template<bool RESP, bool PERIODIC>
+__global__ void __launch_bounds__(BNT, 2)
+planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner,
+                     const uint32_t *__restrict__ cellmap)
+{
+    __shared__ uint16_t s_tab[BW][32];
+    __shared__ uint32_t s_err[BW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t nw = (int64_t) gridDim.x * BW;
+    const int64_t gw = (int64_t) blockIdx.x * BW + warp;
+    const int64_t e0 = (nowner * gw) / nw, e1 = (nowner * (gw + 1)) / nw;
+    const uint32_t nsamp = (uint32_t) a.nsamp;
+    const uint32_t nlines = nsamp >> 5;
+    const float *__restrict__ yrow = a.xp;
+    const float *__restrict__ xrow = a.xp + nsamp;
+    const float *__restrict__ arow = a.xp + 2 * (size_t) nsamp;
+    uint32_t err = a.partial ? 0u : check_plan_cells(cellmap, a);
+    uint16_t *tab = s_tab[warp];
+
+    BandState B;
+#pragma unroll
+    for (int sl = 0; sl < 3; sl++)
+#pragma unroll
+        for (int p = 0; p < 6; p++)
+            B.acc[sl][p] = 0.0f;
+    B.key = kNoKey;
+    B.R0 = 0;
+    B.x0 = 0;
+
+    for (int64_t c = e0; c < e1; c += 32) {
+        const int n = (int) ((e1 - c < 32) ? (e1 - c) : 32);
+        const uint64_t w = (lane < n) ? __ldg(owner_mt + c + lane) : 0ull;
+        const uint32_t wline = (uint32_t) ((w >> 20) & kClMask);
+        const uint32_t wkey = (uint32_t) (w & kCellMask) | ((uint32_t) ((w >> kBandShift) & 63u) << 20);
+        // A plan word always names a line < nsamp/32; anything else means the plan does not belong to
+        // this xpointing, so flag it and skip the line.
+        const bool bad = (lane < n) && (wline >= nlines);
+        err |= bad ? kErrInconsistentNmt : 0u;
+        const unsigned okmask = __ballot_sync(kFullMask, (lane < n) && !bad);
+        for (int j0 = 0; j0 < n; j0 += BUNR) {
+            float y[BUNR], x[BUNR], al[BUNR], tv[BUNR];
+            uint32_t key[BUNR], s[BUNR];
+            bool ok[BUNR];
+#pragma unroll
+            for (int u = 0; u < BUNR; u++) {
+                const int j = j0 + u;    // < 32: 32 is a multiple of BUNR
+                ok[u] = (okmask >> j) & 1u;
+                s[u] = (__shfl_sync(kFullMask, wline, j) << 5) + (uint32_t) lane;
+                key[u] = __shfl_sync(kFullMask, wkey, j);
+                y[u] = ok[u] ? __ldcs(yrow + s[u]) : 0.0f;
+                x[u] = ok[u] ? __ldcs(xrow + s[u]) : 0.0f;
+                al[u] = ok[u] ? __ldcs(arow + s[u]) : 0.0f;
+                tv[u] = ok[u] ? __ldcs(a.in + s[u]) : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < BUNR; u++) {
+                if (!ok[u])
+                    continue;
+                if (key[u] != B.key) {
+                    if (B.key != kNoKey)
+                        band_flush<PERIODIC>(a, B);
+                    B.key = key[u];
+                    B.R0 = ((int) ((key[u] >> 10) & 1023u) << 6) + (int) (key[u] >> 20);
+                    B.x0 = (int) (key[u] & 1023u) << 6;
+                }
+                if (!band_line<RESP, PERIODIC>(a, B, tab, y[u], x[u], al[u], tv[u], s[u]))
+                    band_general_sample<RESP, PERIODIC>(a, y[u], x[u], al[u], tv[u], s[u], err);
+            }
+        }
+    }
+    if (B.key != kNoKey)
+        band_flush<PERIODIC>(a, B);
+    block_publish_err(err, s_err, a.errword);
+}
+
+// ------------------------------------------------------------------------------------------------
 // Unplanned operators (map2tod_unplanned.cu:17-71, tod2map_unplanned.cu:17-66): one pass over the
 // samples, map accesses straight to global memory.  Four consecutive samples per thread with
 // 16-byte loads when the arrays are aligned.
@@ -951,6 +1272,24 @@ cudaError_t launch_planned_periodic(const OpArgs &a, const uint64_t *owner_mt, i
                       : launch_planned_impl<TOD2MAP, RESP, false, FLUSH>(a, owner_mt, nowner, cellmap, stream);
 }
 
+// Band-path tod2map: one warp per contiguous range of at least 32 owner entries, up to
+// ctas_per_sm (default 2) CTAs of BW warps per SM.
+template<bool RESP>
+cudaError_t launch_tod2map_band(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
+                                cudaStream_t stream)
+{
+    if (nowner <= 0)
+        return cudaSuccess;
+    const int per_sm = (a.ctas_per_sm > 0) ? a.ctas_per_sm : 2;
+    int64_t g = (nowner + 32 * BW - 1) / (32 * BW);
+    g = std::max<int64_t>(1, std::min<int64_t>(g, (int64_t) per_sm * device_sm_count()));
+    if (a.periodic)
+        planned_tod2map_band<RESP, true><<<(unsigned) g, BNT, 0, stream>>>(a, owner_mt, nowner, cellmap);
+    else
+        planned_tod2map_band<RESP, false><<<(unsigned) g, BNT, 0, stream>>>(a, owner_mt, nowner, cellmap);
+    return cudaGetLastError();
+}
+
 template<bool TOD2MAP, bool RESP>
 cudaError_t launch_planned_dispatch(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                     cudaStream_t stream)
@@ -960,6 +1299,8 @@ cudaError_t launch_planned_dispatch(const OpArgs &a, const uint64_t *owner_mt, i
             return launch_planned_periodic<true, RESP, kFlushCompensated>(a, owner_mt, nowner, cellmap, stream);
         if (a.flush == kFlushF64)
             return launch_planned_periodic<true, RESP, kFlushF64>(a, owner_mt, nowner, cellmap, stream);
+        if (g_tod2map_kernel == GMM_TOD2MAP_BANDS)
+            return launch_tod2map_band<RESP>(a, owner_mt, nowner, cellmap, stream);
     }
     return launch_planned_periodic<TOD2MAP, RESP, kFlushF32>(a, owner_mt, nowner, cellmap, stream);
 }

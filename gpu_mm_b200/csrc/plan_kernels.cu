@@ -203,6 +203,7 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
     __shared__ int s_off[kRoundLines];
     __shared__ int s_fill[kRoundLines];
     __shared__ int s_ring[4];
+    __shared__ int s_brow[kRoundLines];
     __shared__ int64_t s_base;
     // Slot analysis of each line of the round, kept here between the phases instead of in registers.
     __shared__ int s_slots[kRoundLines][6][32];
@@ -257,6 +258,8 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
                 for (int k = 0; k < 6; k++)
                     s_amask[li][k] = ls.amask[k];
                 s_cnt[li] = cnt;
+                // Upper footprint row of the line's first sample (locate's clamp to [0, ny-2]).
+                s_brow[li] = min(max(__float2int_rz(y[j]), 0), ny - 2);
             }
         }
         __syncthreads();
@@ -318,8 +321,10 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
                 pos += __popc(am);
             }
             minc = __reduce_min_sync(kFullMask, minc);
+            // Row band: the first sample's row within the owner cell's tile rows, clamped to [0, 63].
+            const int band = min(max(s_brow[li] - (int) ((minc >> 10) << 6), 0), 63);
             if (lane == 0)
-                owner_out[l] = (uint64_t) minc | hi;
+                owner_out[l] = (uint64_t) minc | hi | ((uint64_t) band << kBandShift);
         }
         __syncthreads();
         if (threadIdx.x == 0)
@@ -355,18 +360,21 @@ struct DigitSpec {
     uint32_t ymask;  // mask of the iycell part
     int ybits;       // bits of the iycell part
     uint32_t tmask;  // mask of the TOD index (bits 48+ of batch words) above the cell; 0: cell only
+    uint32_t lmask;  // mask of the row band (bits 48+ of single-TOD owner words) below the cell; 0: none
+    int lbits;       // bits of the row band part
     int shift;       // first compound bit of this pass
     int dbits;       // digit width of this pass
 };
 
-// Compound sort key of a word: ixcell | iycell << xbits | tod << (xbits + ybits), of which this pass
-// takes 'dbits' bits from bit 'shift'.
+// Compound sort key of a word: band | (ixcell | iycell << xbits) << lbits | tod << (lbits + xbits + ybits),
+// of which this pass takes 'dbits' bits from bit 'shift'.  A word has a band or a TOD index, not both.
 __device__ __forceinline__ uint32_t key_digit(uint64_t w, const DigitSpec &ds)
 {
     uint32_t c = (uint32_t) w;
     uint32_t ix = c & 0x3ffu, iy = (c >> 10) & 0x3ffu;
-    uint32_t comp = (ix & ds.xmask) | ((iy & ds.ymask) << ds.xbits) |
-                    (((uint32_t) (w >> 48) & ds.tmask) << (ds.xbits + ds.ybits));
+    const uint32_t hi = (uint32_t) (w >> 48);
+    uint32_t comp = (hi & ds.lmask) | (((ix & ds.xmask) | ((iy & ds.ymask) << ds.xbits)) << ds.lbits) |
+                    ((hi & ds.tmask) << (ds.lbits + ds.xbits + ds.ybits));
     return (comp >> ds.shift) & ((1u << ds.dbits) - 1u);
 }
 
@@ -596,15 +604,16 @@ static int sort_grid(int64_t n, int num_sms)
 
 int sort_grid_for(int64_t n) { return sort_grid(n, device_sm_count()); }
 
-// Sorts 'n' mt words by cell.  The input is in 'a'; the result ends in 'a' if npasses is even and in
-// 'b' if it is odd (callers place the input accordingly).
+// Sorts 'n' mt words by cell (with tod_bits > 0: by (TOD, cell); with band_bits > 0: by (cell, row band)),
+// stably.  The input is in 'a'; the result ends in 'a' if npasses is even and in 'b' if it is odd
+// (callers place the input accordingly).
 cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, int nxcells_max, int digit_bits,
-                          int npasses, uint32_t *hist, cudaStream_t stream, int tod_bits)
+                          int npasses, uint32_t *hist, cudaStream_t stream, int tod_bits, int band_bits)
 {
     if ((n <= 0) || (npasses == 0))
         return cudaSuccess;
     const int xbits = bits_for(nxcells_max), ybits = bits_for(nycells_max);
-    const int kbits = xbits + ybits + tod_bits;
+    const int kbits = xbits + ybits + tod_bits + band_bits;
     const int G = sort_grid_for(n);
     const int64_t chunk = (((n + G - 1) / G) + 255) / 256 * 256;
     constexpr int K = 8;
@@ -622,6 +631,8 @@ cudaError_t radix_sort_mt(uint64_t *a, uint64_t *b, int64_t n, int nycells_max, 
         ds.ymask = (1u << ybits) - 1u;
         ds.ybits = ybits;
         ds.tmask = (1u << tod_bits) - 1u;
+        ds.lmask = (1u << band_bits) - 1u;
+        ds.lbits = band_bits;
         ds.shift = p * digit_bits;
         ds.dbits = min(digit_bits, kbits - p * digit_bits);
         const int ndp = 1 << ds.dbits;

@@ -93,9 +93,24 @@ const char *gmm_version(void);
 
 /* Maximum radix digit width (4..11 bits) of the plan sort, used by later gmm_preplan calls.  The
  * reference's sort is CUB's (PointingPlan.cu:300-309), whose digit width is not a parameter; here
- * it is a tuning knob set by the autotuner (gpu_mm_b200/tuning.py).  Default 8. */
+ * it is a tuning knob set by the autotuner (gpu_mm_b200/autotune.py).  Default 8. */
 int gmm_set_sort_digit_bits(int32_t bits);
 int gmm_get_sort_digit_bits(void);
+
+/* Kernel of the plain (float) planned tod2map of single-TOD plans, for later calls in this process.
+ * The reference has one tod2map kernel (tod2map.cu:16-150: shared-memory tile per cell, one
+ * atomic per sample and pixel); here there are two, which give the same result within float
+ * rounding:
+ *   GMM_TOD2MAP_BANDS (default): lines grouped by (cell, row band) in the plan; each warp sums a
+ *     band's lines in registers and adds them to the map once per band;
+ *   GMM_TOD2MAP_TILES: shared-memory tile of each cell plus halo, as the precision modes and
+ *     batches use.
+ * A tuning knob: the bands kernel is faster for raster scans, the tiles kernel for pointing that
+ * is not (e.g. scans faster than one pixel per sample or rotated against the pixel grid). */
+#define GMM_TOD2MAP_BANDS 0
+#define GMM_TOD2MAP_TILES 1
+int gmm_set_planned_tod2map_kernel(int32_t which);
+int gmm_get_planned_tod2map_kernel(void);
 
 /* Replaces the PointingPrePlan constructor (PointingPrePlan.cu:129-251 / gpu_mm.hpp:74-77).
  * Counts mt words per planner block on the device, writes the inclusive cumsum (padded with the
@@ -137,6 +152,7 @@ int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum_gpu,
  *  - All calls share the one array.  Calls that overlap on the GPU (other streams, other host
  *    threads) race on it and must be serialised by the caller.  Nothing in the array needs to
  *    start at zero: every call overwrites what it reads.
+ *  - Like gmm_plan_build, each call synchronises with 'stream' once, to read the error flags.
  * Allocates nothing. */
 #define GMM_NOALLOC_SCRATCH_BYTES (32ll << 20)
 int gmm_plan_build_noalloc(const gmm_preplan_info *info, const uint32_t *nmt_cumsum_gpu, const float *xpointing_gpu,

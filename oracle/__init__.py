@@ -13,6 +13,11 @@ Two native libraries sit behind it:
   templates compiled from the reference source tree by ``oracle/Makefile``.  It pins the C
   restatement and serves as the "reference" CPU baseline.  It is built only where the reference
   tree exists; the committed golden vectors under ``tests/golden/`` carry its outputs elsewhere.
+* ``_ref/libgpu_mm_refgpu.so`` (optional) -- the reference's own plan builder and planned /
+  unplanned GPU operators (its ``src_lib`` sources, unchanged) compiled for sm_100a against a minimal
+  stand-in for the ksgpu containers (``oracle/ksgpu_shim``).  It pins this implementation's plans to
+  the reference's PointingPlan and PointingPlanTester and times the reference's kernels on the same
+  GPU (``RefGpuPlan``, ``refgpu_*``).
 """
 
 import ctypes
@@ -152,6 +157,129 @@ def ref():
     return _REF
 
 
+def refgpu_path():
+    return os.path.join(_HERE, "_ref", "libgpu_mm_refgpu.so")
+
+
+def refgpu_available():
+    return os.path.exists(refgpu_path())
+
+
+_REFGPU = None
+
+
+def refgpu():
+    """The reference's own plan builder and GPU operators (oracle/_ref/libgpu_mm_refgpu.so: its
+    src_lib sources compiled unchanged for sm_100a against oracle/ksgpu_shim).  Raises if it was not
+    built."""
+    global _REFGPU
+    if _REFGPU is None:
+        if not refgpu_available():
+            raise RuntimeError("oracle/_ref/libgpu_mm_refgpu.so was not built (it needs the reference source tree)")
+        R = ctypes.CDLL(refgpu_path())
+        vp, l, i = ctypes.c_void_p, ctypes.c_long, ctypes.c_int
+        R.refgpu_last_error.restype = ctypes.c_char_p
+        R.refgpu_plan_create.argtypes = [vp, l, l, l, i]
+        R.refgpu_plan_create.restype = vp
+        R.refgpu_plan_free.argtypes = [vp]
+        R.refgpu_plan_info.argtypes = [vp, vp, vp]
+        R.refgpu_plan_get.argtypes = [vp, vp, vp]
+        R.refgpu_plan_tester.argtypes = [vp, l, l, l, i, vp, l, vp, vp]
+        lp_args = [l, l, vp, vp, l, l, l, l, i]
+        R.refgpu_planned_map2tod.argtypes = [vp, vp, vp, l, vp, l] + lp_args + [i, i]
+        R.refgpu_planned_tod2map.argtypes = [vp, vp, l, vp, vp, l] + lp_args + [i]
+        R.refgpu_unplanned_map2tod.argtypes = [vp, vp, l, vp, l] + lp_args + [vp, l, i, i]
+        R.refgpu_unplanned_tod2map.argtypes = [vp, l, vp, vp, l] + lp_args + [vp, l, i]
+        R.refgpu_reference_map2tod.argtypes = [vp, vp, l, vp, l, l, l, vp, l, l, l, l, i, i, i]
+        R.refgpu_reference_tod2map.argtypes = [vp, l, vp, vp, l, l, l, vp, l, l, l, l, i, i]
+        for name in ("plan_info", "plan_get", "plan_tester", "planned_map2tod", "planned_tod2map",
+                     "unplanned_map2tod", "unplanned_tod2map", "reference_map2tod", "reference_tod2map"):
+            getattr(R, "refgpu_" + name).restype = i
+        _REFGPU = R
+    return _REFGPU
+
+
+def _refgpu_check(rc):
+    if rc != 0:
+        raise RuntimeError("reference: " + refgpu().refgpu_last_error().decode())
+
+
+class RefGpuPlan:
+    """PointingPrePlan + PointingPlan built by the reference's own code on the GPU.  'xp_gpu' is any
+    (3, nsamp) float32 CUDA array with a data pointer (a torch tensor); the plan keeps no reference to
+    it.  Device-array arguments of the methods are likewise raw CUDA tensors."""
+
+    def __init__(self, xp_gpu, nypix_global, nxpix_global, periodic_xcoord=True):
+        R = refgpu()
+        self.nsamp = xp_gpu.numel() // 3
+        self.ny, self.nx, self.periodic = int(nypix_global), int(nxpix_global), bool(periodic_xcoord)
+        self.h = R.refgpu_plan_create(xp_gpu.data_ptr(), self.nsamp, self.ny, self.nx, int(self.periodic))
+        if not self.h:
+            raise RuntimeError("reference: " + R.refgpu_last_error().decode())
+        info = np.zeros(8, np.int64)
+        ov = ctypes.c_double()
+        R.refgpu_plan_info(self.h, info.ctypes.data, ctypes.addressof(ov))
+        (self.plan_nmt, self.ncl_per_threadblock, self.planner_nblocks, self.nmt_per_threadblock,
+         self.pointing_nblocks, self.plan_nbytes, self.plan_constructor_tmp_nbytes, self.cub_nbytes) = \
+            (int(v) for v in info)
+        self.overhead = ov.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            refgpu().refgpu_plan_free(self.h)
+            self.h = None
+
+    def get(self):
+        """(plan_mt uint64[plan_nmt] in the reference's own order, nmt_cumsum uint32[planner_nblocks])."""
+        mt = np.zeros(self.plan_nmt, np.uint64)
+        cs = np.zeros(1024, np.uint32)
+        _refgpu_check(refgpu().refgpu_plan_get(self.h, mt.ctypes.data, cs.ctypes.data))
+        return mt, cs[:self.planner_nblocks]
+
+    @staticmethod
+    def _lp(lp, offs_gpu):
+        offs = np.ascontiguousarray(lp.cell_offsets, dtype=np.int64)
+        return offs, [lp.nypix_global, lp.nxpix_global, offs.ctypes.data, offs_gpu.data_ptr(), lp.nycells,
+                      lp.nxcells, lp.ystride, lp.polstride, int(lp.periodic_xcoord)]
+
+    def map2tod(self, tod, lmap, xp, lp, offs_gpu, partial=False, accum=False):
+        offs, a = self._lp(lp, offs_gpu)
+        _refgpu_check(refgpu().refgpu_planned_map2tod(self.h, tod.data_ptr(), lmap.data_ptr(), lmap.numel(),
+                                                      xp.data_ptr(), self.nsamp, *a, int(partial), int(accum)))
+
+    def tod2map(self, lmap, tod, xp, lp, offs_gpu, partial=False):
+        offs, a = self._lp(lp, offs_gpu)
+        _refgpu_check(refgpu().refgpu_planned_tod2map(self.h, lmap.data_ptr(), lmap.numel(), tod.data_ptr(),
+                                                      xp.data_ptr(), self.nsamp, *a, int(partial)))
+
+
+def refgpu_unplanned_map2tod(tod, lmap, xp, lp, offs_gpu, errflags, partial=False, accum=False):
+    offs, a = RefGpuPlan._lp(lp, offs_gpu)
+    _refgpu_check(refgpu().refgpu_unplanned_map2tod(tod.data_ptr(), lmap.data_ptr(), lmap.numel(), xp.data_ptr(),
+                                                    xp.numel() // 3, *a, errflags.data_ptr(), errflags.numel(),
+                                                    int(partial), int(accum)))
+
+
+def refgpu_unplanned_tod2map(lmap, tod, xp, lp, offs_gpu, errflags, partial=False):
+    offs, a = RefGpuPlan._lp(lp, offs_gpu)
+    _refgpu_check(refgpu().refgpu_unplanned_tod2map(lmap.data_ptr(), lmap.numel(), tod.data_ptr(), xp.data_ptr(),
+                                                    xp.numel() // 3, *a, errflags.data_ptr(), errflags.numel(),
+                                                    int(partial)))
+
+
+def refgpu_plan_tester(xp_gpu, nypix_global, nxpix_global, periodic_xcoord=True, capacity=None):
+    """The reference's PointingPlanTester (PointingPlanTester.cu:69-161): (sorted_mt, nmt_cumsum)."""
+    nsamp = xp_gpu.numel() // 3
+    cap = int(capacity) if capacity else 8 * (nsamp // 32) + 64
+    mt = np.zeros(cap, np.uint64)
+    cs = np.zeros(1024, np.uint32)
+    n = ctypes.c_long()
+    _refgpu_check(refgpu().refgpu_plan_tester(xp_gpu.data_ptr(), nsamp, int(nypix_global), int(nxpix_global),
+                                              int(periodic_xcoord), mt.ctypes.data, cap, cs.ctypes.data,
+                                              ctypes.addressof(n)))
+    return mt[:n.value], cs
+
+
 # ------------------------------------------------------------------------------------------------
 
 
@@ -262,6 +390,31 @@ def plan(xpointing, nypix_global, nxpix_global, periodic_xcoord=True, nmt=None):
     err = lib().oracle_plan(_ptr(xp, ctypes.c_float), _nsamp(xp), int(nypix_global), int(nxpix_global),
                             int(periodic_xcoord), int(nmt), _ptr(mt, ctypes.c_uint64), _ptr(owner, ctypes.c_uint32))
     return mt[:nmt], owner[:(nmt + 31) // 32], int(err)
+
+
+def owner_words(xpointing, nypix_global, mt, owner_bits):
+    """Owner list of a single-TOD plan as the plan builder must produce it (the owner list is this
+    implementation's own addition to the reference's plan; there is no reference counterpart).
+
+    One word per cache line: the line's lowest cell | line << 20 | mflag << 46 | band << 48, sorted
+    stably by (cell, band), i.e. in (cell, band, line) order.  'mt' and 'owner_bits' are plan()'s
+    outputs (the owner bit marks the first mt word of each line in (cell, line) order, which is the
+    line's lowest cell).  The band is the upper bilinear row of the line's first sample (locate's
+    clamp of trunc(y) to [0, ny-2]) minus 64 * iycell of the owner, clamped to [0, 63]."""
+    xp = np.ascontiguousarray(xpointing, dtype=np.float32)
+    n = _nsamp(xp)
+    mt = np.asarray(mt, dtype=np.uint64)
+    bits = np.unpackbits(np.asarray(owner_bits).view(np.uint8), bitorder="little")[:len(mt)].astype(bool)
+    words = mt[bits] & np.uint64((1 << 47) - 1)          # cell, line, mflag (no zflag)
+    lines = ((words >> np.uint64(20)) & np.uint64((1 << 26) - 1)).astype(np.int64)
+    y = xp.reshape(3, n)[0][32 * lines].astype(np.float64)
+    y = np.nan_to_num(y, nan=0.0, posinf=float(nypix_global), neginf=-1.0)
+    iy0 = np.clip(np.trunc(np.clip(y, -1.0, float(nypix_global))), 0, nypix_global - 2).astype(np.int64)
+    iyc = ((words >> np.uint64(10)) & np.uint64(1023)).astype(np.int64)
+    band = np.clip(iy0 - 64 * iyc, 0, 63).astype(np.uint64)
+    words = words | (band << np.uint64(48))
+    order = np.lexsort((lines, band, (words & np.uint64(0xFFFFF)).astype(np.int64)))
+    return words[order]
 
 
 def sample_slots(xpointing, nypix_global, nxpix_global, periodic_xcoord=True):

@@ -51,9 +51,7 @@ def check_plan(g, xp, ny, nx, periodic, pp, plan):
     assert err == 0
     mt = plan.get_plan_mt()
     np.testing.assert_array_equal(mt, mt_ref)   # all 64 bits, canonical order
-    bits = np.unpackbits(owner_ref.view(np.uint8), bitorder="little")[:len(mt_ref)].astype(bool)
-    owner = plan._get_owner_mt()
-    np.testing.assert_array_equal(owner & np.uint64((1 << 46) - 1), mt_ref[bits] & np.uint64((1 << 46) - 1))
+    np.testing.assert_array_equal(plan._get_owner_mt(), oracle.owner_words(xp, ny, mt_ref, owner_ref))
 
 
 def lpix_from(g, ny, nx, offs, ys, ps, periodic):
