@@ -155,12 +155,23 @@ def cpu_reference_run(xp, tod, m, lp, nthreads, use_ref):
     return dt
 
 
+def _synthetic():
+    """gpu_mm_b200/synthetic.py (the seeded raster generator; it imports only numpy and torch), loaded
+    from its file so that the CPU legs never run the package's __init__ and never map its native
+    library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_bench_synthetic", os.path.join(ROOT, "gpu_mm_b200", "synthetic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def cpu_sample(ndet, ndet_rows_cfg):
     """The first 'ndet' detectors of the workload, on the host: xpointing, tod, map, oracle Lpix."""
     import numpy as np
     import torch
     import oracle
-    from gpu_mm_b200 import synthetic
+    synthetic = _synthetic()
     rows = max(1, ndet // 32)
     xp = synthetic.raster_xpointing(rows, 32, 2 ** 18, 2.0, 0.7, 32768, 100.0, 2.0e-4, device="cpu").numpy()
     xp = np.ascontiguousarray(xp[:, :ndet])
@@ -213,8 +224,7 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Gsamples/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(args.ndet_rows, 2 ** 18 * 32 * args.ndet_rows, len(lp.cell_offsets[lp.cell_offsets >= 0]), lp.npix)
-        | {"reference_sample": f"{ndet} detectors ({nsamp} samples) per step"},
+        "config": workload_config(args.ndet_rows, 2 ** 18 * 32 * args.ndet_rows, len(lp.cell_offsets[lp.cell_offsets >= 0]), lp.npix),
         "cpu_baseline": {"value": round(value, 4), "unit": "Gsamples/s", "cores": nthreads, "kind": kind,
                          "sample": f"{ndet} detectors ({nsamp} samples) per step, map2tod + tod2map, "
                                    f"{nthreads} threads"},

@@ -23,6 +23,19 @@ A worker thread runs the loop.  Every iteration it
 A completion thread waits on each launch's CUDA event in launch order, completes its requests and
 returns their memory to the budget, waking the worker for requests that wait for memory.
 
+Streams: submit() records an event on the caller's current CUDA stream, and the launch that serves
+the request waits for it before reading the request's TOD, the pointing or the resident maps, so
+inputs written asynchronously by the caller are safe to submit.  A map2tod result is recorded on the
+submitting stream (Tensor.record_stream), so the caching allocator does not hand its memory to a
+later launch while work the caller queues on that stream may still read it; use it on other streams
+only after ordering them after the submitting stream.
+
+Errors: a request with bad arguments raises in submit().  Device error bits (the reference's
+xpointing-range and pixelization errors) are read back per launch, and every request of a launch
+that reported bits fails with a RuntimeError naming them (a launch batches several requests; the
+bits are not attributed to one of them); check() raises if any launch reported bits since the last
+check().
+
 Results do not depend on the mix: map2tod evaluates every sample with the same rounded operations as
 the single-TOD operator (bit-identical), and tod2map adds the same per-sample contributions into the
 output map (float atomics: the order, and so the last bits, differ).
@@ -97,7 +110,7 @@ class PointingServer:
         self._wake = threading.Condition(self._lock)   # signalled by submit() and close()
         self._submitted = collections.deque()
         self._waiting = collections.deque()
-        self._inflight = collections.deque()               # (event, requests, bytes, keepalive), launch order
+        self._inflight = collections.deque()               # (event, requests, bytes, keepalive, error words, n), launch order
         self._done = threading.Condition(self._lock)       # signalled when a launch is queued, and at exit
         self._freed = 0                                    # bytes released by completions, not yet in _used
         self._worker_done = False
@@ -111,7 +124,8 @@ class PointingServer:
         self.evictions = 0
         self.iterations = []                               # (requests launched, host seconds)
         self.errors = []
-        self._errwords = []
+        self._err_bits = 0                                 # device error bits seen since the last check()
+        self._pinned_free = []                             # pinned host words for per-launch error readback
         self._thread = threading.Thread(target=self._run, daemon=True)
         self._completer = threading.Thread(target=self._complete_loop, daemon=True)
         self._thread.start()
@@ -120,15 +134,29 @@ class PointingServer:
     # ---- client side ----
 
     def submit(self, kind, tod_id, tod=None):
+        """Queues a request and returns a concurrent.futures.Future: None for 'plan' and 'tod2map', the
+        TOD (a CUDA tensor shaped like the pointing's sample axes) for 'map2tod'.  The request is served
+        after the work queued so far on the caller's current CUDA stream."""
         if kind not in ("plan", "map2tod", "tod2map"):
             raise ValueError(f"unknown request kind {kind}")
         if tod_id not in self.xpointings:
             raise KeyError(f"unknown tod_id {tod_id}")
-        if kind == "tod2map" and tod is None:
-            raise ValueError("tod2map needs a TOD array")
+        if kind == "tod2map":
+            if tod is None:
+                raise ValueError("tod2map needs a TOD array")
+            want = tuple(self.xpointings[tod_id].shape[1:])
+            if not isinstance(tod, torch.Tensor) or tuple(tod.shape) != want:
+                raise ValueError(f"tod2map: TOD shape {tuple(getattr(tod, 'shape', ()))} does not match the "
+                                 f"pointing's sample shape {want}")
+            if tod.dtype != torch.float32 or not tod.is_cuda or not tod.is_contiguous() or tod.data_ptr() % 16:
+                raise ValueError("tod2map: the TOD must be a contiguous, 16-byte aligned float32 CUDA tensor")
+        stream = torch.cuda.current_stream()
+        ready = torch.cuda.Event()
+        ready.record(stream)
         fut = concurrent.futures.Future()
         with self._lock:
-            self._submitted.append({"kind": kind, "id": tod_id, "tod": tod, "t0": time.perf_counter(), "fut": fut})
+            self._submitted.append({"kind": kind, "id": tod_id, "tod": tod, "t0": time.perf_counter(), "fut": fut,
+                                    "ready": ready, "stream": stream})
             self._wake.notify()
         return fut
 
@@ -219,13 +247,9 @@ class PointingServer:
                     self._launching = bool(self._waiting)
                 try:
                     launched = self._launch()
-                except Exception as e:   # surfaced to the waiting requests
+                except Exception as e:   # _launch has failed the requests of that launch only
                     launched = False
                     self.errors.append(repr(e))
-                    with self._lock:
-                        for r in list(self._waiting):
-                            r["fut"].set_exception(e)
-                        self._waiting.clear()
                 finally:
                     self._launching = False
                 if not launched:
@@ -249,17 +273,27 @@ class PointingServer:
                     self._done.wait(timeout=0.05)
                 if not self._inflight:
                     return
-                ev, reqs, nb, keepalive = self._inflight[0]
+                ev, reqs, nb, keepalive, errs, nerr = self._inflight[0]
             err = None
             try:
                 ev.synchronize()
+                bits = 0
+                for w in errs[:nerr].tolist():      # copied on the launch's stream before 'ev'
+                    bits |= w
+                if bits:
+                    err = RuntimeError(f"PointingServer: device error bits {bits:#x} in a launch of "
+                                       f"{len(reqs)} request(s) (1/2: xpointing y/x out of range, "
+                                       f"8: not in LocalPixelization)")
             except Exception as e:
+                bits = 0
                 err = e
                 self.errors.append(repr(e))
             t1 = time.perf_counter()
             with self._lock:
                 self._inflight.popleft()
                 self._freed += nb
+                self._err_bits |= bits
+                self._pinned_free.append(errs)
                 for r in reqs:
                     self.latencies[r["kind"]].append(t1 - r["t0"])
                 self._wake.notify()
@@ -306,11 +340,22 @@ class PointingServer:
                     self._used -= nb
             raise
 
+    def _pinned_words(self, n):
+        with self._lock:
+            for i, b in enumerate(self._pinned_free):
+                if b.numel() >= n:
+                    return self._pinned_free.pop(i)
+        return torch.empty(max(n, 16), dtype=torch.int32, pin_memory=True)
+
     def _launch_admitted(self, admitted, reserved):
         stream = self._stream()
         keep = []
+        errwords = []
         # Everything below is allocated and launched on 'stream', so allocations, copies and kernels
-        # of one iteration are ordered, and iterations on different streams overlap.
+        # of one iteration are ordered, and iterations on different streams overlap.  It starts after
+        # the work each request's caller had queued when submitting.
+        for r in admitted:
+            stream.wait_event(r["ready"])
         with torch.cuda.stream(stream):
             # Plans to (re)build: plan requests, and operator requests whose plan is not cached --
             # all built together (one owner pass, one sort, one scatter).
@@ -334,7 +379,7 @@ class PointingServer:
                     nb = max(self._plan_nbytes(i), sp.plan.numel())
                     self._plans[i] = (sp, ev, nb)
                     self._used += nb - reserved.get(i, 0)
-                self._errwords.append(builder.err)
+                errwords.append(builder.err)
                 keep.append(builder)
             for r in admitted:
                 self._plans.move_to_end(r["id"])
@@ -353,6 +398,7 @@ class PointingServer:
                     flat = torch.empty(sum(sizes), device="cuda")
                     tods = [v.view(x.shape[1:]) for v, x in zip(flat.split(sizes), xps)]
                     for r, t in zip(reqs, tods):
+                        t.record_stream(r["stream"])
                         r["result"] = t
                 else:
                     tods = [r["tod"] for r in reqs]
@@ -374,18 +420,25 @@ class PointingServer:
                 self.samples_done += b.total_samples
                 self.launches += 1
                 keep.append(b)
-                self._errwords.append(b.err)
+                errwords.append(b.err)
+            # The launch's error words go to pinned host memory on the same stream, ahead of its event.
+            dev = torch.cat(errwords) if len(errwords) > 1 else errwords[0]
+            errs = self._pinned_words(dev.numel())
+            errs[:dev.numel()].copy_(dev, non_blocking=True)
+            keep.append(dev)
             ev = torch.cuda.Event()
             ev.record(stream)
         nb = sum(self._request_nbytes(r) for r in admitted)
         with self._lock:
-            self._inflight.append((ev, admitted, nb, keep))
+            self._inflight.append((ev, admitted, nb, keep, errs, dev.numel()))
             self._done.notify()
         return True
 
     def check(self):
-        """Raises if any plan build or launch reported device error bits (waits for the GPU)."""
-        torch.cuda.synchronize()
-        words = [int(w) for e in self._errwords for w in e.cpu().tolist()]
-        if any(words):
-            raise RuntimeError(f"PointingServer: device error bits {sorted(set(w for w in words if w))}")
+        """Waits for the submitted requests, then raises if any launch since the last check() reported
+        device error bits (and clears them)."""
+        self.drain()
+        with self._lock:
+            bits, self._err_bits = self._err_bits, 0
+        if bits:
+            raise RuntimeError(f"PointingServer: device error bits {bits:#x} since the last check()")

@@ -147,3 +147,43 @@ def test_pybind_surface_has_reference_names():
                  "plan_constructor_tmp_nbytes", "overhead", "ncl_per_threadblock", "planner_nblocks",
                  "nmt_per_threadblock", "pointing_nblocks", "plan_nmt", "cub_nbytes", "get_nmt_cumsum"):
         assert hasattr(m.PointingPrePlan, attr), attr
+
+
+def test_drop_in_import_names():
+    """The reference's import names resolve to this build (SURVEY boundary: the module must import as
+    gpu_mm.gpu_mm_pybind11)."""
+    import importlib
+    import gpu_mm_b200
+    gm = importlib.import_module("gpu_mm")
+    m = importlib.import_module("gpu_mm.gpu_mm_pybind11")
+    assert m is gpu_mm_b200.gpu_mm_pybind11 and gm.gpu_mm_pybind11 is m
+    from gpu_mm import gpu_mm_pybind11 as m2, map2tod, tod2map, PointingPlan
+    assert m2 is m and map2tod is gpu_mm_b200.map2tod and tod2map is gpu_mm_b200.tod2map
+    assert PointingPlan is gpu_mm_b200.PointingPlan
+    from gpu_mm.gpu_mm import LocalPixelization
+    assert LocalPixelization is gpu_mm_b200.LocalPixelization
+
+
+@pytest.mark.parametrize("ntu", [64, 100, 31, 1])
+def test_read_xpointing_npzfile_round_trip(tmp_path, ntu):
+    """The reference's .npz pointing format (gpu_mm.py:1305-1329): rows stored as (x, y, alpha) over
+    (ndet, nt); read back as (y, x, alpha) with nt padded to a multiple of 32 by repeating each
+    detector's last sample."""
+    import gpu_mm_b200 as g
+    rng = np.random.default_rng(ntu)
+    ndet = 3
+    stored = rng.standard_normal((3, ndet, ntu)).astype(np.float32)
+    path = tmp_path / "xp.npz"
+    np.savez(path, xpointing=stored)
+    xp = g.read_xpointing_npzfile(str(path))
+    ntp = 32 * ((ntu + 31) // 32)
+    assert xp.shape == (3, ndet, ntp) and xp.dtype == np.float32
+    np.testing.assert_array_equal(xp[0, :, :ntu], stored[1])
+    np.testing.assert_array_equal(xp[1, :, :ntu], stored[0])
+    np.testing.assert_array_equal(xp[2, :, :ntu], stored[2])
+    for r, src in ((0, 1), (1, 0), (2, 2)):
+        np.testing.assert_array_equal(xp[r, :, ntu:], np.repeat(stored[src, :, -1:], ntp - ntu, axis=1))
+    bad = tmp_path / "bad.npz"
+    np.savez(bad, xpointing=stored[:2])
+    with pytest.raises(AssertionError):
+        g.read_xpointing_npzfile(str(bad))

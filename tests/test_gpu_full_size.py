@@ -1,26 +1,31 @@
 """GPU tests at the full size of the large raster workload: 1024 detectors (32x32, 2 px spacing) x
 2^18 samples (nsamp = 2^28), x sweep 0.7 px/sample over a periodic 3x8192x32768 map, LocalPixelization
-holding the hit cells.  The oracle would take minutes over the whole TOD, so the checks here are the
-size-independent properties of the operators:
+holding the hit cells.
 
-  * the plan is deterministic: a second build gives the same plan words, bit for bit;
-  * planned map2tod is the same on every call of a plan-reuse loop (ten calls);
-  * planned and unplanned map2tod agree within the float32 tolerance, and map2tod is per sample, so
-    a handful of detectors checks against the oracle exactly like a small case;
-  * planned and unplanned tod2map agree within the float32 tolerance (different atomic orders);
-  * the operators are adjoint: <t, A m> = <A^T t, m> (A = map2tod), summed in float64;
-  * at nsamp = 2^31, the largest the API accepts, planned and unplanned operators agree and the last
+  * The plan equals the oracle's in every 64-bit word (plan_mt and the owner list), together with
+    nmt_cumsum and the preplan geometry; and it equals the reference's own PointingPlan, built by the
+    reference's code on the same GPU, put in canonical order (where that comparator was built).
+  * Planned and unplanned map2tod and tod2map (both tod2map kernels) over the whole TOD agree with
+    the multithreaded oracle (the reference's CPU operator arithmetic), and with the reference's own
+    GPU operators where built.
+  * The plan is deterministic (a second build gives the same words), planned map2tod is the same on
+    every call of a plan-reuse loop (ten calls), and the operators are adjoint:
+    <t, A m> = <A^T t, m> (A = map2tod), summed in float64.
+  * At nsamp = 2^31, the largest the API accepts, planned and unplanned operators agree and the last
     detectors match the oracle.
 
 Tolerances as in the parity tests: rel-L1 < 1e-6 and max|a-b| / max|b| < 1e-5; the adjoint identity
 to 1e-6 of sum |t_i (A m)_i|.
 """
 
+import ctypes
+import os
+
 import numpy as np
 import pytest
 
 import oracle
-from tests._common import rel_stats
+from tests._common import canonical, rel_stats
 
 pytestmark = pytest.mark.gpu
 
@@ -60,6 +65,78 @@ def gpu_rel_stats(a, b, chunk=1 << 26):
         dmax = max(dmax, float(d.max()))
         bmax = max(bmax, float(bc.abs().max()))
     return dsum / asum, dmax / bmax
+
+
+@pytest.fixture(scope="module")
+def host_inputs(workload):
+    """Host copies of the workload (3 GiB of xpointing) and the oracle's view of the pixelization."""
+    g, xp, pp, plan, lp, m, t = workload
+    xs = xp.cpu().numpy()
+    lp_o = oracle.Lpix(NY, NX, lp.cell_offsets_cpu, lp.ystride, lp.polstride, True)
+    return xs, lp_o, m.cpu().numpy(), t.cpu().numpy()
+
+
+def test_plan_equals_oracle_and_reference(workload, host_inputs):
+    g, xp, pp, plan, lp, m, t = workload
+    xs, lp_o, _, _ = host_inputs
+    ref = oracle.preplan(xs, NY, NX, True)
+    assert pp.plan_nmt == ref["nmt"]
+    for k in ("ncl_per_threadblock", "planner_nblocks", "nmt_per_threadblock", "pointing_nblocks"):
+        assert getattr(pp, k) == ref[k], k
+    np.testing.assert_array_equal(pp.get_nmt_cumsum(), ref["nmt_cumsum"][:pp.planner_nblocks])
+    mt_ref, owner_bits, err = oracle.plan(xs, NY, NX, True, nmt=ref["nmt"])
+    assert err == 0
+    mt = plan.get_plan_mt()
+    np.testing.assert_array_equal(mt, mt_ref)
+    np.testing.assert_array_equal(plan._get_owner_mt(), oracle.owner_words(xs, NY, mt_ref, owner_bits))
+    if oracle.refgpu_available():
+        rp = oracle.RefGpuPlan(xp, NY, NX, True)
+        assert rp.plan_nmt == pp.plan_nmt
+        rmt, rcs = rp.get()
+        del rp
+        np.testing.assert_array_equal(rcs, pp.get_nmt_cumsum())
+        np.testing.assert_array_equal(canonical(rmt), mt)
+
+
+def test_operators_equal_oracle(workload, host_inputs):
+    """The whole TOD and map, planned and unplanned, both tod2map kernels, against the multithreaded
+    oracle; and against the reference's own GPU operators where that comparator was built."""
+    import torch
+    g, xp, pp, plan, lp, m, t = workload
+    xs, lp_o, m_h, t_h = host_inputs
+    nthreads = os.cpu_count() or 1
+    want = np.zeros(t_h.shape, np.float32)
+    assert oracle.map2tod_mt(want, m_h, xs, lp_o, nthreads) == 0
+    lmap = g.LocalMap(lp, m)
+    tod = torch.empty(xp.shape[1:], device="cuda")
+    for pl in (plan, None):
+        g.map2tod(tod, lmap, xp, pl)
+        rl1, mx = rel_stats(tod.cpu().numpy(), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, ("map2tod", pl is None, rl1, mx)
+    want_m = np.zeros(3 * lp.npix, np.float32)
+    assert oracle.tod2map_mt(want_m, t_h, xs, lp_o, nthreads) == 0
+    lib = ctypes.CDLL(g.library_path())
+    old = lib.gmm_get_planned_tod2map_kernel()
+    try:
+        for pl, which in ((plan, 0), (plan, 1), (None, 0)):
+            lib.gmm_set_planned_tod2map_kernel(which)
+            out = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+            g.tod2map(out, t, xp, pl)
+            rl1, mx = rel_stats(out.arr.cpu().numpy(), want_m)
+            assert rl1 < RL1_TOL and mx < MAX_TOL, ("tod2map", pl is None, which, rl1, mx)
+    finally:
+        lib.gmm_set_planned_tod2map_kernel(old)
+    if oracle.refgpu_available():
+        rp = oracle.RefGpuPlan(xp, NY, NX, True)
+        offs_gpu = torch.from_numpy(np.ascontiguousarray(lp_o.cell_offsets)).cuda()
+        rt = torch.empty(xp[0].numel(), device="cuda")
+        rp.map2tod(rt, m, xp, lp_o, offs_gpu)
+        rl1, mx = rel_stats(rt.cpu().numpy(), want.reshape(-1))
+        assert rl1 < RL1_TOL and mx < MAX_TOL, ("reference GPU map2tod", rl1, mx)
+        rm = torch.zeros(3 * lp.npix, device="cuda")
+        rp.tod2map(rm, t.reshape(-1), xp, lp_o, offs_gpu)
+        rl1, mx = rel_stats(rm.cpu().numpy(), want_m)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, ("reference GPU tod2map", rl1, mx)
 
 
 def test_plan_deterministic(workload):

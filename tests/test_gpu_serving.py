@@ -132,8 +132,8 @@ def test_serving_rejects_bad_requests(g):
 
 
 def test_serving_reports_errors_and_keeps_serving(g):
-    """Device error bits from a plan build reach check(); a request whose launch fails on the host
-    fails alone (its future raises) and the server goes on serving later requests."""
+    """Device error bits of a launch fail that launch's requests and reach check(), which clears them;
+    a request with bad arguments raises in submit(); the server goes on serving later requests."""
     import torch
     ny, nx = 256, 512
     rng, xps, tods = pool(13, n=3)
@@ -144,16 +144,21 @@ def test_serving_reports_errors_and_keeps_serving(g):
     m = torch.from_numpy(rng.standard_normal(3 * lp.npix).astype(np.float32)).cuda()
     srv = g.PointingServer(xg, m, torch.zeros(3 * lp.npix, device="cuda"), lp, hbm_budget_bytes=1 << 30)
     try:
-        srv.submit("plan", 0).result(timeout=30)
-        srv.drain()
+        with pytest.raises(RuntimeError, match="device error bits 0x1"):
+            srv.submit("plan", 0).result(timeout=30)
         with pytest.raises(RuntimeError, match="device error bits"):
             srv.check()
-        bad = srv.submit("tod2map", 1, tod=torch.zeros(7, device="cuda"))    # wrong shape
-        with pytest.raises(RuntimeError, match="shape"):
-            bad.result(timeout=30)
-        assert srv.errors
-        r = srv.submit("map2tod", 1).result(timeout=30)
-        srv.drain()
+        srv.check()                                       # cleared by the previous check()
+        with pytest.raises(ValueError, match="shape"):
+            srv.submit("tod2map", 1, tod=torch.zeros(7, device="cuda"))
+        with pytest.raises(ValueError, match="float32"):
+            srv.submit("tod2map", 1, tod=torch.zeros(xps[1].shape[1:], dtype=torch.float64, device="cuda"))
+        futs = [srv.submit("map2tod", 1)] + [srv.submit("tod2map", 2, tod=torch.from_numpy(tods[2]).cuda())
+                                             for _ in range(3)]
+        r = futs[0].result(timeout=30)
+        for f in futs[1:]:
+            assert f.result(timeout=30) is None
+        srv.check()
     finally:
         srv.close()
     alone = torch.zeros(xps[1].shape[1:], device="cuda")
@@ -161,3 +166,45 @@ def test_serving_reports_errors_and_keeps_serving(g):
     assert torch.equal(r, alone)
     g.serving.release_scratch()          # no server running: the shared scratch can go
     assert not g.serving._SCRATCH
+
+
+def test_serving_waits_for_the_callers_stream(g):
+    """Inputs written asynchronously on the caller's stream just before submit(): a TOD and the
+    resident input map are filled by copies queued behind a long-running kernel on a side stream, and
+    the requests are submitted from that stream without synchronising.  The server orders its launches
+    after the caller's work, so tod2map and map2tod see the final inputs."""
+    import torch
+    ny, nx = 256, 512
+    rng, xps, tods = pool(21, n=4)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, True)
+    lp_o = oracle.Lpix.rectangle(ny, nx, True)
+    xg = {i: torch.from_numpy(x).cuda() for i, x in xps.items()}
+    m = rng.standard_normal(3 * lp.npix).astype(np.float32)
+    m_src = torch.from_numpy(m).cuda()
+    t_src = torch.from_numpy(tods[1]).cuda()
+    in_map = torch.zeros(3 * lp.npix, device="cuda")
+    out_map = torch.zeros(3 * lp.npix, device="cuda")
+    tod = torch.zeros(xps[1].shape[1:], device="cuda")
+    torch.cuda.synchronize()
+    srv = g.PointingServer(xg, in_map, out_map, lp, hbm_budget_bytes=1 << 30)
+    side = torch.cuda.Stream()
+    try:
+        with torch.cuda.stream(side):
+            torch.cuda._sleep(50_000_000)                 # about 25 ms of GPU time on this stream
+            tod.copy_(t_src)
+            in_map.copy_(m_src)
+            f_t2m = srv.submit("tod2map", 1, tod=tod)
+            f_m2t = srv.submit("map2tod", 2)
+        f_t2m.result(timeout=30)
+        r = f_m2t.result(timeout=30)
+        srv.check()
+    finally:
+        srv.close()
+    want = np.zeros(3 * lp.npix, np.float32)
+    oracle.tod2map(want, tods[1], xps[1], lp_o)
+    rl1, mx = rel_stats(out_map.cpu().numpy(), want)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+    want_t = np.zeros(xps[2].shape[1:], np.float32)
+    oracle.map2tod(want_t, m, xps[2], lp_o)
+    rl1, mx = rel_stats(r.cpu().numpy(), want_t)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
