@@ -233,7 +233,7 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def precision_study(max_run_lines=1024):
+def precision_study(max_run_lines=32):
     """tod2map precision variants on the high-hit workload: 64 detectors x 2^22 samples (2^28)
     confined to the 512x512 box [256, 768)^2 of a 3x1024x1024 map (~1000 hits/pixel), tod = 1e3 +
     N(0,1).  Each mode is timed with CUDA events (3 calls after 1 warm-up) and compared with the FP64

@@ -101,17 +101,18 @@ __device__ __forceinline__ void cell_slots(const Located &L, int slots[6])
 }
 
 // Per-slot warp analysis of one 32-sample cache line (the role of cell_analysis,
-// PointingPlan.cu:19-37): amask[k] has one bit per distinct valid cell of slot k, at the lowest
-// lane holding it.
+// PointingPlan.cu:19-37): amask[k] has one bit per distinct valid cell of slot k, at the highest lane
+// holding it -- the reference marks the lane where (match_any mask >> lane) == 1 -- so that a slot's
+// cells come in the reference's ring-buffer order (marked lanes in lane order), which decides which
+// of them carries zflag.
 __device__ __forceinline__ void line_slot_masks(const int slots[6], unsigned amask[6])
 {
     const unsigned lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
     for (int k = 0; k < 6; k++) {
         unsigned peers = __match_any_sync(kFullMask, (unsigned) slots[k]);
-        bool lowest = (peers & lt) == 0;
-        amask[k] = __ballot_sync(kFullMask, lowest && (slots[k] >= 0));
+        bool highest = (peers >> lane) == 1u;
+        amask[k] = __ballot_sync(kFullMask, highest && (slots[k] >= 0));
     }
 }
 

@@ -762,14 +762,20 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
 // move by at most one column per sample in one direction (a raster scan slower than 1 px/sample,
 // except at its turnarounds) is added with shuffles instead of atomics: each sample's contribution
 // is split between its two columns, the samples of one column are summed at the last lane of their
-// run, and every lane pulls the totals of the column it holds.  When the (cell, band) changes, the
-// accumulator goes into the map with one L2 reduction per pixel and plane (zeros skipped).  Other
-// lines go sample by sample straight into the map (twelve reductions each), and so do precision
-// modes and batches, which use planned_kernel.
+// run, and every lane pulls the totals of the column it holds.  When the (cell, band) changes, or
+// after max_run_lines lines (precision modes), the accumulator goes into the map with one L2
+// reduction per pixel and plane (zeros skipped), in flush mode FLUSH.  Other lines go sample by
+// sample straight into the map (twelve reductions each).  Batches use planned_kernel.
+//
+// Each warp streams its lines through a ring of BP line slots in shared memory (y, x, alpha and TOD
+// rows, 512 bytes per line): every lane copies 16 bytes of a line with cp.async, BP - 1 lines ahead
+// of the one being processed, so a warp keeps BP - 1 lines of memory traffic in flight while it
+// works without holding registers for them.
 
 constexpr int BW = 16;                 // warps per CTA
 constexpr int BNT = BW * 32;
-constexpr int BUNR = 2;                // cache lines loaded together per warp
+constexpr int BP = 8;                  // line slots per warp (a power of two)
+constexpr size_t kBandSmem = (size_t) BW * BP * 128 * sizeof(float);
 constexpr uint32_t kNoKey = 0xffffffffu;
 
 struct BandState {
@@ -784,10 +790,11 @@ __device__ __forceinline__ bool bit_at(unsigned m, int n)
     return (n >= 0) && (n < 32) && ((m >> n) & 1u);
 }
 
-// Adds the accumulator into the map (one reduction per non-zero pixel and plane) and clears it.
+// Adds the accumulator into the map (one addition per non-zero pixel and plane, in flush mode FLUSH)
+// and clears it.
 // Rows and columns outside the map, and absent cells, only ever hold zeros: every line the band path
 // takes has its footprint inside the map (absent cells are reported through the plan's cell bitmap).
-template<bool PERIODIC>
+template<bool PERIODIC, int FLUSH>
 __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
 {
     const int lane = threadIdx.x & 31;
@@ -806,9 +813,9 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
             if (__any_sync(kFullMask, nz) && nz && xin) {
                 const int64_t off = global_pixel_offset(B.R0 + r, gx, a);
                 if (off >= 0) {
-                    if (t != 0.0f) atomicAdd(a.out + off, t);
-                    if (q != 0.0f) atomicAdd(a.out + off + a.polstride, q);
-                    if (u != 0.0f) atomicAdd(a.out + off + 2 * a.polstride, u);
+                    if (t != 0.0f) global_add<FLUSH>(a, off, t);
+                    if (q != 0.0f) global_add<FLUSH>(a, off + a.polstride, q);
+                    if (u != 0.0f) global_add<FLUSH>(a, off + 2 * a.polstride, u);
                 }
             }
             B.acc[sl][3 * r] = 0.0f;
@@ -967,7 +974,7 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint16_
 
 // One sample of a line that the band path does not take: exact locate with error bits, then the
 // four neighbours straight into the map.
-template<bool RESP, bool PERIODIC>
+template<bool RESP, bool PERIODIC, int FLUSH>
 __device__ __forceinline__ void band_general_sample(const OpArgs &a, float y, float x, float al, float tv, uint32_t s,
                                                     uint32_t &err)
 {
@@ -989,30 +996,43 @@ __device__ __forceinline__ void band_general_sample(const OpArgs &a, float y, fl
     }
     const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
     uint32_t unused = 0;
-    global_accum(a, a.out, L.iy0, L.ix0, t, q, u, wy0 * wx0, unused);
-    global_accum(a, a.out, L.iy0, L.ix1, t, q, u, wy0 * L.dx, unused);
-    global_accum(a, a.out, L.iy1, L.ix0, t, q, u, L.dy * wx0, unused);
-    global_accum(a, a.out, L.iy1, L.ix1, t, q, u, L.dy * L.dx, unused);
+    global_accum<FLUSH>(a, a.out, L.iy0, L.ix0, t, q, u, wy0 * wx0, unused);
+    global_accum<FLUSH>(a, a.out, L.iy0, L.ix1, t, q, u, wy0 * L.dx, unused);
+    global_accum<FLUSH>(a, a.out, L.iy1, L.ix0, t, q, u, L.dy * wx0, unused);
+    global_accum<FLUSH>(a, a.out, L.iy1, L.ix1, t, q, u, L.dy * L.dx, unused);
 }
 
-template<bool RESP, bool PERIODIC>
+// cp.async of 16 bytes, global -> shared (L2 only), and its group bookkeeping.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const uint32_t d = (uint32_t) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template<int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template<bool RESP, bool PERIODIC, int FLUSH>
 __global__ void __launch_bounds__(BNT, 2)
 planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner,
                      const uint32_t *__restrict__ cellmap)
 {
+    extern __shared__ float s_lines[];    // [BW][BP][4 rows][32]: y, x, alpha, TOD
     __shared__ uint16_t s_tab[BW][32];
     __shared__ uint32_t s_err[BW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t nw = (int64_t) gridDim.x * BW;
     const int64_t gw = (int64_t) blockIdx.x * BW + warp;
     const int64_t e0 = (nowner * gw) / nw, e1 = (nowner * (gw + 1)) / nw;
+    const int64_t n = e1 - e0;
     const uint32_t nsamp = (uint32_t) a.nsamp;
     const uint32_t nlines = nsamp >> 5;
-    const float *__restrict__ yrow = a.xp;
-    const float *__restrict__ xrow = a.xp + nsamp;
-    const float *__restrict__ arow = a.xp + 2 * (size_t) nsamp;
     uint32_t err = a.partial ? 0u : check_plan_cells(cellmap, a);
     uint16_t *tab = s_tab[warp];
+    float *ring = s_lines + (size_t) warp * BP * 128;
+    // This lane's 16-byte piece of every line: row lane/8 (y, x, alpha, TOD), samples 4 (lane%8) + [0, 4).
+    const int row = lane >> 3, piece = 4 * (lane & 7);
+    const float *__restrict__ src_row = (row < 3) ? (a.xp + (size_t) row * nsamp) : a.in;
 
     BandState B;
 #pragma unroll
@@ -1023,50 +1043,78 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
     B.key = kNoKey;
     B.R0 = 0;
     B.x0 = 0;
+    int64_t run = 0;   // lines in the accumulator since its last flush (precision modes cap it)
 
-    for (int64_t c = e0; c < e1; c += 32) {
-        const int n = (int) ((e1 - c < 32) ? (e1 - c) : 32);
-        const uint64_t w = (lane < n) ? __ldg(owner_mt + c + lane) : 0ull;
-        const uint32_t wline = (uint32_t) ((w >> 20) & kClMask);
-        const uint32_t wkey = (uint32_t) (w & kCellMask) | ((uint32_t) ((w >> kBandShift) & 63u) << 20);
-        // A plan word always names a line < nsamp/32; anything else means the plan does not belong to
-        // this xpointing, so flag it and skip the line.
-        const bool bad = (lane < n) && (wline >= nlines);
-        err |= bad ? kErrInconsistentNmt : 0u;
-        const unsigned okmask = __ballot_sync(kFullMask, (lane < n) && !bad);
-        for (int j0 = 0; j0 < n; j0 += BUNR) {
-            float y[BUNR], x[BUNR], al[BUNR], tv[BUNR];
-            uint32_t key[BUNR], s[BUNR];
-            bool ok[BUNR];
-#pragma unroll
-            for (int u = 0; u < BUNR; u++) {
-                const int j = j0 + u;    // < 32: 32 is a multiple of BUNR
-                ok[u] = (okmask >> j) & 1u;
-                s[u] = (__shfl_sync(kFullMask, wline, j) << 5) + (uint32_t) lane;
-                key[u] = __shfl_sync(kFullMask, wkey, j);
-                y[u] = ok[u] ? __ldcs(yrow + s[u]) : 0.0f;
-                x[u] = ok[u] ? __ldcs(xrow + s[u]) : 0.0f;
-                al[u] = ok[u] ? __ldcs(arow + s[u]) : 0.0f;
-                tv[u] = ok[u] ? __ldcs(a.in + s[u]) : 0.0f;
-            }
-#pragma unroll
-            for (int u = 0; u < BUNR; u++) {
-                if (!ok[u])
-                    continue;
-                if (key[u] != B.key) {
-                    if (B.key != kNoKey)
-                        band_flush<PERIODIC>(a, B);
-                    B.key = key[u];
-                    B.R0 = ((int) ((key[u] >> 10) & 1023u) << 6) + (int) (key[u] >> 20);
-                    B.x0 = (int) (key[u] & 1023u) << 6;
-                }
-                if (!band_line<RESP, PERIODIC>(a, B, tab, y[u], x[u], al[u], tv[u], s[u]))
-                    band_general_sample<RESP, PERIODIC>(a, y[u], x[u], al[u], tv[u], s[u], err);
-            }
+    // Owner words of entries [32 G, 32 G + 64) of this warp's range: lane i holds entry 32 G + i (A)
+    // and 32 (G + 1) + i (B), decoded as (line, key); lines >= nlines (a plan that does not belong to
+    // this xpointing) are flagged and skipped.
+    auto decode = [&](int64_t g, uint32_t &line, uint32_t &key) {
+        const int64_t q = 32 * g + lane;
+        const uint64_t w = (q < n) ? __ldg(owner_mt + e0 + q) : 0ull;
+        line = (q < n) ? (uint32_t) ((w >> 20) & kClMask) : 0xffffffffu;
+        key = (uint32_t) (w & kCellMask) | ((uint32_t) ((w >> kBandShift) & 63u) << 20);
+        if ((q < n) && (line >= nlines)) {
+            err |= kErrInconsistentNmt;
+            line = 0xffffffffu;
         }
+    };
+    uint32_t lineA, keyA, lineB, keyB;
+    decode(0, lineA, keyA);
+    decode(1, lineB, keyB);
+    int64_t G = 0;
+
+    // Entry q's line (0xffffffff: none), for q in groups G and G + 1; warp-uniform.
+    auto line_of = [&](int64_t q) -> uint32_t {
+        const uint32_t la = __shfl_sync(kFullMask, lineA, (int) (q & 31));
+        const uint32_t lb = __shfl_sync(kFullMask, lineB, (int) (q & 31));
+        return ((q >> 5) == G) ? la : lb;
+    };
+    // Starts the copy of entry q's line into its ring slot (always commits one group, maybe empty).
+    auto issue = [&](int64_t q) {
+        const uint32_t line = (q < n) ? line_of(q) : 0xffffffffu;
+        if (line != 0xffffffffu)
+            cp_async16(ring + (q & (BP - 1)) * 128 + 32 * row + piece, src_row + 32 * (size_t) line + piece);
+        cp_async_commit();
+    };
+
+#pragma unroll 1
+    for (int q = 0; q < BP - 1; q++)
+        issue(q);
+#pragma unroll 1
+    for (int64_t q = 0; q < n; q++) {
+        if (((q & 31) == 0) && (q > 0)) {
+            lineA = lineB;
+            keyA = keyB;
+            G++;
+            decode(G + 1, lineB, keyB);
+        }
+        issue(q + BP - 1);             // into the slot of line q - 1, released at the end of that step
+        cp_async_wait<BP - 1>();       // this lane's piece of line q has landed
+        __syncwarp();
+        const uint32_t line = __shfl_sync(kFullMask, lineA, (int) (q & 31));
+        const uint32_t key = __shfl_sync(kFullMask, keyA, (int) (q & 31));
+        if (line != 0xffffffffu) {
+            const float *slot = ring + (q & (BP - 1)) * 128;
+            const float y = slot[lane], x = slot[32 + lane], al = slot[64 + lane], tv = slot[96 + lane];
+            const uint32_t s = (line << 5) + (uint32_t) lane;
+            if ((key != B.key) || ((FLUSH != kFlushF32) && (a.max_run_lines > 0) && (run >= a.max_run_lines))) {
+                if (B.key != kNoKey)
+                    band_flush<PERIODIC, FLUSH>(a, B);
+                B.key = key;
+                B.R0 = ((int) ((key >> 10) & 1023u) << 6) + (int) (key >> 20);
+                B.x0 = (int) (key & 1023u) << 6;
+                run = 0;
+            }
+            if (band_line<RESP, PERIODIC>(a, B, tab, y, x, al, tv, s))
+                run++;
+            else
+                band_general_sample<RESP, PERIODIC, FLUSH>(a, y, x, al, tv, s, err);
+        }
+        __syncwarp();                  // everyone is done with this slot before it is refilled
     }
+    cp_async_wait<0>();
     if (B.key != kNoKey)
-        band_flush<PERIODIC>(a, B);
+        band_flush<PERIODIC, FLUSH>(a, B);
     block_publish_err(err, s_err, a.errword);
 }
 
@@ -1273,21 +1321,31 @@ cudaError_t launch_planned_periodic(const OpArgs &a, const uint64_t *owner_mt, i
 }
 
 // Band-path tod2map: one warp per contiguous range of at least 32 owner entries, up to
-// ctas_per_sm (default 2) CTAs of BW warps per SM.
-template<bool RESP>
+// ctas_per_sm (default 2) CTAs of BW warps per SM.  Needs xpointing and the TOD 16-byte aligned
+// (the cp.async line copies); the caller falls back to the tile kernel otherwise.
+template<bool RESP, bool PERIODIC, int FLUSH>
+cudaError_t launch_tod2map_band_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner,
+                                     const uint32_t *cellmap, cudaStream_t stream)
+{
+    static std::atomic<uint64_t> attr_done{0};
+    cudaError_t e = set_smem_limit(planned_tod2map_band<RESP, PERIODIC, FLUSH>, kBandSmem, attr_done);
+    if (e != cudaSuccess)
+        return e;
+    const int per_sm = (a.ctas_per_sm > 0) ? a.ctas_per_sm : 2;
+    int64_t g = (nowner + 32 * BW - 1) / (32 * BW);
+    g = std::max<int64_t>(1, std::min<int64_t>(g, (int64_t) per_sm * device_sm_count()));
+    planned_tod2map_band<RESP, PERIODIC, FLUSH><<<(unsigned) g, BNT, kBandSmem, stream>>>(a, owner_mt, nowner, cellmap);
+    return cudaGetLastError();
+}
+
+template<bool RESP, int FLUSH>
 cudaError_t launch_tod2map_band(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                 cudaStream_t stream)
 {
     if (nowner <= 0)
         return cudaSuccess;
-    const int per_sm = (a.ctas_per_sm > 0) ? a.ctas_per_sm : 2;
-    int64_t g = (nowner + 32 * BW - 1) / (32 * BW);
-    g = std::max<int64_t>(1, std::min<int64_t>(g, (int64_t) per_sm * device_sm_count()));
-    if (a.periodic)
-        planned_tod2map_band<RESP, true><<<(unsigned) g, BNT, 0, stream>>>(a, owner_mt, nowner, cellmap);
-    else
-        planned_tod2map_band<RESP, false><<<(unsigned) g, BNT, 0, stream>>>(a, owner_mt, nowner, cellmap);
-    return cudaGetLastError();
+    return a.periodic ? launch_tod2map_band_impl<RESP, true, FLUSH>(a, owner_mt, nowner, cellmap, stream)
+                      : launch_tod2map_band_impl<RESP, false, FLUSH>(a, owner_mt, nowner, cellmap, stream);
 }
 
 template<bool TOD2MAP, bool RESP>
@@ -1295,12 +1353,18 @@ cudaError_t launch_planned_dispatch(const OpArgs &a, const uint64_t *owner_mt, i
                                     cudaStream_t stream)
 {
     if constexpr (TOD2MAP) {
+        const bool aligned = ((((uintptr_t) a.xp) | ((uintptr_t) a.in)) & 15) == 0;
+        if ((g_tod2map_kernel == GMM_TOD2MAP_BANDS) && aligned) {
+            if (a.flush == kFlushCompensated)
+                return launch_tod2map_band<RESP, kFlushCompensated>(a, owner_mt, nowner, cellmap, stream);
+            if (a.flush == kFlushF64)
+                return launch_tod2map_band<RESP, kFlushF64>(a, owner_mt, nowner, cellmap, stream);
+            return launch_tod2map_band<RESP, kFlushF32>(a, owner_mt, nowner, cellmap, stream);
+        }
         if (a.flush == kFlushCompensated)
             return launch_planned_periodic<true, RESP, kFlushCompensated>(a, owner_mt, nowner, cellmap, stream);
         if (a.flush == kFlushF64)
             return launch_planned_periodic<true, RESP, kFlushF64>(a, owner_mt, nowner, cellmap, stream);
-        if (g_tod2map_kernel == GMM_TOD2MAP_BANDS)
-            return launch_tod2map_band<RESP>(a, owner_mt, nowner, cellmap, stream);
     }
     return launch_planned_periodic<TOD2MAP, RESP, kFlushF32>(a, owner_mt, nowner, cellmap, stream);
 }

@@ -338,117 +338,134 @@ class LocalMap:
 
 class DynamicMap:
     """
-    A LocalMap that starts with zero cells and grows as tod2map() touches new cells; call finalize()
-    to obtain a LocalMap (gpu_mm.py:586-806).  Layout: float32 local_map[ncells][3][64][64].
-    'cell_mask' (bool, (nycells, nxcells)) restricts growth to a target region.
+    A local map that grows while tod2map() runs (the reference's DynamicMap, gpu_mm.py:586-806, with
+    the same constructor, methods and errors).  It starts with no cells; every tod2map() into it,
+    which needs a PointingPlan, first adds the cells that plan touches, zero-filled, then accumulates.
+    finalize() ends the growth and returns a LocalMap.  map2tod() does not take a DynamicMap.
+
+    Storage: float32 [ncells][3][64][64] on the device, cells in the order they were first touched
+    (unspecified between runs), or in the order given to permute().  The cell table is the device
+    cell_offsets array of a LocalPixelization: -1 marks a cell that may still be added, -2 a cell
+    outside 'cell_mask' (bool (nycells, nxcells), True where cells may be added), offsets >= 0 the
+    cells present.  New cells are found and numbered on the device (expand_dynamic_map2); only their
+    number comes back to the host.  The cell buffer is a capacity of whole cells that grows to the
+    next power of two when it overflows (one device copy per growth), so N cells cost O(log N)
+    reallocations.
     """
 
+    _GROWING, _PERMUTED, _FINALIZED = 0, 1, 2
+    _CELL = 3 * 64 * 64
+
     def __init__(self, nypix_global, nxpix_global, dtype, cell_mask=None, periodic_xcoord=True, initial_ncells=1024):
-        assert 0 < nxpix_global <= 64 * 1024
         assert 0 < nypix_global <= 64 * 1024
-        assert np.dtype(dtype) == np.float32 or dtype == torch.float32
+        assert 0 < nxpix_global <= 64 * 1024
+        assert np.dtype(dtype) == np.float32 or dtype == torch.float32, "DynamicMap: only float32 maps"
         assert initial_ncells > 0
-
-        self.nypix_global = nypix_global
-        self.nxpix_global = nxpix_global
+        self.nypix_global, self.nxpix_global = nypix_global, nxpix_global
         self.periodic_xcoord = periodic_xcoord
-        self.have_cell_mask = (cell_mask is not None)
-        self.ncells_allocated = initial_ncells
-        self.reallocation_factor = 1.5
         self.dtype = np.float32
-
-        # cell_offsets: -1 for "targeted" cells, -2 for "untargeted" ones (expand_dynamic_map.cu:67-68).
+        self.have_cell_mask = cell_mask is not None
+        shape = ((nypix_global + 63) // 64, (nxpix_global + 63) // 64)
         if cell_mask is None:
-            nycells = (nypix_global + 63) // 64
-            nxcells = (nxpix_global + 63) // 64
-            cell_offsets = np.full((nycells, nxcells), -1, dtype=np.int64)
+            table = np.full(shape, -1, dtype=np.int64)
         else:
             cell_mask = np.asarray(cell_mask)
-            assert cell_mask.ndim == 2
-            assert cell_mask.dtype == bool
-            cell_offsets = np.where(cell_mask, -1, -2).astype(np.int64)
+            assert cell_mask.ndim == 2 and cell_mask.dtype == bool, "DynamicMap: cell_mask must be a 2-d bool array"
+            table = np.where(cell_mask, -1, -2).astype(np.int64)
+        # The cell layout [ncells][3][64][64]: ystride 64, polstride 64*64.
+        self._unstable_pixelization = LocalPixelization(nypix_global, nxpix_global, table, ystride=64,
+                                                        polstride=64 * 64, periodic_xcoord=periodic_xcoord)
+        self.global_ncells = torch.zeros(32, dtype=torch.int32, device="cuda")[:1]   # device cell counter
+        self._cells = torch.zeros((initial_ncells, 3, 64, 64), dtype=torch.float32, device="cuda")
+        self._n = 0
+        self._state = self._GROWING
+        self._view()
 
-        self._unstable_pixelization = LocalPixelization(nypix_global, nxpix_global, cell_offsets,
-                                                        ystride=64, polstride=64 * 64, periodic_xcoord=periodic_xcoord)
-        self._padded_arr = torch.zeros(self.ncells_allocated * 3 * 64 * 64, dtype=torch.float32, device="cuda")
-        self._unstable_arr = self._padded_arr[:0]
-        self.global_ncells = torch.zeros(32, dtype=torch.int32, device="cuda")[:1]
-        self.ncells_curr = 0
-        self.pixelization_is_finalized = False
-        self.map_is_finalized = False
+    # Read-only state under the reference's attribute names.
+    ncells_curr = property(lambda self: self._n)
+    ncells_allocated = property(lambda self: self._n if self._cells is None else int(self._cells.shape[0]))
+    pixelization_is_finalized = property(lambda self: self._state != self._GROWING)
+    map_is_finalized = property(lambda self: self._state == self._FINALIZED)
+
+    def _view(self):
+        """Points the pixelization's npix and the flat map array at the cells present."""
+        self._unstable_pixelization.npix = 64 * 64 * self._n
+        self._unstable_arr = self._cells[:self._n].view(-1)
+
+    def _reserve(self, n):
+        cap = int(self._cells.shape[0])
+        if n <= cap:
+            return
+        grown = torch.zeros((1 << (n - 1).bit_length(), 3, 64, 64), dtype=torch.float32, device="cuda")
+        grown[:self._n].copy_(self._cells[:self._n])
+        self._cells = grown
 
     def expand(self, plan):
-        """Adds the cells a PointingPlan touches, zero-initialised (gpu_mm.py:674-702)."""
-        if self.pixelization_is_finalized:
+        """Adds the cells 'plan' touches (zero-filled), as tod2map() does before accumulating."""
+        if self._state != self._GROWING:
             raise RuntimeError("Can't currently call tod2map() [or DynamicMap.expand()]"
                                + " after MpiPixelization.__init__() [or DynamicMap.permute()].")
         assert isinstance(plan, PointingPlan)
-        assert plan.nypix_global == self.nypix_global
-        assert plan.nxpix_global == self.nxpix_global
+        assert (plan.nypix_global, plan.nxpix_global) == (self.nypix_global, self.nxpix_global)
         assert plan.periodic_xcoord == self.periodic_xcoord
-
-        self.ncells_curr = gpu_mm_pybind11.expand_dynamic_map2(self.global_ncells, self._unstable_pixelization, plan)
-
-        if self.ncells_curr > self.ncells_allocated:
-            self.ncells_allocated = int(self.reallocation_factor * self.ncells_allocated)
-            self.ncells_allocated = max(self.ncells_allocated, self.ncells_curr)
-            new = torch.zeros(self.ncells_allocated * 3 * 64 * 64, dtype=torch.float32, device="cuda")
-            new[:len(self._unstable_arr)] = self._unstable_arr[:]
-            self._padded_arr = new
-
-        self._unstable_pixelization.npix = self.ncells_curr * (64 * 64)
-        self._unstable_arr = self._padded_arr[:(self.ncells_curr * 3 * 64 * 64)]
+        n = gpu_mm_pybind11.expand_dynamic_map2(self.global_ncells, self._unstable_pixelization, plan)
+        self._reserve(n)
+        self._n = n
+        self._view()
 
     def permute(self, iycells, ixcells):
-        """Reorders the cells to the given (iycells, ixcells) order and finalizes the pixelization
-        (gpu_mm.py:705-757).  The data move is one gather on the device."""
-        if self.pixelization_is_finalized:
+        """Puts the cells in the order (iycells[i], ixcells[i]), i = 0..ncells-1 (host integer arrays
+        naming every present cell once), and ends the growth of the pixelization.  The data move is
+        one gather of whole cells on the device (cell_broadcast)."""
+        if self._state != self._GROWING:
             raise RuntimeError("Can't currently call MpiPixelization.__init__() [or DynamicMap.permute()]"
                                + " after DynamicMap.finalize() [or MpiPixelization.__init__(), DynamicMap.permute()]")
-        self._unstable_pixelization.copy_gpu_offsets_to_cpu()
-        assert self._unstable_pixelization.npix == (self.ncells_curr * 64 * 64)
-        new_offsets = self._unstable_pixelization.cell_offsets_cpu
-        old_offsets = np.copy(new_offsets)
-
-        assert isinstance(iycells, np.ndarray) and isinstance(ixcells, np.ndarray)
-        assert iycells.shape == ixcells.shape == (self.ncells_curr,)
-        assert 0 <= np.min(iycells) <= np.max(iycells) < old_offsets.shape[0]
-        assert 0 <= np.min(ixcells) <= np.max(ixcells) < old_offsets.shape[1]
-
-        new_offsets[iycells, ixcells] = np.arange(self.ncells_curr) * (3 * 64 * 64)
-        if not np.all((old_offsets >= 0) == (new_offsets >= 0)):
+        lp = self._unstable_pixelization
+        lp.copy_gpu_offsets_to_cpu()
+        table = lp.cell_offsets_cpu
+        n = self._n
+        assert isinstance(iycells, np.ndarray) and isinstance(ixcells, np.ndarray), "permute(): host arrays"
+        assert iycells.shape == ixcells.shape == (n,)
+        assert np.issubdtype(iycells.dtype, np.integer) and np.issubdtype(ixcells.dtype, np.integer)
+        if n:
+            assert 0 <= iycells.min() and iycells.max() < table.shape[0]
+            assert 0 <= ixcells.min() and ixcells.max() < table.shape[1]
+        flat = iycells.astype(np.int64) * table.shape[1] + ixcells.astype(np.int64)
+        if not np.array_equal(np.sort(flat), np.flatnonzero(table >= 0)):
             raise RuntimeError('DynamicMap.permute(): specified (iycells,ixcells) do not match footprint of current pixelization')
-
-        self.pixelization_is_finalized = True
-        self._unstable_pixelization.copy_cpu_offsets_to_gpu()
-        assert self._unstable_pixelization.npix == (self.ncells_curr * 64 * 64)
-
-        src_cells = torch.as_tensor(old_offsets[iycells, ixcells] // (3 * 64 * 64), device="cuda")
-        old = self._unstable_arr.view(-1, 3 * 64 * 64)
-        self._padded_arr = self._unstable_arr = old.index_select(0, src_cells).reshape(-1).contiguous()
-        self.ncells_allocated = self.ncells_curr
+        src = table[iycells, ixcells] // self._CELL          # current position of each new cell
+        table[iycells, ixcells] = self._CELL * np.arange(n, dtype=np.int64)
+        lp.copy_cpu_offsets_to_gpu()
+        out = torch.empty((n, 3, 64, 64), dtype=torch.float32, device="cuda")
+        if n:
+            gpu_mm_pybind11.cell_broadcast(out.view(-1), self._cells[:n].reshape(-1),
+                                           torch.as_tensor(src, dtype=torch.int64, device="cuda"))
+        self._cells = out
+        self._state = self._PERMUTED
+        self._view()
 
     def finalize(self):
-        """Called at the end of the TOD loop; returns a LocalMap (gpu_mm.py:760-779)."""
-        if self.map_is_finalized:
+        """Ends the TOD loop: returns the LocalMap (its pixelization lists the cells present, with
+        cell_offsets[iycell, ixcell] = 3*64*64 * i for the i-th cell; absent cells are negative)."""
+        if self._state == self._FINALIZED:
             raise RuntimeError('Double call to DynamicMap.finalize() [not currently allowed]')
-        if not self.pixelization_is_finalized:
+        if self._state == self._GROWING:
             self._unstable_pixelization.copy_gpu_offsets_to_cpu()
-            self.pixelization_is_finalized = True
-        if self.ncells_allocated > self.ncells_curr:
-            self._unstable_arr = self._unstable_arr.clone()
-        ret = LocalMap(self._unstable_pixelization, self._unstable_arr)
-        assert self._unstable_pixelization.npix == (self.ncells_curr * 64 * 64)
-        self._padded_arr = self._unstable_arr = None
-        self.map_is_finalized = True
+        cells = self._cells[:self._n]
+        if self._cells.shape[0] > self._n:
+            cells = cells.clone()                 # drop the spare capacity
+        ret = LocalMap(self._unstable_pixelization, cells.view(-1))
+        assert self._unstable_pixelization.npix == 64 * 64 * self._n
+        self._cells = self._unstable_arr = None
+        self._state = self._FINALIZED
         return ret
 
     def randomly_permute(self):
-        """Only called during testing."""
+        """permute() into a random order of the present cells (for tests of permute())."""
         self._unstable_pixelization.copy_gpu_offsets_to_cpu()
-        iycells, ixcells = np.where(self._unstable_pixelization.cell_offsets_cpu >= 0)
-        perm = np.random.permutation(self.ncells_curr)
-        self.permute(iycells[perm], ixcells[perm])
+        iy, ix = np.nonzero(self._unstable_pixelization.cell_offsets_cpu >= 0)
+        order = np.random.permutation(len(iy))
+        self.permute(iy[order], ix[order])
 
 
 ####################################################################################################

@@ -268,9 +268,10 @@ def refgpu_unplanned_tod2map(lmap, tod, xp, lp, offs_gpu, errflags, partial=Fals
 
 
 def refgpu_plan_tester(xp_gpu, nypix_global, nxpix_global, periodic_xcoord=True, capacity=None):
-    """The reference's PointingPlanTester (PointingPlanTester.cu:69-161): (sorted_mt, nmt_cumsum)."""
+    """The reference's PointingPlanTester (PointingPlanTester.cu:69-161): (sorted_mt, nmt_cumsum).
+    'capacity' (at least the plan's nmt) sizes the output; by default 4 words per cache line."""
     nsamp = xp_gpu.numel() // 3
-    cap = int(capacity) if capacity else 8 * (nsamp // 32) + 64
+    cap = int(capacity) if capacity else 4 * (nsamp // 32) + 64
     mt = np.zeros(cap, np.uint64)
     cs = np.zeros(1024, np.uint32)
     n = ctypes.c_long()

@@ -453,7 +453,9 @@ static inline void sample_slots(int iy0, int iy1, int ix0, int ix1, int slots[6]
 }
 
 /* Distinct cells of one 32-sample cache line: entries grouped by slot (slot order), within a slot
- * in order of the lowest lane holding the cell (PointingPlan.cu:27-35, :71-73).
+ * in order of the HIGHEST lane holding the cell.  The reference's cell_analysis marks a cell at the
+ * lane where (match_any mask >> lane) == 1, i.e. at its highest lane (PointingPlan.cu:27-35), and the
+ * ring buffer takes the marked lanes in lane order (__fns, :71-73).
  * Returns the entry count; na[k] gets per-slot counts. */
 static int line_cells(const float *xp, int64_t nsamp, int64_t icl, int ny, int nx, int periodic,
                       int cells_out[192], int na[6], uint32_t *err)
@@ -472,10 +474,10 @@ static int line_cells(const float *xp, int64_t nsamp, int64_t icl, int ny, int n
         for (int lane = 0; lane < 32; lane++) {
             int c = slots[lane][k];
             if (c < 0) continue;
-            int seen = 0;
-            for (int j = n0; j < n; j++)
-                if (cells_out[j] == c) { seen = 1; break; }
-            if (!seen) cells_out[n++] = c;
+            int later = 0;
+            for (int j = lane + 1; j < 32; j++)
+                if (slots[j][k] == c) { later = 1; break; }
+            if (!later) cells_out[n++] = c;
         }
         na[k] = n - n0;
     }

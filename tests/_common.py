@@ -23,7 +23,8 @@ def literal_enumerate(iy0, iy1, ix0, ix1):
 
 def literal_plan_words(located, nsamp):
     """Simulates the reference's plan_kernel (PointingPlan.cu:121-231 with W=4) warp by warp:
-    cell_analysis (match_any + ballot over the 32 lanes), mt_ringbuf::absorb with its running
+    cell_analysis (match_any + ballot over the 32 lanes, each cell at its highest lane),
+    mt_ringbuf::absorb with its running
     nmt_local / na_cumul, and the per-line na_cumul reset.  'located' is a list of
     (iy0, iy1, ix0, ix1) per sample.  Returns the emitted 64-bit words (unordered)."""
     ncl = nsamp // 32
@@ -44,8 +45,10 @@ def literal_plan_words(located, nsamp):
                     active = []
                     for lane in range(32):
                         v, valid = icells[lane]
-                        lowest = all(icells[j][0] != v for j in range(lane))
-                        if valid and lowest:
+                        # cell_analysis (PointingPlan.cu:27-35): is_lowest = ((mmask >> lane) == 1),
+                        # which holds at the HIGHEST lane of the matching lanes.
+                        highest = all(icells[j][0] != v for j in range(lane + 1, 32))
+                        if valid and highest:
                             active.append(v)
                     cas.append(active)
                 mflag = sum(len(a) for a in cas) > 1

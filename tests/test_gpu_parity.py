@@ -406,6 +406,54 @@ def test_dynamic_map(g):
     assert rl1 < RL1_TOL and mx < MAX_TOL
 
 
+def test_dynamic_map_cell_mask_growth_and_errors(g):
+    """A cell mask limits growth to the target cells (tod2map with partial_pixelization, as the
+    reference requires); capacity grows from one cell; permute() rejects a cell list that is not the
+    footprint; the map cannot grow after permute() or be finalized twice."""
+    import torch
+    rng = np.random.default_rng(33)
+    ny, nx = 256, 512
+    xp = random_raster(rng, 4, 2048, ny, nx, True, speed=0.8)
+    t = rng.standard_normal((4, 2048)).astype(np.float32)
+    nyc, nxc = 4, 8
+    mask = np.zeros((nyc, nxc), bool)
+    mask[:, ::2] = True
+    mask[1, :] = True
+    offs = np.full((nyc, nxc), -1, np.int64)
+    for k, (iy, ix) in enumerate(zip(*np.nonzero(mask))):
+        offs[iy, ix] = 3 * 4096 * k
+    lp_o = oracle.Lpix(ny, nx, offs, 64, 4096, True)
+    want = np.zeros(3 * lp_o.npix, np.float32)
+    oracle.tod2map(want, t, xp, lp_o, True)
+    xc = cuda(xp)
+    plan = g.PointingPlan(g.PointingPrePlan(xc, ny, nx), xc)
+    dmap = g.DynamicMap(ny, nx, np.float32, cell_mask=mask, initial_ncells=1)
+    with pytest.raises(RuntimeError, match="have_cell_mask"):
+        g.tod2map(dmap, cuda(t), xc, plan, partial_pixelization=False)
+    g.tod2map(dmap, cuda(t), xc, plan, partial_pixelization=True)
+    touched = {(int(c) >> 10, int(c) & 1023) for c in np.unique(plan.get_plan_mt() & np.uint64(0xFFFFF))}
+    present = {c for c in touched if mask[c]}
+    assert dmap.ncells_curr == len(present) and dmap.ncells_allocated >= dmap.ncells_curr
+    iy, ix = np.nonzero(dmap._unstable_pixelization.cell_offsets_gpu.cpu().numpy() >= 0)
+    assert set(zip(iy.tolist(), ix.tolist())) == present
+    with pytest.raises(RuntimeError, match="do not match footprint"):
+        dmap.permute(np.append(iy[:-1], iy[0]), np.append(ix[:-1], ix[0]))
+    dmap.permute(iy[::-1].copy(), ix[::-1].copy())
+    with pytest.raises(RuntimeError, match="after MpiPixelization"):
+        dmap.expand(plan)
+    lmap = dmap.finalize()
+    with pytest.raises(RuntimeError, match="Double call"):
+        dmap.finalize()
+    got = lmap.to_global()
+    ref_global = np.zeros((3, ny, nx), np.float32)
+    for (cy, cx) in present:
+        k = offs[cy, cx] // 4096
+        blk = want.reshape(-1, 3, 64, 64)[k // 3]
+        ref_global[:, 64 * cy:64 * cy + 64, 64 * cx:64 * cx + 64] = blk[:, :min(64, ny - 64 * cy), :min(64, nx - 64 * cx)]
+    rl1, mx = rel_stats(got, ref_global)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+
+
 def test_reference_cpu_operators(g):
     """plan='reference' runs the library's CPU operator and agrees with the oracle."""
     rng = np.random.default_rng(4)

@@ -130,8 +130,8 @@ def test_precision_modes_full_size_high_hit(g):
     """The high-hit precision workload at its full size: 64 detectors x 2^22 samples (2^28) confined to
     the 512x512 box [256, 768)^2 of a 3x1024x1024 map (~1000 hits/pixel), tod = 1e3 + N(0,1), against
     the FP64 oracle over the whole TOD.  Bars: the north star's 1e-5 max relative error for the float
-    path (both tod2map kernels); 1e-6 max and 2e-7 rms for the compensated and float64-map modes
-    (runs of 1024 lines)."""
+    path (both tod2map kernels); 1e-6 max and 2e-7 rms for the compensated and float64-map modes on
+    both kernels, with float partials of at most 32 lines (max_run_lines)."""
     import ctypes
     import os
     import torch
@@ -155,17 +155,19 @@ def test_precision_modes_full_size_high_hit(g):
             m = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
             g.tod2map(m, tg, xg, plan)
             errs[f"fp32-{which}"] = err_vs(m.arr.cpu().numpy(), want)
+        for which in (0, 1):
+            lib.gmm_set_planned_tod2map_kernel(which)
+            m = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+            comp = torch.zeros(3 * lp.npix, device="cuda")
+            g.tod2map_compensated(m, comp, tg, xg, plan, max_run_lines=32)
+            g.fold_compensation(m, comp)
+            errs[f"compensated-{which}"] = err_vs(m.arr.cpu().numpy(), want)
+            m64 = torch.zeros(3 * lp.npix, dtype=torch.float64, device="cuda")
+            g.tod2map_f64(m64, lp, tg, xg, plan, max_run_lines=32)
+            errs[f"fp64map-{which}"] = err_vs(m64.cpu().numpy(), want)
     finally:
         lib.gmm_set_planned_tod2map_kernel(old)
-    m = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
-    comp = torch.zeros(3 * lp.npix, device="cuda")
-    g.tod2map_compensated(m, comp, tg, xg, plan, max_run_lines=1024)
-    g.fold_compensation(m, comp)
-    errs["compensated"] = err_vs(m.arr.cpu().numpy(), want)
-    m64 = torch.zeros(3 * lp.npix, dtype=torch.float64, device="cuda")
-    g.tod2map_f64(m64, lp, tg, xg, plan, max_run_lines=1024)
-    errs["fp64map"] = err_vs(m64.cpu().numpy(), want)
     for k in ("fp32-0", "fp32-1"):
         assert errs[k][0] < 1e-5, (k, errs)
-    for k in ("compensated", "fp64map"):
+    for k in ("compensated-0", "compensated-1", "fp64map-0", "fp64map-1"):
         assert errs[k][0] < 1e-6 and errs[k][1] < 2e-7, (k, errs)

@@ -79,7 +79,7 @@ def test_plan_equals_reference_plan_tester(g, i):
     xg = torch.from_numpy(np.ascontiguousarray(xp)).cuda()
     pp = g.PointingPrePlan(xg, ny, nx, periodic_xcoord=periodic)
     plan = g.PointingPlan(pp, xg)
-    t_mt, t_cs = oracle.refgpu_plan_tester(xg, ny, nx, periodic)
+    t_mt, t_cs = oracle.refgpu_plan_tester(xg, ny, nx, periodic, capacity=pp.plan_nmt)
     np.testing.assert_array_equal(pp.get_nmt_cumsum(), t_cs[:pp.planner_nblocks])
     low = np.uint64((1 << 46) - 1)
     np.testing.assert_array_equal(np.sort(plan.get_plan_mt() & low), np.sort(t_mt & low))
