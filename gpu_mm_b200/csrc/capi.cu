@@ -281,7 +281,8 @@ int gmm_preplan_info_init(int64_t nsamp, int32_t ny, int32_t nx, int32_t periodi
 
     const int64_t ncl = nsamp / 32;
     const int64_t max_nblocks = std::max(info->planner_nblocks, info->pointing_nblocks);
-    info->plan_nbytes = align128(8 * nmt) + align128(4 * max_nblocks) + align128(8 * ncl) + kCellmapBytes;
+    info->plan_nbytes = align128(8 * nmt) + align128(4 * max_nblocks) + align128(8 * ncl) + kCellmapBytes +
+                        align128(8 * ncl);
     info->plan_constructor_tmp_nbytes = align128(8 * nmt) + align128(8 * ncl) + info->sort_nbytes;
     return 0;
 }
@@ -295,7 +296,8 @@ int gmm_plan_layout_get(const gmm_preplan_info *info, gmm_plan_layout *layout)
     layout->err_offset = align128(8 * info->plan_nmt);
     layout->owner_offset = layout->err_offset + align128(4 * max_nblocks);
     layout->cellmap_offset = layout->owner_offset + align128(8 * (info->nsamp / 32));
-    layout->total_nbytes = layout->cellmap_offset + kCellmapBytes;
+    layout->band_offset = layout->cellmap_offset + kCellmapBytes;
+    layout->total_nbytes = layout->band_offset + align128(8 * (info->nsamp / 32));
     return 0;
 }
 
@@ -354,6 +356,7 @@ int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum, con
     uint32_t *errflags = (uint32_t *) (b + lay.err_offset);
     uint64_t *owner = (uint64_t *) (b + lay.owner_offset);
     uint32_t *cellmap = (uint32_t *) (b + lay.cellmap_offset);
+    uint64_t *band = (uint64_t *) (b + lay.band_offset);
     const int64_t nmt = info->plan_nmt, ncl = info->nsamp / 32;
     char *t = (char *) tmp;
     uint64_t *mt_alt = (uint64_t *) t;
@@ -375,12 +378,18 @@ int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum, con
     if (e == cudaSuccess)
         e = launch_plan_emit(xp, info->nsamp, info->nypix_global, info->nxpix_global, info->periodic_xcoord != 0,
                              info->ncl_per_threadblock, (int) info->planner_nblocks, nmt_cumsum,
-                             even ? plan_mt : mt_alt, oeven ? owner : owner_alt, errflags, stream);
+                             even ? plan_mt : mt_alt, oeven ? owner : owner_alt, band, errflags, stream);
     if (e == cudaSuccess)
         e = radix_sort_mt(even ? plan_mt : mt_alt, even ? mt_alt : plan_mt, nmt, nyc, nxc, dbits, passes, hist, stream);
     if (e == cudaSuccess)
         e = radix_sort_mt(oeven ? owner : owner_alt, oeven ? owner_alt : owner, ncl, nyc, nxc, obits, opasses, hist,
                           stream, 0, kBandBits);
+    // Band words were written in line order; mt_alt (8 * nmt >= 8 * ncl bytes) is free after the sort
+    // of plan_mt, so they go there and come back in owner-list order.
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(mt_alt, band, 8 * ncl, cudaMemcpyDeviceToDevice, stream);
+    if (e == cudaSuccess)
+        e = launch_band_gather(owner, ncl, mt_alt, band, stream);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(cellmap, 0, kCellmapBytes, stream);
     if (e == cudaSuccess)
@@ -439,6 +448,7 @@ static int planned_op(bool tod2map, float *out, const float *in, const float *xp
     const char *b = (const char *) plan_buf;
     const uint64_t *owner = (const uint64_t *) (b + lay.owner_offset);
     const uint32_t *cellmap = (const uint32_t *) (b + lay.cellmap_offset);
+    const uint64_t *band = (const uint64_t *) (b + lay.band_offset);
     uint32_t *word = errword ? errword : (uint32_t *) (b + lay.err_offset);
 
     OpArgs a = make_args(lp, xp, info->nsamp, partial != 0, accum != 0, word);
@@ -456,7 +466,7 @@ static int planned_op(bool tod2map, float *out, const float *in, const float *xp
     }
     cudaError_t e = cudaMemsetAsync(word, 0, sizeof(uint32_t), stream);
     if (e == cudaSuccess)
-        e = tod2map ? launch_planned_tod2map(a, owner, info->nsamp / 32, cellmap, stream)
+        e = tod2map ? launch_planned_tod2map(a, owner, info->nsamp / 32, cellmap, band, stream)
                     : launch_planned_map2tod(a, owner, info->nsamp / 32, cellmap, stream);
     if (e != cudaSuccess)
         return cuda_fail(e, where);

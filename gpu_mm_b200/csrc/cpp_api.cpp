@@ -415,6 +415,7 @@ PointingPlan::PointingPlan(const PointingPrePlan &preplan, const Array<T> &xp, c
     plan_mt = (ulong *) (buf.data + lay.mt_offset);
     err_gpu = (uint *) (buf.data + lay.err_offset);
     owner_mt = (ulong *) (buf.data + lay.owner_offset);
+    band_words = (ulong *) (buf.data + lay.band_offset);
     throw_on_error(gmm_plan_build(&pp.info, (const uint32_t *) pp.nmt_cumsum.data, (const float *) xp.data,
                                   buf.data, buf.size, tmp_buf.data, tmp_buf.size, debug ? 1 : 0, 0));
 }
@@ -438,6 +439,14 @@ Array<ulong> PointingPlan::get_owner_mt(bool gpu) const
     const long n = nsamp / 32;
     Array<ulong> ret = gpu ? Array<ulong>::alloc_gpu({n}) : Array<ulong>::alloc_host({n});
     cuda_check(cudaMemcpy(ret.data, owner_mt, n * sizeof(ulong), cudaMemcpyDefault), "PointingPlan::get_owner_mt");
+    return ret;
+}
+
+Array<ulong> PointingPlan::get_band_words(bool gpu) const
+{
+    const long n = nsamp / 32;
+    Array<ulong> ret = gpu ? Array<ulong>::alloc_gpu({n}) : Array<ulong>::alloc_host({n});
+    cuda_check(cudaMemcpy(ret.data, band_words, n * sizeof(ulong), cudaMemcpyDefault), "PointingPlan::get_band_words");
     return ret;
 }
 

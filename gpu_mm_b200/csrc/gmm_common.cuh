@@ -123,10 +123,22 @@ __device__ __forceinline__ void line_slot_masks(const int slots[6], unsigned ama
 // (the hardware approximations' own error dominates; the tail term adds at most 163 * 2^-34).
 __device__ __forceinline__ void sincos_reduced(float th, float *s, float *c)
 {
-    const float j = rintf(th * 0.15915494309189535f);
+    // j = rint(th / 2pi), rounded by adding and subtracting 1.5 * 2^23 (round-to-nearest-even on the
+    // FMA pipe; exact for |th / 2pi| < 2^22), the same value rintf gives.
+    const float j = __fadd_rn(__fadd_rn(__fmul_rn(th, 0.15915494309189535f), 12582912.0f), -12582912.0f);
     float r = fmaf(j, -6.28125f, th);
     r = fmaf(j, -1.9353071795864769e-3f, r);
     __sincosf(r, s, c);
+}
+
+// floor(v) of a float v in [0, 2^23) as an int, and as an exact float in *fv, without a conversion
+// instruction: v + 2^23 rounded toward zero is 2^23 + floor(v), whose low mantissa bits are floor(v).
+// For v >= 0 this is the truncation __float2int_rz(v) that locate() uses, bit for bit.
+__device__ __forceinline__ int floor_nonneg(float v, float *fv)
+{
+    const float b = __fadd_rz(v, 8388608.0f);
+    *fv = __fadd_rn(b, -8388608.0f);
+    return __float_as_int(b) - 0x4B000000;
 }
 
 // sin(2a) and cos(2a) for the detector response: sincos_reduced for |2a| <= 1024, sincosf beyond.
@@ -137,6 +149,52 @@ __device__ __forceinline__ void sincos2a(float alpha, float *s, float *c)
         sincos_reduced(th, s, c);
     else
         sincosf(th, s, c);
+}
+
+// Band word of a line of a single-TOD plan (one per owner entry, stored in owner-list order): the
+// shape of the line as the tod2map band path needs it, computed once from the pointing when the
+// plan is built.  The band path accumulates a line in the rows R0, R0 + 1 and the columns
+// x0 + [0, 96) of its (cell, band) (R0 = 64 iycell + band, x0 = 64 ixcell); column k = floor(x) - x0.
+//   bits 0-31  bit i set iff sample i lies in the same column as sample i - 1 (i >= 1)
+//   bits 32-38 the first column in scan order, kmin (0..94)
+//   bits 39-44 number of columns, ncol (1..32): the columns are kmin .. kmin + ncol - 1
+//   bit  45    x increases along the line (scan order = lane order; else reversed)
+//   bit  46    the line takes the band path (all conditions of band_line_word below hold)
+//   bit  47    some column holds three or four consecutive samples
+constexpr int kBandKminShift = 32, kBandNcolShift = 39;
+constexpr uint64_t kBandInc = 1ull << 45, kBandFast = 1ull << 46, kBandRun3 = 1ull << 47;
+
+// The band word of one cache line, by the full warp (lane = sample).  The line takes the band path
+// (bit 46) iff every sample has y in [R0, R0 + 1) with R0 <= ny - 2 (upper neighbours in row R0; no
+// clamp in locate), x in [x0, x0 + 95) and x < x_hi (nx if periodic: no fold; nx - 2 otherwise:
+// in range), and the column moves along the line in one direction by 0 or 1 per sample, stays in
+// one column for at most four consecutive samples, and repeats at least once (so the line spans at
+// most 32 columns).  dy = y - R0 and xr = x - x0 are exact; non-negative floats compare as unsigned
+// integers (negative values and NaN fail).  The word is 0 when the line does not take the path.
+__device__ __forceinline__ uint64_t band_line_word(float y, float x, int R0, int x0, int ny, float x_hi)
+{
+    const int lane = threadIdx.x & 31;
+    const float dy = y - (float) R0;
+    const float xr = x - (float) x0;
+    const bool ok = (R0 <= ny - 2) && ((unsigned) __float_as_int(dy) < 0x3f800000u) &&
+                    ((unsigned) __float_as_int(xr) < 0x42be0000u) &&
+                    ((unsigned) __float_as_int(x) < (unsigned) __float_as_int(x_hi));
+    const int k = (int) floorf(xr);
+    const int dk = k - __shfl_up_sync(kFullMask, k, 1);
+    const unsigned su = __ballot_sync(kFullMask, (lane > 0) && (dk == 0));
+    const unsigned up = __ballot_sync(kFullMask, (lane > 0) && (dk == 1));
+    const unsigned down = __ballot_sync(kFullMask, (lane > 0) && (dk == -1));
+    const unsigned bad = __ballot_sync(kFullMask, !ok);
+    const unsigned r3 = su & (su >> 1);
+    const int k0 = __shfl_sync(kFullMask, k, 0), k31 = __shfl_sync(kFullMask, k, 31);
+    if ((bad != 0u) || ((su | up | down) != 0xfffffffeu) || ((up != 0u) && (down != 0u)) || (su == 0u) ||
+        ((r3 & (r3 >> 2)) != 0u))
+        return 0ull;
+    const bool inc = down == 0u;
+    const int kmin = inc ? k0 : k31;
+    const int ncol = (inc ? k31 : k0) - kmin + 1;
+    return (uint64_t) su | ((uint64_t) kmin << kBandKminShift) | ((uint64_t) ncol << kBandNcolShift) |
+           (inc ? kBandInc : 0ull) | kBandFast | ((r3 != 0u) ? kBandRun3 : 0ull);
 }
 
 // OR-reduce an error word over the block and publish it with one atomicOr per block (only if

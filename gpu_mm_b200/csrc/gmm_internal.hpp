@@ -31,7 +31,10 @@ cudaError_t launch_preplan(const float *xp, int64_t nsamp, int ny, int nx, bool 
                            int nblocks, uint32_t *nmt, uint32_t *err, cudaStream_t stream);
 cudaError_t launch_plan_emit(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
                              int nblocks, const uint32_t *nmt_cumsum, uint64_t *mt_out, uint64_t *owner_out,
-                             uint32_t *errflags, cudaStream_t stream);
+                             uint64_t *band_out, uint32_t *errflags, cudaStream_t stream);
+// Band words (gmm_common.cuh) from line order into owner-list order.
+cudaError_t launch_band_gather(const uint64_t *owner, int64_t n, const uint64_t *band_by_line, uint64_t *band_out,
+                               cudaStream_t stream);
 cudaError_t launch_plan_cellmap(const uint64_t *plan_mt, int64_t nmt, uint32_t *cellmap, cudaStream_t stream);
 cudaError_t launch_expand_dynamic_map(uint32_t *global_ncells, int64_t *cell_offsets, int nycells, int nxcells,
                                       const uint64_t *plan_mt, int64_t nmt, cudaStream_t stream);
@@ -100,8 +103,9 @@ extern int g_tod2map_kernel;
 
 cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                    cudaStream_t stream);
+// 'band' (tod2map): the plan's band words, one per owner entry, or null (batch-format plans).
 cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
-                                   cudaStream_t stream);
+                                   const uint64_t *band, cudaStream_t stream);
 cudaError_t launch_fold_compensation(float *lmap, float *comp, int64_t n, cudaStream_t stream);
 // Batches of TODs.
 constexpr int kBatchTodShift = 48;

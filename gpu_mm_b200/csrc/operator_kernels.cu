@@ -424,23 +424,26 @@ struct TileSample {
 template<bool PERIODIC>
 __device__ __forceinline__ bool tile_sample(float y, float x, float al, const Tile &T, const OpArgs &a, TileSample &S)
 {
-    // y in [0, ny-1): trunc(y) is in [0, ny-2], so locate's clamp does nothing.
+    // y in [0, ny-1): trunc(y) is in [0, ny-2], so locate's clamp does nothing.  The truncations of
+    // non-negative coordinates go through floor_nonneg (no conversion instructions; the same values).
     bool fast = (y >= 0.0f) && (y < (float) (a.ny - 1));
-    const int iy0 = __float2int_rz(y);
-    S.dy = y - (float) iy0;
+    float fy;
+    const int iy0 = floor_nonneg(y, &fy);
+    S.dy = y - fy;
     int ix0;
+    float fx;
     if constexpr (PERIODIC) {
         // locate's fold; a folded x in [0, nx) comes only from a valid x and needs no wrap of ix0.
         const float fnx = (float) a.nx;
         float xf = (x >= 0.0f) ? x : (x + fnx);
         xf = (xf <= fnx) ? xf : (xf - fnx);
         fast = fast && (xf >= 0.0f) && (xf < fnx);
-        ix0 = __float2int_rz(xf);
-        S.dx = xf - (float) ix0;
+        ix0 = floor_nonneg(xf, &fx);
+        S.dx = xf - fx;
     } else {
         fast = fast && (x >= 0.0f) && (x < (float) (a.nx - 2));
-        ix0 = __float2int_rz(x);
-        S.dx = x - (float) ix0;
+        ix0 = floor_nonneg(x, &fx);
+        S.dx = x - fx;
     }
     const int ry = iy0 - T.gy0;
     int rx = ix0 - T.gx0;
@@ -772,7 +775,7 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
 // of the one being processed, so a warp keeps BP - 1 lines of memory traffic in flight while it
 // works without holding registers for them.
 
-constexpr int BW = 16;                 // warps per CTA
+constexpr int BW = 12;                 // warps per CTA (2 CTAs per SM: 85 registers a thread)
 constexpr int BNT = BW * 32;
 constexpr int BP = 8;                  // line slots per warp (a power of two)
 constexpr size_t kBandSmem = (size_t) BW * BP * 128 * sizeof(float);
@@ -783,12 +786,6 @@ struct BandState {
     uint32_t key;       // cell | band << 20 of the accumulated lines, or kNoKey
     int R0, x0;         // rows R0, R0 + 1; columns x0 + [0, 96) (unwrapped; mod nx with PERIODIC)
 };
-
-// Bit n of 'm', or 0 outside [0, 32).
-__device__ __forceinline__ bool bit_at(unsigned m, int n)
-{
-    return (n >= 0) && (n < 32) && ((m >> n) & 1u);
-}
 
 // Adds the accumulator into the map (one addition per non-zero pixel and plane, in flush mode FLUSH)
 // and clears it.
@@ -825,51 +822,31 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
     }
 }
 
-// One cache line (lane = sample) on the band path.  Returns false, having added nothing, unless every
-// sample is valid and needs no clamp or x = nx wrap (as tile_sample), has its upper neighbours in row
-// R0, has |2a| <= 1024 and column k = ix0 - x0 (mod nx with PERIODIC) in [0, 94], and unless k moves
-// along the line in one direction by 0 or 1 per sample, stays in one column for at most four
-// consecutive samples, and repeats at least once (so that the line covers at most 32 columns and
-// some lane holds no column total).  'tab' is the warp's 32-entry table.
+// One cache line (lane = sample) on the band path, whose shape the plan has analysed: 'bw' is its band
+// word (gmm_common.cuh), with the fast bit set.  Returns false, having added nothing, if some sample
+// has |2a| > 1024 (those go the general way, through sincosf).  'tab' is the warp's table (bytes
+// 0..63 by column, 64 for a zero lane, 65..80 a sink).
 template<bool RESP, bool PERIODIC>
-__device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint16_t *tab, float y, float x, float al,
-                                          float tv, uint32_t s)
+__device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint8_t *tab, uint64_t bw, float y, float x,
+                                          float al, float tv, uint32_t s)
 {
     const int lane = threadIdx.x & 31;
-    bool ok = (y >= 0.0f) && (y < (float) (a.ny - 1));
-    const int iy0 = __float2int_rz(y);
-    const float dy = y - (float) iy0;
-    int ix0;
-    float dx;
-    if constexpr (PERIODIC) {
-        const float fnx = (float) a.nx;
-        float xf = (x >= 0.0f) ? x : (x + fnx);
-        xf = (xf <= fnx) ? xf : (xf - fnx);
-        ok = ok && (xf >= 0.0f) && (xf < fnx);
-        ix0 = __float2int_rz(xf);
-        dx = xf - (float) ix0;
-    } else {
-        ok = ok && (x >= 0.0f) && (x < (float) (a.nx - 2));
-        ix0 = __float2int_rz(x);
-        dx = x - (float) ix0;
-    }
-    int k = ix0 - B.x0;
-    if constexpr (PERIODIC)
-        k += (k < 0) ? a.nx : 0;
     const float th = 2.0f * al;
-    ok = ok && (iy0 == B.R0) && ((unsigned) k <= 94u) && (fabsf(th) <= 1024.0f);
-    const int dk = k - __shfl_up_sync(kFullMask, k, 1);
-    const unsigned su = __ballot_sync(kFullMask, (lane > 0) && (dk == 0));   // bit i: k[i] == k[i-1]
-    const bool all_ok = __all_sync(kFullMask, ok);
-    const bool inc = __all_sync(kFullMask, (lane == 0) || (dk == 0) || (dk == 1));
-    const bool dec = __all_sync(kFullMask, (lane == 0) || (dk == 0) || (dk == -1));
-    const unsigned r3 = su & (su >> 1);      // runs of three or more samples in one column
-    const unsigned r5 = r3 & (r3 >> 2);      // runs of five or more
-    if (!(all_ok && (inc || dec) && (su != 0u) && (r5 == 0u)))
+    if (!__all_sync(kFullMask, fabsf(th) <= 1024.0f))
         return false;
+    const unsigned su = (unsigned) bw;                   // bit i: sample i in the column of sample i - 1
+    const int kmin = (int) ((bw >> kBandKminShift) & 127u);
+    const int ncol = (int) ((bw >> kBandNcolShift) & 63u);
+    const bool inc = (bw & kBandInc) != 0ull;
+    const bool r3 = (bw & kBandRun3) != 0ull;
+    // dy = y - R0 and xr = x - x0 are exact (integers R0 <= y, x0 <= x; the plan checked both).
+    const float dy = y - (float) B.R0;
+    float fk;
+    const float xr = x - (float) B.x0;
+    const int k = floor_nonneg(xr, &fk);
+    const float dx = xr - fk;   // = x - floor(x), exactly
 
     // Lanes in scan order ("virtual" order): lane order if x increases, reversed if it decreases.
-    const int dir = inc ? 1 : -1;
     float sn, cs;
     sincos_reduced(th, &sn, &cs);
     float ft, fq, fu;
@@ -886,19 +863,21 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint16_
     }
     const float wy0 = 1.0f - dy;
     const float V[6] = {wy0 * ft, wy0 * fq, wy0 * fu, dy * ft, dy * fq, dy * fu};
-    // The previous sample in scan order (lane - dir); unused where it does not exist.
-    const int src = (lane - dir) & 31;
+    // The previous sample in scan order (lane -+ 1); unused where it does not exist.
+    const int src = (lane + (inc ? 31 : 1)) & 31;
     float Vp[6];
 #pragma unroll
     for (int p = 0; p < 6; p++)
         Vp[p] = __shfl_sync(kFullMask, V[p], src);
     const float dxp = __shfl_sync(kFullMask, dx, src);
-    // Same column as the previous / next sample in scan order.
-    const bool sprev = inc ? bit_at(su, lane) : bit_at(su, lane + 1);
-    const bool snext = inc ? bit_at(su, lane + 1) : bit_at(su, lane);
+    // Same column as the previous / next sample in scan order: bits 0 and 1 of su >> lane, swapped
+    // for decreasing x.
+    const unsigned sl = su >> lane;
+    const bool sprev = (inc ? sl : (sl >> 1)) & 1u;
+    const bool snext = (inc ? (sl >> 1) : sl) & 1u;
     const bool last = !snext;   // the last sample of its column holds the column's totals
     float SA[6], SB[6];         // totals of this lane's column (weights 1 - dx) and the next (dx)
-    if (r3 == 0u) {
+    if (!r3) {
         // At most two samples per column: the last one adds the previous one's share.
         const bool lp = last && sprev;
         const float wa = last ? 1.0f - dx : 0.0f, wb = last ? dx : 0.0f;
@@ -916,8 +895,9 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint16_
             SA[p] = fmaf(wap, Vp[p], (1.0f - dx) * V[p]);
             SB[p] = fmaf(wbp, Vp[p], dx * V[p]);
         }
-        const int src2 = (lane - 2 * dir) & 31;
-        const bool sprev2 = sprev && (inc ? bit_at(su, lane - 1) : bit_at(su, lane + 2));
+        const int src2 = (lane + (inc ? 30 : 2)) & 31;
+        const unsigned sp2 = inc ? (lane > 0 ? (su >> (lane - 1)) : 0u) : ((lane < 30) ? (su >> (lane + 2)) : 0u);
+        const bool sprev2 = sprev && (sp2 & 1u);
 #pragma unroll
         for (int p = 0; p < 6; p++) {
             const float a2 = __shfl_sync(kFullMask, SA[p], src2);
@@ -926,25 +906,20 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint16_
             SB[p] = last ? (sprev2 ? SB[p] + b2 : SB[p]) : 0.0f;
         }
     }
-    // Column n (in scan order) of the line is kmin + n.  tab[n] = (lane holding column n's own
-    // totals) | (lane holding column n-1's, whose dx share falls on column n) << 8.
-    const unsigned lm = __ballot_sync(kFullMask, last);
-    const unsigned lt = (1u << lane) - 1u;
-    const int n = __popc(lm & (inc ? lt : ~(lt | (1u << lane))));
-    const int ncol = __popc(lm);
-    uint8_t *tb = reinterpret_cast<uint8_t *>(tab);
+    // Column n (in scan order) of the line is kmin + n.  tab[2n] = the lane holding column n's own
+    // totals, tab[2n + 3] = the same lane (its dx share falls on column n + 1); the other lanes, whose
+    // totals are zero, write their number into tab[64] (any one of them will do).  (& 31: a plan
+    // used with pointing other than its own gives wrong sums, never an access outside the table.)
+    const int n = (k - kmin) & 31;
     __syncwarp();   // the previous line's reads of the table are done
-    if (last) {
-        tb[2 * n] = (uint8_t) lane;
-        tb[2 * (n + 1) + 1] = (uint8_t) lane;
-    }
+    tab[last ? 2 * n : 64] = (uint8_t) lane;
+    tab[last ? 2 * n + 3 : 65 + (lane & 15)] = (uint8_t) lane;
     __syncwarp();
-    const int kmin = (int) __reduce_min_sync(kFullMask, (unsigned) k);
     const int nA = (lane - kmin) & 31;   // this lane's column kmin + nA is congruent to lane mod 32
-    const uint16_t e = tab[nA];
-    const int zl = __ffs(~lm) - 1;       // a lane whose totals are zero
+    const unsigned e = reinterpret_cast<const uint16_t *>(tab)[nA];
+    const int zl = tab[64];              // a lane whose totals are zero
     const int srcA = (nA < ncol) ? (int) (e & 0xffu) : zl;
-    const int srcB = ((nA >= 1) && (nA <= ncol)) ? (int) (e >> 8) : zl;
+    const int srcB = ((unsigned) (nA - 1) < (unsigned) ncol) ? (int) (e >> 8) : zl;
     float C[6];
 #pragma unroll
     for (int p = 0; p < 6; p++)
@@ -955,19 +930,15 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint16_
     if (slo == 0) {
 #pragma unroll
         for (int p = 0; p < 6; p++) {
-            if (hi) B.acc[1][p] += C[p];
-            else B.acc[0][p] += C[p];
+            B.acc[0][p] += hi ? 0.0f : C[p];
+            B.acc[1][p] += hi ? C[p] : 0.0f;
         }
-    } else if (slo == 1) {
+    } else {
 #pragma unroll
         for (int p = 0; p < 6; p++) {
-            if (hi) B.acc[2][p] += C[p];
-            else B.acc[1][p] += C[p];
+            B.acc[1][p] += (slo == 1 && !hi) ? C[p] : 0.0f;
+            B.acc[2][p] += (slo == 1) == hi ? C[p] : 0.0f;
         }
-    } else if (!hi) {
-#pragma unroll
-        for (int p = 0; p < 6; p++)
-            B.acc[2][p] += C[p];
     }
     return true;
 }
@@ -1015,10 +986,10 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template<bool RESP, bool PERIODIC, int FLUSH>
 __global__ void __launch_bounds__(BNT, 2)
 planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner,
-                     const uint32_t *__restrict__ cellmap)
+                     const uint32_t *__restrict__ cellmap, const uint64_t *__restrict__ band)
 {
     extern __shared__ float s_lines[];    // [BW][BP][4 rows][32]: y, x, alpha, TOD
-    __shared__ uint16_t s_tab[BW][32];
+    __shared__ __align__(4) uint8_t s_tab[BW][96];
     __shared__ uint32_t s_err[BW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t nw = (int64_t) gridDim.x * BW;
@@ -1028,7 +999,7 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
     const uint32_t nsamp = (uint32_t) a.nsamp;
     const uint32_t nlines = nsamp >> 5;
     uint32_t err = a.partial ? 0u : check_plan_cells(cellmap, a);
-    uint16_t *tab = s_tab[warp];
+    uint8_t *tab = s_tab[warp];
     float *ring = s_lines + (size_t) warp * BP * 128;
     // This lane's 16-byte piece of every line: row lane/8 (y, x, alpha, TOD), samples 4 (lane%8) + [0, 4).
     const int row = lane >> 3, piece = 4 * (lane & 7);
@@ -1048,9 +1019,10 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
     // Owner words of entries [32 G, 32 G + 64) of this warp's range: lane i holds entry 32 G + i (A)
     // and 32 (G + 1) + i (B), decoded as (line, key); lines >= nlines (a plan that does not belong to
     // this xpointing) are flagged and skipped.
-    auto decode = [&](int64_t g, uint32_t &line, uint32_t &key) {
+    auto decode = [&](int64_t g, uint32_t &line, uint32_t &key, uint64_t &bw) {
         const int64_t q = 32 * g + lane;
         const uint64_t w = (q < n) ? __ldg(owner_mt + e0 + q) : 0ull;
+        bw = (q < n) ? __ldg(band + e0 + q) : 0ull;
         line = (q < n) ? (uint32_t) ((w >> 20) & kClMask) : 0xffffffffu;
         key = (uint32_t) (w & kCellMask) | ((uint32_t) ((w >> kBandShift) & 63u) << 20);
         if ((q < n) && (line >= nlines)) {
@@ -1059,15 +1031,14 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
         }
     };
     uint32_t lineA, keyA, lineB, keyB;
-    decode(0, lineA, keyA);
-    decode(1, lineB, keyB);
+    uint64_t bwA, bwB;
+    decode(0, lineA, keyA, bwA);
+    decode(1, lineB, keyB, bwB);
     int64_t G = 0;
 
     // Entry q's line (0xffffffff: none), for q in groups G and G + 1; warp-uniform.
     auto line_of = [&](int64_t q) -> uint32_t {
-        const uint32_t la = __shfl_sync(kFullMask, lineA, (int) (q & 31));
-        const uint32_t lb = __shfl_sync(kFullMask, lineB, (int) (q & 31));
-        return ((q >> 5) == G) ? la : lb;
+        return __shfl_sync(kFullMask, ((q >> 5) == G) ? lineA : lineB, (int) (q & 31));
     };
     // Starts the copy of entry q's line into its ring slot (always commits one group, maybe empty).
     auto issue = [&](int64_t q) {
@@ -1085,14 +1056,16 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
         if (((q & 31) == 0) && (q > 0)) {
             lineA = lineB;
             keyA = keyB;
+            bwA = bwB;
             G++;
-            decode(G + 1, lineB, keyB);
+            decode(G + 1, lineB, keyB, bwB);
         }
         issue(q + BP - 1);             // into the slot of line q - 1, released at the end of that step
         cp_async_wait<BP - 1>();       // this lane's piece of line q has landed
         __syncwarp();
         const uint32_t line = __shfl_sync(kFullMask, lineA, (int) (q & 31));
         const uint32_t key = __shfl_sync(kFullMask, keyA, (int) (q & 31));
+        const uint64_t bw = __shfl_sync(kFullMask, bwA, (int) (q & 31));
         if (line != 0xffffffffu) {
             const float *slot = ring + (q & (BP - 1)) * 128;
             const float y = slot[lane], x = slot[32 + lane], al = slot[64 + lane], tv = slot[96 + lane];
@@ -1105,7 +1078,7 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
                 B.x0 = (int) (key & 1023u) << 6;
                 run = 0;
             }
-            if (band_line<RESP, PERIODIC>(a, B, tab, y, x, al, tv, s))
+            if ((bw & kBandFast) && band_line<RESP, PERIODIC>(a, B, tab, bw, y, x, al, tv, s))
                 run++;
             else
                 band_general_sample<RESP, PERIODIC, FLUSH>(a, y, x, al, tv, s, err);
@@ -1325,7 +1298,7 @@ cudaError_t launch_planned_periodic(const OpArgs &a, const uint64_t *owner_mt, i
 // (the cp.async line copies); the caller falls back to the tile kernel otherwise.
 template<bool RESP, bool PERIODIC, int FLUSH>
 cudaError_t launch_tod2map_band_impl(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner,
-                                     const uint32_t *cellmap, cudaStream_t stream)
+                                     const uint32_t *cellmap, const uint64_t *band, cudaStream_t stream)
 {
     static std::atomic<uint64_t> attr_done{0};
     cudaError_t e = set_smem_limit(planned_tod2map_band<RESP, PERIODIC, FLUSH>, kBandSmem, attr_done);
@@ -1334,32 +1307,33 @@ cudaError_t launch_tod2map_band_impl(const OpArgs &a, const uint64_t *owner_mt, 
     const int per_sm = (a.ctas_per_sm > 0) ? a.ctas_per_sm : 2;
     int64_t g = (nowner + 32 * BW - 1) / (32 * BW);
     g = std::max<int64_t>(1, std::min<int64_t>(g, (int64_t) per_sm * device_sm_count()));
-    planned_tod2map_band<RESP, PERIODIC, FLUSH><<<(unsigned) g, BNT, kBandSmem, stream>>>(a, owner_mt, nowner, cellmap);
+    planned_tod2map_band<RESP, PERIODIC, FLUSH><<<(unsigned) g, BNT, kBandSmem, stream>>>(a, owner_mt, nowner, cellmap,
+                                                                                         band);
     return cudaGetLastError();
 }
 
 template<bool RESP, int FLUSH>
 cudaError_t launch_tod2map_band(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
-                                cudaStream_t stream)
+                                const uint64_t *band, cudaStream_t stream)
 {
     if (nowner <= 0)
         return cudaSuccess;
-    return a.periodic ? launch_tod2map_band_impl<RESP, true, FLUSH>(a, owner_mt, nowner, cellmap, stream)
-                      : launch_tod2map_band_impl<RESP, false, FLUSH>(a, owner_mt, nowner, cellmap, stream);
+    return a.periodic ? launch_tod2map_band_impl<RESP, true, FLUSH>(a, owner_mt, nowner, cellmap, band, stream)
+                      : launch_tod2map_band_impl<RESP, false, FLUSH>(a, owner_mt, nowner, cellmap, band, stream);
 }
 
 template<bool TOD2MAP, bool RESP>
 cudaError_t launch_planned_dispatch(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
-                                    cudaStream_t stream)
+                                    const uint64_t *band, cudaStream_t stream)
 {
     if constexpr (TOD2MAP) {
         const bool aligned = ((((uintptr_t) a.xp) | ((uintptr_t) a.in)) & 15) == 0;
-        if ((g_tod2map_kernel == GMM_TOD2MAP_BANDS) && aligned) {
+        if ((g_tod2map_kernel == GMM_TOD2MAP_BANDS) && aligned && band) {
             if (a.flush == kFlushCompensated)
-                return launch_tod2map_band<RESP, kFlushCompensated>(a, owner_mt, nowner, cellmap, stream);
+                return launch_tod2map_band<RESP, kFlushCompensated>(a, owner_mt, nowner, cellmap, band, stream);
             if (a.flush == kFlushF64)
-                return launch_tod2map_band<RESP, kFlushF64>(a, owner_mt, nowner, cellmap, stream);
-            return launch_tod2map_band<RESP, kFlushF32>(a, owner_mt, nowner, cellmap, stream);
+                return launch_tod2map_band<RESP, kFlushF64>(a, owner_mt, nowner, cellmap, band, stream);
+            return launch_tod2map_band<RESP, kFlushF32>(a, owner_mt, nowner, cellmap, band, stream);
         }
         if (a.flush == kFlushCompensated)
             return launch_planned_periodic<true, RESP, kFlushCompensated>(a, owner_mt, nowner, cellmap, stream);
@@ -1400,15 +1374,15 @@ cudaError_t launch_unplanned_impl(const OpArgs &a, cudaStream_t stream)
 cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                    cudaStream_t stream)
 {
-    return a.response ? launch_planned_dispatch<false, true>(a, owner_mt, nowner, cellmap, stream)
-                      : launch_planned_dispatch<false, false>(a, owner_mt, nowner, cellmap, stream);
+    return a.response ? launch_planned_dispatch<false, true>(a, owner_mt, nowner, cellmap, nullptr, stream)
+                      : launch_planned_dispatch<false, false>(a, owner_mt, nowner, cellmap, nullptr, stream);
 }
 
 cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
-                                   cudaStream_t stream)
+                                   const uint64_t *band, cudaStream_t stream)
 {
-    return a.response ? launch_planned_dispatch<true, true>(a, owner_mt, nowner, cellmap, stream)
-                      : launch_planned_dispatch<true, false>(a, owner_mt, nowner, cellmap, stream);
+    return a.response ? launch_planned_dispatch<true, true>(a, owner_mt, nowner, cellmap, band, stream)
+                      : launch_planned_dispatch<true, false>(a, owner_mt, nowner, cellmap, band, stream);
 }
 
 template<bool PERIODIC>

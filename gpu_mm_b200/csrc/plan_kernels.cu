@@ -197,7 +197,7 @@ preplan_finalize_kernel(uint32_t *__restrict__ nmt, uint32_t *__restrict__ err, 
 __global__ void __launch_bounds__(kPlanWarps * 32, 4)
 plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
                  const uint32_t *__restrict__ nmt_cumsum, uint64_t *__restrict__ mt_out,
-                 uint64_t *__restrict__ owner_out, uint32_t *__restrict__ errflags)
+                 uint64_t *__restrict__ owner_out, uint64_t *__restrict__ band_out, uint32_t *__restrict__ errflags)
 {
     __shared__ int s_cnt[kRoundLines];
     __shared__ int s_off[kRoundLines];
@@ -323,8 +323,12 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
             minc = __reduce_min_sync(kFullMask, minc);
             // Row band: the first sample's row within the owner cell's tile rows, clamped to [0, 63].
             const int band = min(max(s_brow[li] - (int) ((minc >> 10) << 6), 0), 63);
-            if (lane == 0)
+            const uint64_t bw = band_line_word(y[j], x[j], (int) ((minc >> 10) << 6) + band, (int) ((minc & 1023u) << 6),
+                                               ny, periodic ? (float) nx : (float) (nx - 2));
+            if (lane == 0) {
                 owner_out[l] = (uint64_t) minc | hi | ((uint64_t) band << kBandShift);
+                band_out[l] = bw;
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0)
@@ -879,10 +883,30 @@ cudaError_t launch_preplan(const float *xp, int64_t nsamp, int ny, int nx, bool 
 
 cudaError_t launch_plan_emit(const float *xp, int64_t nsamp, int ny, int nx, bool periodic, int64_t nclpb,
                              int nblocks, const uint32_t *nmt_cumsum, uint64_t *mt_out, uint64_t *owner_out,
-                             uint32_t *errflags, cudaStream_t stream)
+                             uint64_t *band_out, uint32_t *errflags, cudaStream_t stream)
 {
     plan_emit_kernel<<<nblocks, kPlanWarps * 32, 0, stream>>>(xp, nsamp, ny, nx, periodic, nclpb, nmt_cumsum,
-                                                               mt_out, owner_out, errflags);
+                                                               mt_out, owner_out, band_out, errflags);
+    return cudaGetLastError();
+}
+
+// Band words into owner-list order: band_out[q] = band_by_line[line of owner[q]].
+__global__ void __launch_bounds__(256)
+band_gather_kernel(const uint64_t *__restrict__ owner, int64_t n, const uint64_t *__restrict__ band_by_line,
+                   uint64_t *__restrict__ band_out)
+{
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t q = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; q < n; q += stride)
+        band_out[q] = band_by_line[(owner[q] >> 20) & kClMask];
+}
+
+cudaError_t launch_band_gather(const uint64_t *owner, int64_t n, const uint64_t *band_by_line, uint64_t *band_out,
+                               cudaStream_t stream)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 8 * (int64_t) device_sm_count()));
+    band_gather_kernel<<<(unsigned) g, 256, 0, stream>>>(owner, n, band_by_line, band_out);
     return cudaGetLastError();
 }
 

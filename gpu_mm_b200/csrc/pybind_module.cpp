@@ -293,7 +293,10 @@ PYBIND11_MODULE(gpu_mm_pybind11, m)
         .def("get_plan_mt", [](const PointingPlan &p) { return host_to_numpy(p.get_plan_mt(false)); },
              "Length nmt_cumsum[-1] array, sorted by (map cell, cache line)")
         .def("_get_owner_mt", [](const PointingPlan &p) { return host_to_numpy(p.get_owner_mt(false)); },
-             "One word per cache line (cell | line << 20), sorted by the line's lowest cell")
+             "One word per cache line (cell | line << 20 | mflag << 46 | row band << 48), sorted by "
+             "(the line's lowest cell, row band, line)")
+        .def("_get_band_words", [](const PointingPlan &p) { return host_to_numpy(p.get_band_words(false)); },
+             "One word per owner entry: the line's shape for the tod2map band path (0: not on that path)")
         .def("__str__", &PointingPlan::str);
 
     // Test utilities (gpu_mm_pybind11.cu:228-262).  ToyPointing fills caller-allocated arrays.

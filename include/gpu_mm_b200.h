@@ -76,13 +76,15 @@ typedef struct gmm_preplan_info {
 } gmm_preplan_info;
 
 /* Byte offsets of the arrays inside a plan buffer (the reference's 'buf' holds plan_mt and err,
- * PointingPlan.cu:251-260; this layout appends the owner-line list). */
+ * PointingPlan.cu:251-260; this layout appends the owner-line list, the cell bitmap and the band
+ * words of the tod2map band path). */
 typedef struct gmm_plan_layout {
     int64_t mt_offset;        /* uint64 plan_mt[plan_nmt], sorted by (cell, cache line) */
     int64_t err_offset;       /* uint32 err[max(planner_nblocks, pointing_nblocks)] */
     int64_t owner_offset;     /* uint64 owner_mt[nsamp/32]: one word per cache line, sorted */
     int64_t cellmap_offset;   /* uint32 cellmap[2^20/32]: bit c set iff cell c occurs in plan_mt */
     int64_t total_nbytes;
+    int64_t band_offset;      /* uint64 band[nsamp/32]: per owner entry, the line's shape for tod2map */
 } gmm_plan_layout;
 
 /* Thread-local message of the last failing call on this thread ("" if none). */

@@ -136,6 +136,7 @@ struct PointingPlan
     ulong *plan_mt = nullptr;
     uint *err_gpu = nullptr;
     ulong *owner_mt = nullptr;   // one word per cache line, sorted by owner cell
+    ulong *band_words = nullptr; // one word per owner entry: the line's shape for the tod2map band path
 
     template<typename T>
     PointingPlan(const PointingPrePlan &pp, const Array<T> &xpointing_gpu,
@@ -147,6 +148,7 @@ struct PointingPlan
 
     Array<ulong> get_plan_mt(bool gpu) const;
     Array<ulong> get_owner_mt(bool gpu) const;
+    Array<ulong> get_band_words(bool gpu) const;
     void _check_errflags(const std::string &where) const;
     std::string str() const;
 };

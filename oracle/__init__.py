@@ -418,6 +418,50 @@ def owner_words(xpointing, nypix_global, mt, owner_bits):
     return words[order]
 
 
+def band_words(xpointing, nypix_global, nxpix_global, periodic_xcoord, owner):
+    """Band words of a single-TOD plan, one per entry of its owner list 'owner' (as owner_words()
+    gives it), as the plan builder must produce them (this implementation's own addition to the plan;
+    no reference counterpart).  Bits: 0-31 same column as the previous sample; 32-38 first column in
+    scan order, relative to the owner cell's x0; 39-44 number of columns; 45 x increases; 46 the line
+    takes the tod2map band path; 47 some column holds three or four consecutive samples.  Zero for
+    lines off that path."""
+    xp = np.ascontiguousarray(xpointing, dtype=np.float32)
+    n = _nsamp(xp)
+    owner = np.asarray(owner, dtype=np.uint64)
+    lines = ((owner >> np.uint64(20)) & np.uint64((1 << 26) - 1)).astype(np.int64)
+    cell = (owner & np.uint64(0xFFFFF)).astype(np.int64)
+    band = ((owner >> np.uint64(48)) & np.uint64(63)).astype(np.int64)
+    R0 = (cell >> 10) * 64 + band
+    x0 = (cell & 1023) * 64
+    idx = 32 * lines[:, None] + np.arange(32)[None, :]
+    y = xp.reshape(3, n)[0][idx]
+    x = xp.reshape(3, n)[1][idx]
+    dy = (y - R0[:, None].astype(np.float32)).astype(np.float32)
+    xr = (x - x0[:, None].astype(np.float32)).astype(np.float32)
+    x_hi = np.float32(nxpix_global if periodic_xcoord else nxpix_global - 2)
+    # Range checks on the float bit patterns as unsigned integers, as the builder does: negative
+    # values (-0.0 included) and NaN fail.
+    bits = lambda v: np.ascontiguousarray(v, dtype=np.float32).view(np.uint32)
+    ok = ((R0[:, None] <= nypix_global - 2) & (bits(dy) < bits(np.float32(1.0))) & (bits(xr) < bits(np.float32(95.0)))
+          & (bits(x) < bits(x_hi)))
+    k = np.floor(np.where(ok, xr, np.float32(0))).astype(np.int64)
+    dk = np.diff(k, axis=1)
+    bit = np.uint64(1) << np.arange(1, 32, dtype=np.uint64)
+    su = ((dk == 0) * bit).sum(axis=1, dtype=np.uint64)
+    up = ((dk == 1) * bit).sum(axis=1, dtype=np.uint64)
+    down = ((dk == -1) * bit).sum(axis=1, dtype=np.uint64)
+    r3 = su & (su >> np.uint64(1))
+    fast = (ok.all(axis=1) & ((su | up | down) == np.uint64(0xFFFFFFFE)) & ~((up != 0) & (down != 0)) & (su != 0)
+            & ((r3 & (r3 >> np.uint64(2))) == 0))
+    inc = down == 0
+    kmin = np.where(inc, k[:, 0], k[:, 31])
+    ncol = np.where(inc, k[:, 31], k[:, 0]) - kmin + 1
+    w = (su | (kmin.astype(np.uint64) << np.uint64(32)) | (ncol.astype(np.uint64) << np.uint64(39))
+         | (inc.astype(np.uint64) << np.uint64(45)) | (np.uint64(1) << np.uint64(46))
+         | ((r3 != 0).astype(np.uint64) << np.uint64(47)))
+    return np.where(fast, w, np.uint64(0))
+
+
 def sample_slots(xpointing, nypix_global, nxpix_global, periodic_xcoord=True):
     xp = np.ascontiguousarray(xpointing, dtype=np.float32)
     n = _nsamp(xp)

@@ -26,7 +26,7 @@ class PreplanInfo(ctypes.Structure):
 
 class PlanLayout(ctypes.Structure):
     _fields_ = [("mt_offset", ctypes.c_int64), ("err_offset", ctypes.c_int64), ("owner_offset", ctypes.c_int64),
-                ("cellmap_offset", ctypes.c_int64), ("total_nbytes", ctypes.c_int64)]
+                ("cellmap_offset", ctypes.c_int64), ("total_nbytes", ctypes.c_int64), ("band_offset", ctypes.c_int64)]
 
 
 @pytest.fixture(scope="module")
@@ -82,7 +82,8 @@ def test_preplan_info_matches_reference_geometry(lib, nsamp_lines, nmt):
     assert lay.total_nbytes == info.plan_nbytes
     assert lay.err_offset >= 8 * nmt and lay.err_offset % 128 == 0 and lay.owner_offset % 128 == 0
     assert lay.cellmap_offset >= lay.owner_offset + 8 * nsamp_lines and lay.cellmap_offset % 128 == 0
-    assert lay.total_nbytes - lay.cellmap_offset == (1 << 20) // 8
+    assert lay.band_offset - lay.cellmap_offset == (1 << 20) // 8 and lay.band_offset % 128 == 0
+    assert lay.total_nbytes >= lay.band_offset + 8 * nsamp_lines
 
 
 def test_preplan_geometry_matches_oracle(lib):

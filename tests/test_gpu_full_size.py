@@ -88,7 +88,11 @@ def test_plan_equals_oracle_and_reference(workload, host_inputs):
     assert err == 0
     mt = plan.get_plan_mt()
     np.testing.assert_array_equal(mt, mt_ref)
-    np.testing.assert_array_equal(plan._get_owner_mt(), oracle.owner_words(xs, NY, mt_ref, owner_bits))
+    owner = oracle.owner_words(xs, NY, mt_ref, owner_bits)
+    np.testing.assert_array_equal(plan._get_owner_mt(), owner)
+    bw = plan._get_band_words()
+    np.testing.assert_array_equal(bw, oracle.band_words(xs, NY, NX, True, owner))
+    assert np.mean(bw != 0) > 0.99        # the raster's lines take the band path
     if oracle.refgpu_available():
         rp = oracle.RefGpuPlan(xp, NY, NX, True)
         assert rp.plan_nmt == pp.plan_nmt

@@ -51,7 +51,9 @@ def check_plan(g, xp, ny, nx, periodic, pp, plan):
     assert err == 0
     mt = plan.get_plan_mt()
     np.testing.assert_array_equal(mt, mt_ref)   # all 64 bits, canonical order
-    np.testing.assert_array_equal(plan._get_owner_mt(), oracle.owner_words(xp, ny, mt_ref, owner_ref))
+    owner = oracle.owner_words(xp, ny, mt_ref, owner_ref)
+    np.testing.assert_array_equal(plan._get_owner_mt(), owner)
+    np.testing.assert_array_equal(plan._get_band_words(), oracle.band_words(xp, ny, nx, periodic, owner))
 
 
 def lpix_from(g, ny, nx, offs, ys, ps, periodic):
