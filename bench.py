@@ -229,8 +229,57 @@ def run_reference_arm(args):
                          "sample": f"{ndet} detectors ({nsamp} samples) per step, map2tod + tod2map, "
                                    f"{nthreads} threads"},
         "e2e": {"value": round(value, 4), "unit": "Gsamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": reference_gpu_times(args.ndet_rows, lp),
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_times(ndet_rows, lp):
+    """The reference's own plan builder and GPU operators (its src_lib sources compiled unchanged for
+    sm_100a in oracle/_ref) on the same workload and GPU, timed with CUDA events around each call of
+    its C++ API (which waits for its error-flag readback, as the reference always does).  None where
+    that comparator was not built or there is no GPU."""
+    import torch
+    import oracle
+    if not (oracle.refgpu_available() and torch.cuda.is_available()):
+        return None
+    synthetic = _synthetic()
+    xp = synthetic.raster_xpointing(ndet_rows, 32, 2 ** 18, 2.0, 0.7, 32768, 100.0, 2.0e-4, device="cuda")
+    nsamp = xp.numel() // 3
+    offs_gpu = torch.from_numpy(lp.cell_offsets).cuda()
+    gen = torch.Generator(device="cuda").manual_seed(1234)
+    m = torch.randn(3 * lp.npix, generator=gen, device="cuda")
+    tod_in = torch.randn(nsamp, generator=gen, device="cuda")
+    tod_out = torch.empty(nsamp, device="cuda")
+    map_out = torch.zeros(3 * lp.npix, device="cuda")
+    errflags = torch.zeros(2048, dtype=torch.int32, device="cuda")
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    plans = []
+    out = {"plan_build_ms": round(timed(lambda: plans.append(oracle.RefGpuPlan(xp, 8192, 32768, True))), 4)}
+    plan = plans[-1]
+    del plans[:-1]
+    out["planned_map2tod_ms"] = round(timed(lambda: plan.map2tod(tod_out, m, xp, lp, offs_gpu)), 4)
+    out["planned_tod2map_ms"] = round(timed(lambda: plan.tod2map(map_out, tod_in, xp, lp, offs_gpu)), 4)
+    out["unplanned_map2tod_ms"] = round(timed(lambda: oracle.refgpu_unplanned_map2tod(tod_out, m, xp, lp, offs_gpu, errflags)), 4)
+    out["unplanned_tod2map_ms"] = round(timed(lambda: oracle.refgpu_unplanned_tod2map(map_out, tod_in, xp, lp, offs_gpu, errflags)), 4)
+    step = out["planned_map2tod_ms"] + out["planned_tod2map_ms"]
+    out["step_ms"] = round(step, 4)
+    out["value"] = round(nsamp / (step * 1e-3) / 1e9, 3)
+    out["unit"] = "Gsamples/s (planned map2tod + tod2map, plan reused)"
+    out["plan_nmt"] = plan.plan_nmt
+    out["build"] = "reference src_lib compiled unchanged for sm_100a against oracle/ksgpu_shim (oracle/Makefile)"
+    return out
 
 
 def precision_study(max_run_lines=32):

@@ -795,29 +795,57 @@ template<bool PERIODIC, int FLUSH>
 __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
 {
     const int lane = threadIdx.x & 31;
+    if constexpr (FLUSH == kFlushCompensated) {
+        // The returning atomics of all eighteen values are issued before any two-sum uses one, so
+        // that their round trips overlap (one after the other they would cost eighteen latencies).
+        int64_t off[18];
+        float old[18];
 #pragma unroll
-    for (int sl = 0; sl < 3; sl++) {
-        int gx = B.x0 + 32 * sl + lane;
-        bool xin = true;
-        if constexpr (PERIODIC)
-            gx %= a.nx;
-        else
-            xin = gx < a.nx;
+        for (int i = 0; i < 18; i++) {
+            const int sl = i / 6, r = (i % 6) / 3, p = i % 3;
+            int gx = B.x0 + 32 * sl + lane;
+            bool xin = true;
+            if constexpr (PERIODIC)
+                gx %= a.nx;
+            else
+                xin = gx < a.nx;
+            const float v = B.acc[sl][3 * r + p];
+            const int64_t o = (xin && (v != 0.0f)) ? global_pixel_offset(B.R0 + r, gx, a) : -1;
+            off[i] = (o >= 0) ? (o + p * a.polstride) : -1;
+            old[i] = (off[i] >= 0) ? atomicAdd(a.out + off[i], v) : 0.0f;
+        }
 #pragma unroll
-        for (int r = 0; r < 2; r++) {
-            const float t = B.acc[sl][3 * r], q = B.acc[sl][3 * r + 1], u = B.acc[sl][3 * r + 2];
-            const bool nz = (t != 0.0f) || (q != 0.0f) || (u != 0.0f);
-            if (__any_sync(kFullMask, nz) && nz && xin) {
-                const int64_t off = global_pixel_offset(B.R0 + r, gx, a);
-                if (off >= 0) {
-                    if (t != 0.0f) global_add<FLUSH>(a, off, t);
-                    if (q != 0.0f) global_add<FLUSH>(a, off + a.polstride, q);
-                    if (u != 0.0f) global_add<FLUSH>(a, off + 2 * a.polstride, u);
+        for (int i = 0; i < 18; i++) {
+            const int sl = i / 6, r = (i % 6) / 3, p = i % 3;
+            if (off[i] >= 0)
+                add_rounding_error(a, off[i], old[i], B.acc[sl][3 * r + p]);
+            B.acc[sl][3 * r + p] = 0.0f;
+        }
+    } else {
+#pragma unroll
+        for (int sl = 0; sl < 3; sl++) {
+            int gx = B.x0 + 32 * sl + lane;
+            bool xin = true;
+            if constexpr (PERIODIC)
+                gx %= a.nx;
+            else
+                xin = gx < a.nx;
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const float t = B.acc[sl][3 * r], q = B.acc[sl][3 * r + 1], u = B.acc[sl][3 * r + 2];
+                const bool nz = (t != 0.0f) || (q != 0.0f) || (u != 0.0f);
+                if (__any_sync(kFullMask, nz) && nz && xin) {
+                    const int64_t off = global_pixel_offset(B.R0 + r, gx, a);
+                    if (off >= 0) {
+                        if (t != 0.0f) global_add<FLUSH>(a, off, t);
+                        if (q != 0.0f) global_add<FLUSH>(a, off + a.polstride, q);
+                        if (u != 0.0f) global_add<FLUSH>(a, off + 2 * a.polstride, u);
+                    }
                 }
+                B.acc[sl][3 * r] = 0.0f;
+                B.acc[sl][3 * r + 1] = 0.0f;
+                B.acc[sl][3 * r + 2] = 0.0f;
             }
-            B.acc[sl][3 * r] = 0.0f;
-            B.acc[sl][3 * r + 1] = 0.0f;
-            B.acc[sl][3 * r + 2] = 0.0f;
         }
     }
 }
@@ -966,11 +994,34 @@ __device__ __forceinline__ void band_general_sample(const OpArgs &a, float y, fl
         u = tv * sn;
     }
     const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
-    uint32_t unused = 0;
-    global_accum<FLUSH>(a, a.out, L.iy0, L.ix0, t, q, u, wy0 * wx0, unused);
-    global_accum<FLUSH>(a, a.out, L.iy0, L.ix1, t, q, u, wy0 * L.dx, unused);
-    global_accum<FLUSH>(a, a.out, L.iy1, L.ix0, t, q, u, L.dy * wx0, unused);
-    global_accum<FLUSH>(a, a.out, L.iy1, L.ix1, t, q, u, L.dy * L.dx, unused);
+    if constexpr (FLUSH == kFlushCompensated) {
+        // All twelve returning atomics first, then the two-sums (their round trips overlap).
+        const float w[4] = {wy0 * wx0, wy0 * L.dx, L.dy * wx0, L.dy * L.dx};
+        const int iy[4] = {L.iy0, L.iy0, L.iy1, L.iy1}, ix[4] = {L.ix0, L.ix1, L.ix0, L.ix1};
+        const float f[3] = {t, q, u};
+        int64_t off[12];
+        float v[12], old[12];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int64_t o = global_pixel_offset(iy[c], ix[c], a);
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                off[3 * c + p] = (o >= 0) ? (o + p * a.polstride) : -1;
+                v[3 * c + p] = w[c] * f[p];
+                old[3 * c + p] = (o >= 0) ? atomicAdd(a.out + off[3 * c + p], v[3 * c + p]) : 0.0f;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 12; i++)
+            if (off[i] >= 0)
+                add_rounding_error(a, off[i], old[i], v[i]);
+    } else {
+        uint32_t unused = 0;
+        global_accum<FLUSH>(a, a.out, L.iy0, L.ix0, t, q, u, wy0 * wx0, unused);
+        global_accum<FLUSH>(a, a.out, L.iy0, L.ix1, t, q, u, wy0 * L.dx, unused);
+        global_accum<FLUSH>(a, a.out, L.iy1, L.ix0, t, q, u, L.dy * wx0, unused);
+        global_accum<FLUSH>(a, a.out, L.iy1, L.ix1, t, q, u, L.dy * L.dx, unused);
+    }
 }
 
 // cp.async of 16 bytes, global -> shared (L2 only), and its group bookkeeping.
