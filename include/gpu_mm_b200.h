@@ -149,8 +149,7 @@ int gmm_plan_build(const gmm_preplan_info *info, const uint32_t *nmt_cumsum_gpu,
  *    with GMM_ERR_BUFFER_TOO_SMALL; that covers up to roughly 2^24 samples at typical overheads.
  *  - The array is reserved on every device where this library's module holding it has been loaded
  *    and is kept until the process exits.
- *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress); make
- *    that first call before any stream capture.
+ *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress).
  *  - All calls share the one array.  Calls that overlap on the GPU (other streams, other host
  *    threads) race on it and must be serialised by the caller.  Nothing in the array needs to
  *    start at zero: every call overwrites what it reads.

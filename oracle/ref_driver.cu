@@ -4,9 +4,10 @@
 // from the reference source tree at build time (see oracle/Makefile; nothing is copied into this
 // repository).  That header holds the reference's complete per-sample arithmetic:
 // pixel_locator (gpu_mm_internals.hpp:104-176), cell_enumerator (:179-237), map_evaluator
-// (:243-293) and map_accumulator (:299-355).  The reference's .cu drivers need the ksgpu library,
-// which is not vendored and not installed, so the 15-line sample loops of map2tod_reference.cu:316-331
-// and tod2map_reference.cu:382-393 are restated here around the reference's own templates.
+// (:243-293) and map_accumulator (:299-355).  The 15-line sample loops of map2tod_reference.cu:35-50
+// and tod2map_reference.cu:32-43 are restated here around those templates, so that this library
+// needs nothing but the header (the reference's .cu files themselves, which need ksgpu, are built
+// against a stand-in into libgpu_mm_refgpu.so by refgpu_driver.cu).
 //
 // Outputs go to oracle/_ref/ only.  Used by tests (as the pin of the C restatement in oracle.c)
 // and by bench.py's reference arm (kind "reference": the reference's CPU operator arithmetic).
