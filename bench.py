@@ -350,6 +350,89 @@ def precision_study(max_run_lines=32):
     }
 
 
+def hot_cells_study(max_run_lines=32):
+    """float64 only in the high-hit cells, on a map with cells of very different depth: the high-hit
+    TOD of the precision study (2^28 samples in the 512x512 box [256, 768)^2, ~1000 hits/pixel) and a
+    shallow TOD over the whole 3x1024x1024 map (64 detectors x 2^20 samples, ~64 hits/pixel), both
+    tod = 1e3 + N(0,1), accumulated into one map.  Modes: float atomics; a float64 map; float64 only
+    in the cells touched by at least min_lines cache lines of the two plans (HotCells), folded into
+    the float map once.  Times are CUDA events over both TODs (and the fold), mean of 3 after 1
+    warm-up; errors against the FP64 oracle over the whole map and over the hot and the other cells."""
+    import numpy as np
+    import torch
+    import oracle
+    import gpu_mm_b200 as g
+    from gpu_mm_b200 import synthetic
+    ny = nx = 1024
+    xd = synthetic.config3_xpointing(device="cuda")
+    xw = synthetic.raster_xpointing(8, 8, 2 ** 20, 2.0, 0.7, nx, 0.0, 0.0, xlo=0.0, xspan=nx - 1.0 - 16.0,
+                                    yspan=ny - 1.0 - 16.0, yspeed=0.0123, wrap_x=False, device="cuda")
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    todos = []
+    for xp in (xd, xw):
+        tod = 1e3 + torch.randn(xp.shape[1:], generator=gen, device="cuda")
+        pp = g.PointingPrePlan(xp, ny, nx, periodic_xcoord=False)
+        todos.append((xp, tod, g.PointingPlan(pp, xp)))
+    nsamp = sum(xp.numel() // 3 for xp, _, _ in todos)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, False)
+    n = 3 * lp.npix
+    plans = [p for _, _, p in todos]
+    lines = g.HotCells(lp, plans, 0).lines()
+    min_lines = int(np.sqrt(float(np.median(lines)) * float(lines.max())))   # between the two depths
+    hot = g.HotCells(lp, plans, min_lines)
+    f32 = torch.zeros(n, device="cuda")
+    f64 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    lmap = g.LocalMap(lp, f32)
+
+    def run_hot():
+        for xp, tod, plan in todos:
+            g.tod2map_hot_f64(lmap, hot, tod, xp, plan, max_run_lines=max_run_lines)
+        hot.fold(lmap)
+
+    calls = {
+        "fp32_atomics": lambda: [g.tod2map(lmap, tod, xp, plan) for xp, tod, plan in todos],
+        "fp64_map": lambda: [g.tod2map_f64(f64, lp, tod, xp, plan, max_run_lines=max_run_lines)
+                             for xp, tod, plan in todos],
+        "fp64_hot_cells": run_hot,
+    }
+    want = np.zeros(n, np.float64)
+    nthreads = os.cpu_count() or 1
+    for xp, tod, _ in todos:
+        assert oracle.tod2map_f64w_mt(want, tod.cpu().numpy(), xp.cpu().numpy(),
+                                      oracle.Lpix.rectangle(ny, nx, False), nthreads) == 0
+    hot_mask = np.repeat(np.repeat(hot.slots() >= 0, 64, axis=0), 64, axis=1)
+    w3 = want.reshape(3, ny, nx)
+    scale = np.abs(want).max()
+    results = {}
+    for name, fn in calls.items():
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        f32.zero_()
+        f64.zero_()
+        fn()
+        torch.cuda.synchronize()
+        out = (f64 if name == "fp64_map" else f32).cpu().numpy().astype(np.float64)
+        d = np.abs(out.reshape(3, ny, nx) - w3)
+        results[name] = {"ms": round(ms, 4), "gsamples_s": round(nsamp / (ms * 1e-3) / 1e9, 3),
+                         "max_rel_err": float(f"{d.max() / scale:.3e}"),
+                         "max_rel_err_hot_cells": float(f"{d[:, hot_mask].max() / scale:.3e}"),
+                         "max_rel_err_other_cells": float(f"{d[:, ~hot_mask].max() / scale:.3e}")}
+    return {
+        "workload": "high-hit TOD (2^28 samples, ~1000 hits/pixel in [256, 768)^2) + shallow TOD over the whole "
+                    "3x1024x1024 map (2^26 samples, ~64 hits/pixel), tod = 1e3 + N(0,1), one map",
+        "min_lines": min_lines, "hot_cells": int(hot.nhot), "cells": int(lp.nycells * lp.nxcells),
+        "hot_accumulator_bytes": int(hot.nhot) * 3 * 4096 * 8, "fp64_map_bytes": 8 * n,
+        "max_run_lines": max_run_lines, "modes": results,
+    }
+
+
 def touched_cells(plan_bytes, total_lines):
     """(iycell, ixcell) of the cells set in a batch plan's cell bitmap (after the owner list)."""
     import numpy as np
@@ -846,6 +929,8 @@ def main():
         return r
 
     precision = study("precision", args.no_precision, precision_study)
+    if precision is not None:
+        precision["hot_cells"] = study("hot cells", False, hot_cells_study)
     batched = study("batched", args.no_batch, batch_study)
     served = study("serving", args.no_serve, serving_study)
 

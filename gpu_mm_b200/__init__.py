@@ -22,7 +22,7 @@ except ImportError as _e:   # pragma: no cover - exercised only on unbuilt trees
 from .gpu_mm import *            # noqa: F401,F403
 from .gpu_mm import (map2tod, tod2map, LocalPixelization, LocalMap, DynamicMap, PointingPrePlan,  # noqa: F401
                      PointingPlan, read_xpointing_npzfile, mm_dtype, ToyPointing, PointingPlanTester, tod2map_compensated, fold_compensation,
-                     tod2map_f64)
+                     tod2map_f64, HotCells, tod2map_hot_f64)
 
 from .batch import TodBatch  # noqa: E402,F401
 from . import autotune  # noqa: E402,F401
@@ -31,7 +31,7 @@ from .host_pipeline import HostPipeline  # noqa: E402,F401
 
 __all__ = ["map2tod", "tod2map", "LocalPixelization", "LocalMap", "DynamicMap", "PointingPrePlan",
            "PointingPlan", "read_xpointing_npzfile", "mm_dtype", "gpu_mm_pybind11", "tod2map_compensated",
-           "fold_compensation", "tod2map_f64", "TodBatch", "autotune", "PointingServer"]
+           "fold_compensation", "tod2map_f64", "HotCells", "tod2map_hot_f64", "TodBatch", "autotune", "PointingServer"]
 
 
 def library_path():

@@ -170,6 +170,8 @@ OpArgs make_args(const gmm_lpix *lp, const float *xp, int64_t nsamp, bool partia
     a.comp = nullptr;
     a.out64 = nullptr;
     a.max_run_lines = 0;
+    a.hot_slot = nullptr;
+    a.hot = nullptr;
     a.descs = nullptr;
     a.ntod = 0;
     a.ctas_per_sm = 0;
@@ -413,6 +415,8 @@ struct Precision {
     float *comp = nullptr;
     double *out64 = nullptr;
     int64_t max_run_lines = 0;
+    const int32_t *hot_slot = nullptr;
+    double *hot = nullptr;
 };
 
 static int planned_op(bool tod2map, float *out, const float *in, const float *xp, const float *response, int64_t ndet,
@@ -427,6 +431,12 @@ static int planned_op(bool tod2map, float *out, const float *in, const float *xp
     }
     if (prec.flush == kFlushCompensated) {
         if (int rc = check_ptr(prec.comp, where, "comp")) return rc;
+    }
+    if (prec.flush == kFlushHotF64) {
+        if (int rc = check_ptr(prec.hot, where, "hot")) return rc;
+        if (int rc = check_ptr(prec.hot_slot, where, "hot_slot")) return rc;
+        if (((uintptr_t) in | (uintptr_t) xp) & 15)
+            return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": tod and xpointing must be 16-byte aligned");
     }
     if (prec.max_run_lines < 0)
         return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": max_run_lines must be >= 0");
@@ -458,6 +468,8 @@ static int planned_op(bool tod2map, float *out, const float *in, const float *xp
     a.comp = prec.comp;
     a.out64 = prec.out64;
     a.max_run_lines = prec.max_run_lines;
+    a.hot_slot = prec.hot_slot;
+    a.hot = prec.hot;
     if (response) {
         a.response = response;
         a.ndet = ndet;
@@ -528,6 +540,67 @@ int gmm_planned_tod2map_f64(double *lmap, const float *tod, const float *xp, con
     prec.max_run_lines = max_run_lines;
     return planned_op(true, nullptr, tod, xp, nullptr, 1, lp, info, plan_buf, partial, 0, errword, stream,
                       "tod2map_f64", prec);
+}
+
+int gmm_plan_cell_lines(const gmm_preplan_info *info, const void *plan_buf, const gmm_lpix *lp, uint32_t *lines,
+                        cudaStream_t stream)
+{
+    const char *where = "plan_cell_lines";
+    if (int rc = check_ptr(info, where, "plan")) return rc;
+    if (int rc = check_ptr(plan_buf, where, "plan buffer")) return rc;
+    if (int rc = check_ptr(lines, where, "lines")) return rc;
+    if (int rc = check_lpix(lp, where)) return rc;
+    if (int rc = check_plan_vs_lpix(lp, info, where)) return rc;
+    gmm_plan_layout lay;
+    gmm_plan_layout_get(info, &lay);
+    const uint64_t *mt = (const uint64_t *) ((const char *) plan_buf + lay.mt_offset);
+    cudaError_t e = launch_plan_cell_lines(mt, info->plan_nmt, lp->nycells, lp->nxcells, lines, stream);
+    return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
+}
+
+int gmm_hot_cells(const uint32_t *lines, const gmm_lpix *lp, uint32_t min_lines, int32_t *hot_slot, int32_t *hot_cells,
+                  int32_t *nhot, cudaStream_t stream)
+{
+    const char *where = "hot_cells";
+    if (int rc = check_ptr(lines, where, "lines")) return rc;
+    if (int rc = check_ptr(hot_slot, where, "hot_slot")) return rc;
+    if (int rc = check_ptr(hot_cells, where, "hot_cells")) return rc;
+    if (int rc = check_ptr(nhot, where, "nhot")) return rc;
+    if (int rc = check_lpix(lp, where)) return rc;
+    cudaError_t e = launch_hot_cells(lines, lp->cell_offsets, lp->nycells * lp->nxcells, min_lines, hot_slot, hot_cells,
+                                     nhot, stream);
+    return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
+}
+
+int gmm_planned_tod2map_hot_f64(float *lmap, double *hot, const int32_t *hot_slot, const float *tod, const float *xp,
+                                const gmm_lpix *lp, const gmm_preplan_info *info, const void *plan_buf, int32_t partial,
+                                int64_t max_run_lines, uint32_t *errword, cudaStream_t stream)
+{
+    Precision prec;
+    prec.flush = kFlushHotF64;
+    prec.hot = hot;
+    prec.hot_slot = hot_slot;
+    prec.max_run_lines = max_run_lines;
+    return planned_op(true, lmap, tod, xp, nullptr, 1, lp, info, plan_buf, partial, 0, errword, stream,
+                      "tod2map_hot_f64", prec);
+}
+
+int gmm_fold_hot_f64(float *lmap, double *hot, const int32_t *hot_cells, int64_t nhot, const gmm_lpix *lp,
+                     cudaStream_t stream)
+{
+    const char *where = "fold_hot_f64";
+    if (int rc = check_ptr(lmap, where, "local_map")) return rc;
+    if (nhot < 0)
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": nhot must be >= 0");
+    if (nhot == 0)
+        return 0;
+    if (int rc = check_ptr(hot, where, "hot")) return rc;
+    if (int rc = check_ptr(hot_cells, where, "hot_cells")) return rc;
+    if (int rc = check_lpix(lp, where)) return rc;
+    if (nhot > (int64_t) lp->nycells * lp->nxcells)
+        return fail(GMM_ERR_INVALID_ARGUMENT, std::string(where) + ": nhot exceeds the number of cells");
+    cudaError_t e = launch_fold_hot(lmap, hot, hot_cells, nhot, lp->cell_offsets, lp->ystride, lp->polstride, stream);
+    return (e == cudaSuccess) ? 0 : cuda_fail(e, where);
 }
 
 int gmm_fold_compensation(float *lmap, float *comp, int64_t n, cudaStream_t stream)

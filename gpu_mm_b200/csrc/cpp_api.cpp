@@ -563,6 +563,67 @@ void fold_compensation(Array<float> &local_map, Array<float> &comp)
     cuda_check(cudaStreamSynchronize(0), "fold_compensation");
 }
 
+HotCells::HotCells(const LocalPixelization &lpix, const std::vector<const PointingPlan *> &plans, long min_lines_)
+    : min_lines(min_lines_), nycells(lpix.nycells), nxcells(lpix.nxcells)
+{
+    const char *where = "HotCells";
+    GMM_ASSERT((min_lines >= 0) && (min_lines <= 0xffffffffl), where);
+    const long ncells = nycells * nxcells;
+    lines = Array<uint>::alloc_gpu({nycells, nxcells}, true);
+    slot = Array<int>::alloc_gpu({nycells, nxcells});
+    cells = Array<int>::alloc_gpu({ncells});
+    gmm_lpix v = lpix.device_view();
+    for (const PointingPlan *plan : plans) {
+        GMM_ASSERT(plan != nullptr, where);
+        throw_on_error(gmm_plan_cell_lines(&plan->pp.info, plan->buf.data, &v, lines.data, 0));
+    }
+    Array<int> n = Array<int>::alloc_gpu({1}, true);
+    throw_on_error(gmm_hot_cells(lines.data, &v, (uint32_t) min_lines, slot.data, cells.data, n.data, 0));
+    int h = 0;
+    cuda_check(cudaMemcpy(&h, n.data, sizeof(int), cudaMemcpyDeviceToHost), where);
+    nhot = h;
+    acc = Array<double>::alloc_gpu({nhot, 3, 64, 64}, true);
+}
+
+void HotCells::fold(Array<float> &local_map, const LocalPixelization &lpix)
+{
+    const char *where = "HotCells::fold";
+    check_local_map(local_map, lpix, where, true);
+    GMM_ASSERT((lpix.nycells == nycells) && (lpix.nxcells == nxcells), where);
+    gmm_lpix v = lpix.device_view();
+    throw_on_error(gmm_fold_hot_f64(local_map.data, acc.data, cells.data, nhot, &v, 0));
+    cuda_check(cudaStreamSynchronize(0), where);
+}
+
+Array<uint> HotCells::get_lines() const
+{
+    Array<uint> h = Array<uint>::alloc_host({nycells, nxcells});
+    cuda_check(cudaMemcpy(h.data, lines.data, h.size * sizeof(uint), cudaMemcpyDeviceToHost), "HotCells::get_lines");
+    return h;
+}
+
+Array<int> HotCells::get_slot() const
+{
+    Array<int> h = Array<int>::alloc_host({nycells, nxcells});
+    cuda_check(cudaMemcpy(h.data, slot.data, h.size * sizeof(int), cudaMemcpyDeviceToHost), "HotCells::get_slot");
+    return h;
+}
+
+void launch_planned_tod2map_hot_f64(Array<float> &local_map, HotCells &hot, const Array<float> &tod,
+                                    const Array<float> &xpointing, const LocalPixelization &lpix,
+                                    const PointingPlan &plan, bool partial, long max_run_lines)
+{
+    const char *where = "launch_tod2map_hot_f64";
+    check_tod(tod, plan.nsamp, where, true);
+    check_local_map(local_map, lpix, where, true);
+    check_xpointing(xpointing, plan.nsamp, where, true);
+    check_op<float>(lpix, plan, where);
+    GMM_ASSERT((lpix.nycells == hot.nycells) && (lpix.nxcells == hot.nxcells), where);
+    gmm_lpix v = lpix.device_view();
+    throw_on_error(gmm_planned_tod2map_hot_f64(local_map.data, hot.acc.data, hot.slot.data, tod.data, xpointing.data,
+                                               &v, &plan.pp.info, plan.buf.data, partial, max_run_lines, nullptr, 0));
+}
+
 template<typename T>
 static long check_response(const Array<T> &response, long nsamp, const char *where)
 {

@@ -66,6 +66,10 @@ struct OpArgs {
     float *comp;
     double *out64;
     int64_t max_run_lines;
+    // Flush mode 3 (hot cells): hot_slot[iycell * nxcells + ixcell] >= 0 names the cell's float64
+    // accumulator hot[slot][3][64][64]; partials of other cells go into 'out' as float atomics.
+    const int32_t *hot_slot;
+    double *hot;
     // Batches: per-TOD descriptors (owner words carry the TOD index in bits 48-63); xp, nsamp and
     // the TOD pointer of the OpArgs are then unused.
     const gmm_tod_desc *descs;
@@ -79,6 +83,8 @@ struct OpArgs {
 constexpr int kFlushF32 = 0;
 constexpr int kFlushCompensated = 1;
 constexpr int kFlushF64 = 2;
+constexpr int kFlushHotF64 = 3;
+constexpr int64_t kHotCellDoubles = 3 * 64 * 64;   // one hot cell's accumulator: [3][64][64]
 
 // Raises a kernel's dynamic shared-memory limit, once per device: 'done' holds one bit per device
 // ordinal (ordinals >= 64 set it on every call).
@@ -107,6 +113,12 @@ cudaError_t launch_planned_map2tod(const OpArgs &a, const uint64_t *owner_mt, in
 cudaError_t launch_planned_tod2map(const OpArgs &a, const uint64_t *owner_mt, int64_t nowner, const uint32_t *cellmap,
                                    const uint64_t *band, cudaStream_t stream);
 cudaError_t launch_fold_compensation(float *lmap, float *comp, int64_t n, cudaStream_t stream);
+cudaError_t launch_plan_cell_lines(const uint64_t *mt, int64_t nmt, int nycells, int nxcells, uint32_t *lines,
+                                   cudaStream_t stream);
+cudaError_t launch_hot_cells(const uint32_t *lines, const int64_t *cell_offsets, int ncells, uint32_t min_lines,
+                             int32_t *slot, int32_t *cells, int32_t *nhot, cudaStream_t stream);
+cudaError_t launch_fold_hot(float *lmap, double *hot, const int32_t *cells, int64_t nhot, const int64_t *cell_offsets,
+                            int64_t ystride, int64_t polstride, cudaStream_t stream);
 // Batches of TODs.
 constexpr int kBatchTodShift = 48;
 cudaError_t launch_batch_owner(const gmm_tod_desc *descs, int ntod, int64_t total_lines, int ny, int nx, bool periodic,

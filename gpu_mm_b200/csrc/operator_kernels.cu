@@ -172,6 +172,32 @@ __device__ __forceinline__ void global_add(const OpArgs &a, int64_t off, float v
     }
 }
 
+// Flush mode kFlushHotF64: adds (t, q, u) at pixel (iy, ix) (inside the map) into the float64
+// accumulator of the pixel's cell if the cell has a hot slot, else into the float map with float
+// atomics (nothing for an absent cell).  Zeros are skipped.
+__device__ __forceinline__ void hot_add3(const OpArgs &a, int iy, int ix, float t, float q, float u)
+{
+    const int iyc = iy >> 6, ixc = ix >> 6;
+    if ((iyc >= a.nycells) || (ixc >= a.nxcells))
+        return;
+    const int64_t c = (int64_t) iyc * a.nxcells + ixc;
+    const int slot = __ldg(a.hot_slot + c);
+    if (slot >= 0) {
+        double *h = a.hot + (int64_t) slot * kHotCellDoubles + (iy & 63) * 64 + (ix & 63);
+        if (t != 0.0f) atomicAdd(h, (double) t);
+        if (q != 0.0f) atomicAdd(h + 4096, (double) q);
+        if (u != 0.0f) atomicAdd(h + 8192, (double) u);
+        return;
+    }
+    const int64_t base = __ldg(a.cell_offsets + c);
+    if (base < 0)
+        return;
+    float *m = a.out + base + (int64_t) (iy & 63) * a.ystride + (ix & 63);
+    if (t != 0.0f) atomicAdd(m, t);
+    if (q != 0.0f) atomicAdd(m + a.polstride, q);
+    if (u != 0.0f) atomicAdd(m + 2 * a.polstride, u);
+}
+
 // Adds the tile into the map (one atomic per non-zero pixel and polarisation, in flush mode FLUSH)
 // and clears it.
 template<int FLUSH = kFlushF32>
@@ -835,11 +861,15 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
                 const float t = B.acc[sl][3 * r], q = B.acc[sl][3 * r + 1], u = B.acc[sl][3 * r + 2];
                 const bool nz = (t != 0.0f) || (q != 0.0f) || (u != 0.0f);
                 if (__any_sync(kFullMask, nz) && nz && xin) {
-                    const int64_t off = global_pixel_offset(B.R0 + r, gx, a);
-                    if (off >= 0) {
-                        if (t != 0.0f) global_add<FLUSH>(a, off, t);
-                        if (q != 0.0f) global_add<FLUSH>(a, off + a.polstride, q);
-                        if (u != 0.0f) global_add<FLUSH>(a, off + 2 * a.polstride, u);
+                    if constexpr (FLUSH == kFlushHotF64) {
+                        hot_add3(a, B.R0 + r, gx, t, q, u);
+                    } else {
+                        const int64_t off = global_pixel_offset(B.R0 + r, gx, a);
+                        if (off >= 0) {
+                            if (t != 0.0f) global_add<FLUSH>(a, off, t);
+                            if (q != 0.0f) global_add<FLUSH>(a, off + a.polstride, q);
+                            if (u != 0.0f) global_add<FLUSH>(a, off + 2 * a.polstride, u);
+                        }
                     }
                 }
                 B.acc[sl][3 * r] = 0.0f;
@@ -1015,6 +1045,15 @@ __device__ __forceinline__ void band_general_sample(const OpArgs &a, float y, fl
         for (int i = 0; i < 12; i++)
             if (off[i] >= 0)
                 add_rounding_error(a, off[i], old[i], v[i]);
+    } else if constexpr (FLUSH == kFlushHotF64) {
+        float w = wy0 * wx0;
+        hot_add3(a, L.iy0, L.ix0, w * t, w * q, w * u);
+        w = wy0 * L.dx;
+        hot_add3(a, L.iy0, L.ix1, w * t, w * q, w * u);
+        w = L.dy * wx0;
+        hot_add3(a, L.iy1, L.ix0, w * t, w * q, w * u);
+        w = L.dy * L.dx;
+        hot_add3(a, L.iy1, L.ix1, w * t, w * q, w * u);
     } else {
         uint32_t unused = 0;
         global_accum<FLUSH>(a, a.out, L.iy0, L.ix0, t, q, u, wy0 * wx0, unused);
@@ -1066,6 +1105,9 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
     B.R0 = 0;
     B.x0 = 0;
     int64_t run = 0;   // lines in the accumulator since its last flush (precision modes cap it)
+    // The cap of the current run: max_run_lines in the precision modes (only for hot owner cells in
+    // the hot-cell mode, whose other cells reduce in float as the plain path does); 0: none.
+    int64_t cap = (FLUSH == kFlushF32) ? 0 : a.max_run_lines;
 
     // Owner words of entries [32 G, 32 G + 64) of this warp's range: lane i holds entry 32 G + i (A)
     // and 32 (G + 1) + i (B), decoded as (line, key); lines >= nlines (a plan that does not belong to
@@ -1121,13 +1163,19 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
             const float *slot = ring + (q & (BP - 1)) * 128;
             const float y = slot[lane], x = slot[32 + lane], al = slot[64 + lane], tv = slot[96 + lane];
             const uint32_t s = (line << 5) + (uint32_t) lane;
-            if ((key != B.key) || ((FLUSH != kFlushF32) && (a.max_run_lines > 0) && (run >= a.max_run_lines))) {
+            if ((key != B.key) || ((cap > 0) && (run >= cap))) {
                 if (B.key != kNoKey)
                     band_flush<PERIODIC, FLUSH>(a, B);
                 B.key = key;
                 B.R0 = ((int) ((key >> 10) & 1023u) << 6) + (int) (key >> 20);
                 B.x0 = (int) (key & 1023u) << 6;
                 run = 0;
+                if constexpr (FLUSH == kFlushHotF64) {
+                    const int iyc = (int) ((key >> 10) & 1023u), ixc = (int) (key & 1023u);
+                    const bool hot = (iyc < a.nycells) && (ixc < a.nxcells) &&
+                                     (__ldg(a.hot_slot + (int64_t) iyc * a.nxcells + ixc) >= 0);
+                    cap = hot ? a.max_run_lines : 0;
+                }
             }
             if ((bw & kBandFast) && band_line<RESP, PERIODIC>(a, B, tab, bw, y, x, al, tv, s))
                 run++;
@@ -1379,6 +1427,12 @@ cudaError_t launch_planned_dispatch(const OpArgs &a, const uint64_t *owner_mt, i
 {
     if constexpr (TOD2MAP) {
         const bool aligned = ((((uintptr_t) a.xp) | ((uintptr_t) a.in)) & 15) == 0;
+        if (a.flush == kFlushHotF64) {
+            // Band kernel only, whatever the kernel setting (the C ABI checks the alignment).
+            if (!aligned || !band)
+                return cudaErrorInvalidValue;
+            return launch_tod2map_band<RESP, kFlushHotF64>(a, owner_mt, nowner, cellmap, band, stream);
+        }
         if ((g_tod2map_kernel == GMM_TOD2MAP_BANDS) && aligned && band) {
             if (a.flush == kFlushCompensated)
                 return launch_tod2map_band<RESP, kFlushCompensated>(a, owner_mt, nowner, cellmap, band, stream);
@@ -1468,6 +1522,124 @@ cudaError_t launch_fold_compensation(float *lmap, float *comp, int64_t n, cudaSt
         return cudaSuccess;
     const int64_t g = std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 8 * (int64_t) device_sm_count()));
     fold_compensation_kernel<<<(unsigned) g, 256, 0, stream>>>(lmap, comp, n);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// Hot cells: the cells whose partial sums tod2map reduces in float64 (flush mode kFlushHotF64).
+//
+// plan_cell_lines_kernel adds, for every cell of the local pixelization's grid, the number of plan
+// mt words (= cache lines touching the cell) into lines[iycell * nxcells + ixcell].  The words are
+// sorted by cell, so the lanes of a warp mostly share one cell: one atomic per distinct cell.
+
+__global__ void plan_cell_lines_kernel(const uint64_t *__restrict__ mt, int64_t nmt, int nycells, int nxcells,
+                                       uint32_t *__restrict__ lines)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t i0 = (int64_t) blockIdx.x * blockDim.x; i0 < nmt; i0 += stride) {
+        const int64_t i = i0 + threadIdx.x;
+        int c = -1;
+        if (i < nmt) {
+            const uint64_t w = __ldg(mt + i);
+            const int ixc = (int) (w & 1023u), iyc = (int) ((w >> 10) & 1023u);
+            c = ((iyc < nycells) && (ixc < nxcells)) ? iyc * nxcells + ixc : -1;
+        }
+        const unsigned peers = __match_any_sync(kFullMask, c);
+        if ((c >= 0) && ((peers & ((1u << lane) - 1u)) == 0u))
+            atomicAdd(lines + c, (uint32_t) __popc(peers));
+    }
+}
+
+// One CTA of 1024 threads: slot[c] = rank of cell c among the present cells with lines[c] >=
+// min_lines (in cell order), else -1; cells[slot] = c; *nhot = the number of hot cells.
+__global__ void __launch_bounds__(1024) hot_cells_kernel(const uint32_t *__restrict__ lines,
+                                                         const int64_t *__restrict__ cell_offsets, int ncells,
+                                                         uint32_t min_lines, int32_t *__restrict__ slot,
+                                                         int32_t *__restrict__ cells, int32_t *__restrict__ nhot)
+{
+    __shared__ int s_warp[32];
+    __shared__ int s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0)
+        s_base = 0;
+    __syncthreads();
+    for (int c0 = 0; c0 < ncells; c0 += 1024) {
+        const int c = c0 + threadIdx.x;
+        const bool hot = (c < ncells) && (lines[c] >= min_lines) && (cell_offsets[c] >= 0);
+        const unsigned b = __ballot_sync(kFullMask, hot);
+        if (lane == 0)
+            s_warp[warp] = __popc(b);
+        __syncthreads();
+        if (warp == 0) {
+            const int v = s_warp[lane];
+            int incl = v;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int u = __shfl_up_sync(kFullMask, incl, d);
+                incl += (lane >= d) ? u : 0;
+            }
+            s_warp[lane] = incl - v;   // exclusive prefix over warps
+        }
+        __syncthreads();
+        const int r = s_base + s_warp[warp] + __popc(b & ((1u << lane) - 1u));
+        if (c < ncells) {
+            slot[c] = hot ? r : -1;
+            if (hot)
+                cells[r] = c;
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023)
+            s_base = r + (hot ? 1 : 0);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        *nhot = s_base;
+}
+
+// One CTA per hot cell: local_map = float(local_map + hot) at every non-zero accumulator value (one
+// rounding), then the accumulator is zeroed.
+__global__ void fold_hot_kernel(float *__restrict__ lmap, double *__restrict__ hot, const int32_t *__restrict__ cells,
+                                const int64_t *__restrict__ cell_offsets, int64_t ystride, int64_t polstride)
+{
+    const int64_t base = cell_offsets[cells[blockIdx.x]];
+    if (base < 0)      // the cell left the pixelization after the hot cells were chosen
+        return;
+    double *h = hot + (int64_t) blockIdx.x * kHotCellDoubles;
+    for (int i = threadIdx.x; i < (int) kHotCellDoubles; i += blockDim.x) {
+        const double v = h[i];
+        if (v != 0.0) {
+            const int p = i >> 12, iy = (i >> 6) & 63, ix = i & 63;
+            float *m = lmap + base + p * polstride + iy * ystride + ix;
+            *m = (float) ((double) *m + v);
+            h[i] = 0.0;
+        }
+    }
+}
+
+cudaError_t launch_plan_cell_lines(const uint64_t *mt, int64_t nmt, int nycells, int nxcells, uint32_t *lines,
+                                   cudaStream_t stream)
+{
+    if (nmt <= 0)
+        return cudaSuccess;
+    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((nmt + 255) / 256, 8 * (int64_t) device_sm_count()));
+    plan_cell_lines_kernel<<<(unsigned) g, 256, 0, stream>>>(mt, nmt, nycells, nxcells, lines);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hot_cells(const uint32_t *lines, const int64_t *cell_offsets, int ncells, uint32_t min_lines,
+                             int32_t *slot, int32_t *cells, int32_t *nhot, cudaStream_t stream)
+{
+    hot_cells_kernel<<<1, 1024, 0, stream>>>(lines, cell_offsets, ncells, min_lines, slot, cells, nhot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_hot(float *lmap, double *hot, const int32_t *cells, int64_t nhot, const int64_t *cell_offsets,
+                            int64_t ystride, int64_t polstride, cudaStream_t stream)
+{
+    if (nhot <= 0)
+        return cudaSuccess;
+    fold_hot_kernel<<<(unsigned) nhot, 512, 0, stream>>>(lmap, hot, cells, cell_offsets, ystride, polstride);
     return cudaGetLastError();
 }
 

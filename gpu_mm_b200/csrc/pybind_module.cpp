@@ -379,6 +379,45 @@ PYBIND11_MODULE(gpu_mm_pybind11, m)
           py::arg("local_map"), py::arg("tod"), py::arg("xpointing"), py::arg("local_pixelization"), py::arg("plan"),
           py::arg("partial_pixelization") = false, py::arg("max_run_lines") = 0);
 
+    // float64 only for high-hit cells (no counterpart in the reference).
+    py::class_<HotCells>(m, "HotCells",
+                         "Cells of a LocalPixelization whose tod2map partials are reduced in float64 "
+                         "(planned_tod2map_hot_f64), chosen by the cache lines of the given plans touching them")
+        .def(py::init([](const LocalPixelization &lpix, py::list plans, long min_lines) {
+                 std::vector<const PointingPlan *> v;
+                 for (py::handle h : plans)
+                     v.push_back(&h.cast<const PointingPlan &>());
+                 py::gil_scoped_release rel;
+                 return new HotCells(lpix, v, min_lines);
+             }),
+             py::arg("local_pixelization"), py::arg("plans"), py::arg("min_lines"), py::keep_alive<1, 2>())
+        .def_readonly("min_lines", &HotCells::min_lines, "Cache lines a cell needs to be hot")
+        .def_readonly("nhot", &HotCells::nhot, "Number of hot cells")
+        .def("get_lines", [](const HotCells &h) { return host_to_numpy(h.get_lines()); },
+             "Cache lines of the plans touching each cell (flat, iycell * nxcells + ixcell)")
+        .def("get_slot", [](const HotCells &h) { return host_to_numpy(h.get_slot()); },
+             "Accumulator slot of each cell, -1 if the cell is not hot (flat, iycell * nxcells + ixcell)")
+        .def("fold",
+             [](HotCells &h, py::object local_map, const LocalPixelization &lpix) {
+                 Array<float> m_ = to_array<float>(local_map, "local_map");
+                 py::gil_scoped_release rel;
+                 h.fold(m_, lpix);
+             },
+             py::arg("local_map"), py::arg("local_pixelization"),
+             "Adds the float64 accumulators into the float local map (one rounding per value) and zeroes them");
+
+    m.def("planned_tod2map_hot_f64",
+          [](py::object local_map, HotCells &hot, py::object tod, py::object xpointing, const LocalPixelization &lpix,
+             const PointingPlan &plan, bool partial_pixelization, long max_run_lines) {
+              Array<float> m_ = to_array<float>(local_map, "local_map");
+              Array<float> t = to_array<float>(tod, "tod");
+              Array<float> x = to_array<float>(xpointing, "xpointing");
+              py::gil_scoped_release rel;
+              launch_planned_tod2map_hot_f64(m_, hot, t, x, lpix, plan, partial_pixelization, max_run_lines);
+          },
+          py::arg("local_map"), py::arg("hot"), py::arg("tod"), py::arg("xpointing"), py::arg("local_pixelization"),
+          py::arg("plan"), py::arg("partial_pixelization") = false, py::arg("max_run_lines") = 0);
+
     m.def("fold_compensation",
           [](py::object local_map, py::object comp) {
               Array<float> m_ = to_array<float>(local_map, "local_map");

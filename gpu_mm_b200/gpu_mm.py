@@ -120,16 +120,16 @@ def tod2map(local_map, tod, xpointing, plan, partial_pixelization=False, respons
 ####################################################################################################
 #
 # Precision variants of planned tod2map (no counterpart in the reference).  The samples are
-# processed exactly as by tod2map() (float arithmetic, float partial sums in a shared-memory tile
-# per cell); only the reduction of those partials into the map differs.
+# processed exactly as by tod2map() (float arithmetic, float partial sums per cell and row band, or
+# per cell on the tile kernel); only the reduction of those partials into the map differs.
 
 
 def tod2map_compensated(local_map, comp, tod, xpointing, plan, partial_pixelization=False, max_run_lines=0):
     """tod2map() into a float LocalMap whose float companion 'comp' (same size, zeroed before the
     first call) collects the rounding error of every float addition into the map (two-sum).
     local_map + comp then holds the sum to about twice float precision, across any number of calls;
-    fold_compensation() adds comp into the map.  max_run_lines > 0 reduces each shared-memory tile
-    partial into the map after at most that many 32-sample cache lines."""
+    fold_compensation() adds comp into the map.  max_run_lines > 0 reduces each partial into the map
+    after at most that many 32-sample cache lines."""
     if not isinstance(local_map, LocalMap) or not isinstance(plan, PointingPlan):
         raise RuntimeError("tod2map_compensated(): expected a LocalMap and a PointingPlan")
     gpu_mm_pybind11.planned_tod2map_compensated(local_map.arr, comp, tod, xpointing, local_map.pixelization, plan,
@@ -142,9 +142,68 @@ def fold_compensation(local_map, comp):
     gpu_mm_pybind11.fold_compensation(arr, comp)
 
 
+class HotCells:
+    """The high-hit cells of a LocalPixelization, for tod2map_hot_f64(): a cell is hot if at least
+    'min_lines' 32-sample cache lines of the given plans touch it (counted over all of them).  Each
+    hot cell gets a float64 accumulator (3 x 64 x 64 doubles) on the device, zero at construction;
+    fold() adds the accumulators into a float LocalMap, rounding each value once, and zeroes them.
+    Cells that are not hot take float atomics, as tod2map().  Rebuild it if the pixelization's
+    cell_offsets change."""
+
+    def __init__(self, local_pixelization, plans, min_lines):
+        if not isinstance(local_pixelization, LocalPixelization):
+            raise RuntimeError("HotCells(): expected a LocalPixelization")
+        if isinstance(plans, PointingPlan):
+            plans = [plans]
+        plans = list(plans)
+        if not all(isinstance(p, PointingPlan) for p in plans):
+            raise RuntimeError("HotCells(): 'plans' must be PointingPlans")
+        self.local_pixelization = local_pixelization
+        self._h = gpu_mm_pybind11.HotCells(local_pixelization, plans, int(min_lines))
+
+    @property
+    def nhot(self):
+        return self._h.nhot
+
+    @property
+    def min_lines(self):
+        return self._h.min_lines
+
+    def lines(self):
+        """numpy (nycells, nxcells): cache lines of the plans touching each cell."""
+        lp = self.local_pixelization
+        return self._h.get_lines().reshape(lp.nycells, lp.nxcells)
+
+    def slots(self):
+        """numpy (nycells, nxcells): accumulator slot of each cell (in cell order), -1 if not hot."""
+        lp = self.local_pixelization
+        return self._h.get_slot().reshape(lp.nycells, lp.nxcells)
+
+    def fold(self, local_map):
+        """local_map += accumulators (one rounding per value); the accumulators become zero."""
+        if not isinstance(local_map, LocalMap):
+            raise RuntimeError("HotCells.fold(): expected a LocalMap")
+        if local_map.pixelization is not self.local_pixelization:
+            raise RuntimeError("HotCells.fold(): the LocalMap has another LocalPixelization")
+        self._h.fold(local_map.arr, self.local_pixelization)
+
+
+def tod2map_hot_f64(local_map, hot, tod, xpointing, plan, partial_pixelization=False, max_run_lines=0):
+    """tod2map() into a float LocalMap in which the hot cells of 'hot' (a HotCells of the same
+    LocalPixelization) reduce their partial sums with float64 atomics into their accumulators; call
+    hot.fold(local_map) after the last TOD.  All other arithmetic is float, as in tod2map().  tod
+    and xpointing must be 16-byte aligned."""
+    if not isinstance(local_map, LocalMap) or not isinstance(plan, PointingPlan) or not isinstance(hot, HotCells):
+        raise RuntimeError("tod2map_hot_f64(): expected a LocalMap, a HotCells and a PointingPlan")
+    if local_map.pixelization is not hot.local_pixelization:
+        raise RuntimeError("tod2map_hot_f64(): the LocalMap and the HotCells have different LocalPixelizations")
+    gpu_mm_pybind11.planned_tod2map_hot_f64(local_map.arr, hot._h, tod, xpointing, local_map.pixelization, plan,
+                                            partial_pixelization, int(max_run_lines))
+
+
 def tod2map_f64(map64, local_pixelization, tod, xpointing, plan, partial_pixelization=False, max_run_lines=0):
     """tod2map() into a float64 map (contiguous, 3*npix doubles, laid out by 'local_pixelization'):
-    float tile partials, reduced with double atomics."""
+    float partials, reduced with double atomics."""
     if not isinstance(local_pixelization, LocalPixelization) or not isinstance(plan, PointingPlan):
         raise RuntimeError("tod2map_f64(): expected a LocalPixelization and a PointingPlan")
     gpu_mm_pybind11.planned_tod2map_f64(map64, tod, xpointing, local_pixelization, plan, partial_pixelization,

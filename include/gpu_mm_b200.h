@@ -286,16 +286,16 @@ int gmm_batch_tod2map(const gmm_tod_desc *descs_gpu, int32_t ntod, int64_t total
                       const gmm_batch_tuning *tuning, uint32_t *errword_gpu, cudaStream_t stream);
 
 /* Precision variants of planned tod2map.  No counterpart in the reference, whose tod2map
- * accumulates in float only (tod2map.cu:157-226); its sample arithmetic is unchanged here (float,
- * shared-memory tile partials), only the reduction into the map differs:
+ * accumulates in float only (tod2map.cu:157-226); its sample arithmetic is unchanged here (float
+ * arithmetic and partial sums), only the reduction into the map differs:
  *   _compensated: float map plus a float 'comp' array of the same size (caller-owned, zeroed
  *                 before the first call) that collects the rounding error of every float addition
  *                 into the map (two-sum).  local_map + comp then holds the sum to about twice float
  *                 precision; gmm_fold_compensation adds comp into local_map and zeroes comp.
  *   _f64:         double local map (same cell_offsets / ystride / polstride, in doubles); partials
  *                 are reduced with double atomics.
- * max_run_lines > 0 bounds how many cache lines a tile partial collects before it is reduced into
- * the map (0: once per cell, as the float path). */
+ * max_run_lines > 0 bounds how many cache lines a partial collects before it is reduced into the
+ * map (0: at each change of cell, or of cell and row band on the row-band kernel). */
 int gmm_planned_tod2map_compensated(float *local_map, float *comp, const float *tod, const float *xpointing,
                                     const gmm_lpix *lpix, const gmm_preplan_info *info, const void *plan_buf,
                                     int32_t partial_pixelization, int64_t max_run_lines, uint32_t *errword_gpu,
@@ -304,6 +304,36 @@ int gmm_planned_tod2map_f64(double *local_map, const float *tod, const float *xp
                             const gmm_preplan_info *info, const void *plan_buf, int32_t partial_pixelization,
                             int64_t max_run_lines, uint32_t *errword_gpu, cudaStream_t stream);
 int gmm_fold_compensation(float *local_map, float *comp, int64_t n, cudaStream_t stream);
+
+/* float64 only where the hit count is high.  No counterpart in the reference.  A float map whose
+ * high-hit ("hot") cells have their partial sums reduced with double atomics into a float64
+ * accumulator of their own, [nhot][3][64][64], and rounded into the float map once, by
+ * gmm_fold_hot_f64; every other cell's partials go into the float map with float atomics, as in
+ * gmm_planned_tod2map.
+ *   gmm_plan_cell_lines: adds, per cell of lpix's grid, the number of the plan's cache lines that
+ *       touch the cell (its mt words) into lines[nycells * nxcells] (uint32, caller-zeroed); call it
+ *       for every plan whose TODs will be accumulated.
+ *   gmm_hot_cells: hot_slot[c] = the accumulator slot of cell c = iycell * nxcells + ixcell if the
+ *       cell is present in lpix and lines[c] >= min_lines (slots in cell order), else -1;
+ *       hot_cells[slot] = c; *nhot (device int32) = the number of hot cells.  hot_slot and
+ *       hot_cells hold nycells * nxcells entries.
+ *   gmm_planned_tod2map_hot_f64: planned tod2map in that mode ('hot': nhot * 3 * 4096 doubles,
+ *       zeroed before the first call).  Runs the row-band kernel whatever
+ *       gmm_set_planned_tod2map_kernel chose; tod and xpointing must be 16-byte aligned.
+ *       max_run_lines bounds the partials of lines owned by hot cells, as for the other precision
+ *       variants; the other cells reduce once per (cell, row band), as gmm_planned_tod2map.
+ *   gmm_fold_hot_f64: local_map = float(local_map + hot) over the hot cells, hot = 0.
+ * hot_slot and hot_cells must be rebuilt if lpix's cell_offsets change. */
+int gmm_plan_cell_lines(const gmm_preplan_info *info, const void *plan_buf, const gmm_lpix *lpix, uint32_t *lines_gpu,
+                        cudaStream_t stream);
+int gmm_hot_cells(const uint32_t *lines_gpu, const gmm_lpix *lpix, uint32_t min_lines, int32_t *hot_slot_gpu,
+                  int32_t *hot_cells_gpu, int32_t *nhot_gpu, cudaStream_t stream);
+int gmm_planned_tod2map_hot_f64(float *local_map, double *hot, const int32_t *hot_slot_gpu, const float *tod,
+                                const float *xpointing, const gmm_lpix *lpix, const gmm_preplan_info *info,
+                                const void *plan_buf, int32_t partial_pixelization, int64_t max_run_lines,
+                                uint32_t *errword_gpu, cudaStream_t stream);
+int gmm_fold_hot_f64(float *local_map, double *hot, const int32_t *hot_cells_gpu, int64_t nhot, const gmm_lpix *lpix,
+                     cudaStream_t stream);
 
 /* Replaces launch_response_map2tod<float> / launch_response_tod2map<float> (gpu_mm.hpp:179-202,
  * map2tod_response.cu:205-290, tod2map_response.cu).  response is [2][ndet] (T, P), ndet divides nsamp. */

@@ -186,7 +186,7 @@ void launch_unplanned_tod2map(Array<T> &local_map, const Array<T> &tod, const Ar
 // Precision variants of planned tod2map (no counterpart in the reference; see gpu_mm_b200.h):
 // float map plus a same-size float compensation array collecting the rounding error of every float
 // addition into the map (fold it in with fold_compensation), or a double map.  max_run_lines > 0
-// bounds how many cache lines a shared-memory tile partial collects before it is reduced.
+// bounds how many cache lines a partial collects before it is reduced into the map.
 void launch_planned_tod2map_compensated(Array<float> &local_map, Array<float> &comp, const Array<float> &tod,
                                         const Array<float> &xpointing, const LocalPixelization &local_pixelization,
                                         const PointingPlan &plan, bool partial_pixelization, long max_run_lines = 0);
@@ -194,6 +194,35 @@ void launch_planned_tod2map_f64(Array<double> &local_map, const Array<float> &to
                                 const LocalPixelization &local_pixelization, const PointingPlan &plan,
                                 bool partial_pixelization, long max_run_lines = 0);
 void fold_compensation(Array<float> &local_map, Array<float> &comp);
+
+// float64 only for high-hit cells (no counterpart in the reference; see gpu_mm_b200.h,
+// gmm_hot_cells): the cells of 'local_pixelization' touched by at least 'min_lines' cache lines of
+// 'plans' (summed over the plans) reduce their tod2map partials into float64 accumulators, which
+// fold() rounds into a float map once; the other cells take float atomics, as plain tod2map.
+struct HotCells
+{
+    HotCells(const LocalPixelization &local_pixelization, const std::vector<const PointingPlan *> &plans,
+             long min_lines);
+
+    const long min_lines;
+    long nycells = 0;
+    long nxcells = 0;
+    long nhot = 0;
+    Array<uint> lines;    // (nycells, nxcells) on the GPU: cache lines of the plans touching each cell
+    Array<int> slot;      // (nycells, nxcells) on the GPU: accumulator slot of each cell, -1 if not hot
+    Array<int> cells;     // (nycells * nxcells,) on the GPU: cells[slot] = iycell * nxcells + ixcell
+    Array<double> acc;    // (nhot, 3, 64, 64) on the GPU, zero after construction and after fold()
+
+    // local_map += acc (one rounding per value), then acc = 0.
+    void fold(Array<float> &local_map, const LocalPixelization &local_pixelization);
+    // Host copies of 'lines' and 'slot'.
+    Array<uint> get_lines() const;
+    Array<int> get_slot() const;
+};
+
+void launch_planned_tod2map_hot_f64(Array<float> &local_map, HotCells &hot, const Array<float> &tod,
+                                    const Array<float> &xpointing, const LocalPixelization &local_pixelization,
+                                    const PointingPlan &plan, bool partial_pixelization, long max_run_lines = 0);
 
 // Non-blocking forms used by batched and served callers: the device error bits are OR-ed into
 // '*errword' (device memory, zeroed by the call) and checked later with check_errword(); nothing

@@ -12,7 +12,8 @@ Lines are spread over the cells with a heavy-tailed number of lines per cell (ma
 line, a few with hundreds), so cell runs start and end anywhere relative to the operators' CTA and
 warp slices; line shapes mix constant x, runs of one to four samples per column, both directions,
 and lines that cross a cell boundary.  The tile kernel is also run with the precision modes and a
-small max_run_lines, which splits cell runs further.
+small max_run_lines, which splits cell runs further, and so is the mode that reduces the partials of
+high-hit cells in float64.
 """
 
 import ctypes
@@ -130,3 +131,16 @@ def test_each_line_exactly_once(g, kernel_knob, seed, nlines):
         g.tod2map_f64(m64, lp, ones, xg, plan, max_run_lines=mrl)
         got = m64.cpu().numpy().reshape(3, ny, nx)
         np.testing.assert_array_equal(got[0], want, err_msg=f"float64 map, max_run_lines {mrl}")
+
+    # float64 only in the cells touched by at least the median number of lines (the rest take float
+    # atomics).
+    lines = g.HotCells(lp, [plan], 0).lines()
+    hot = g.HotCells(lp, [plan], max(1, int(np.median(lines[lines > 0]))))
+    assert 0 < hot.nhot < lp.nycells * lp.nxcells
+    for mrl in (0, 1, 3):
+        out = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+        g.tod2map_hot_f64(out, hot, ones, xg, plan, max_run_lines=mrl)
+        hot.fold(out)
+        got = out.arr.cpu().numpy().reshape(3, ny, nx)
+        np.testing.assert_array_equal(got[0], want, err_msg=f"hot cells, max_run_lines {mrl}")
+        np.testing.assert_array_equal(got[1], want, err_msg=f"hot cells Q, max_run_lines {mrl}")
