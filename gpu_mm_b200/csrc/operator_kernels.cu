@@ -485,11 +485,11 @@ __device__ __forceinline__ bool tile_sample(float y, float x, float al, const Ti
     return fast;
 }
 
-// Not-in-pixelization check of the plan's cells (this CTA's share of the bitmap).
+// Not-in-pixelization check of the plan's cells (this CTA's share of the bitmap; any block size).
 __device__ uint32_t check_plan_cells(const uint32_t *__restrict__ cellmap, const OpArgs &a)
 {
     uint32_t err = 0;
-    for (int w = blockIdx.x * NT + threadIdx.x; w < kCellmapWords; w += gridDim.x * NT) {
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < kCellmapWords; w += gridDim.x * blockDim.x) {
         uint32_t bits = __ldg(cellmap + w);
         while (bits) {
             const int b = __ffs(bits) - 1;
@@ -781,19 +781,20 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
 }
 
 // ------------------------------------------------------------------------------------------------
-// Planned tod2map by row bands (single-TOD plans, float flush).
+// Planned tod2map by row bands (single-TOD plans; every flush mode).
 //
 // The owner list of a single-TOD plan is sorted by (cell, row band, line); the band is the row of a
 // line's first sample within its owner cell.  Each warp walks a contiguous range of the list.  While
-// the (cell, band) stays the same, it accumulates in registers: rows R0 = 64 iycell + band and R0 + 1,
-// columns x0 .. x0 + 95 (x0 = 64 ixcell, unwrapped), planes T, Q, U; lane L holds the columns
-// congruent to L mod 32 (three slots of six values).  A line whose samples all lie in those rows and
-// move by at most one column per sample in one direction (a raster scan slower than 1 px/sample,
-// except at its turnarounds) is added with shuffles instead of atomics: each sample's contribution
-// is split between its two columns, the samples of one column are summed at the last lane of their
-// run, and every lane pulls the totals of the column it holds.  When the (cell, band) changes, or
-// after max_run_lines lines (precision modes), the accumulator goes into the map with one L2
-// reduction per pixel and plane (zeros skipped), in flush mode FLUSH.  Other lines go sample by
+// the (cell, band) stays the same, it accumulates into a per-warp array in shared memory: rows
+// R0 = 64 iycell + band and R0 + 1, columns x0 .. x0 + 95 (x0 = 64 ixcell, unwrapped), planes T, Q,
+// U.  A line whose samples all lie in those rows and move by at most one column per sample in one
+// direction (a raster scan slower than 1 px/sample, except at its turnarounds; the plan's band word
+// says so) is added without atomics: each sample's contribution is split between its two columns,
+// the samples of one column are summed by shuffles at the last lane of their run, and those lanes,
+// one per column, add their totals into the array with plain read-add-writes in two rounds (own
+// column, then the next).  When the (cell, band) changes, or after max_run_lines lines (precision
+// modes), the array goes into the map with one L2 reduction per pixel and plane (zeros skipped), in
+// flush mode FLUSH; lane L flushes the columns congruent to L mod 32.  Other lines go sample by
 // sample straight into the map (twelve reductions each).  Batches use planned_kernel.
 //
 // Each warp streams its lines through a ring of BP line slots in shared memory (y, x, alpha and TOD
@@ -801,16 +802,17 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
 // of the one being processed, so a warp keeps BP - 1 lines of memory traffic in flight while it
 // works without holding registers for them.
 
-constexpr int BW = 12;                 // warps per CTA (2 CTAs per SM: 85 registers a thread)
+constexpr int BW = 12;                 // warps per CTA (2 CTAs per SM; 16 measured no faster)
 constexpr int BNT = BW * 32;
 constexpr int BP = 8;                  // line slots per warp (a power of two)
 constexpr size_t kBandSmem = (size_t) BW * BP * 128 * sizeof(float);
 constexpr uint32_t kNoKey = 0xffffffffu;
 
 struct BandState {
-    float acc[3][6];    // [slot][row * 3 + plane]; slot s holds column 32 s + lane
+    float *acc;         // the warp's accumulator in shared memory: [row * 3 + plane][96 columns]
     uint32_t key;       // cell | band << 20 of the accumulated lines, or kNoKey
     int R0, x0;         // rows R0, R0 + 1; columns x0 + [0, 96) (unwrapped; mod nx with PERIODIC)
+    float R0f, x0f;     // the same as floats
 };
 
 // Adds the accumulator into the map (one addition per non-zero pixel and plane, in flush mode FLUSH)
@@ -835,7 +837,7 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
                 gx %= a.nx;
             else
                 xin = gx < a.nx;
-            const float v = B.acc[sl][3 * r + p];
+            const float v = B.acc[(3 * r + p) * 96 + 32 * sl + lane];
             const int64_t o = (xin && (v != 0.0f)) ? global_pixel_offset(B.R0 + r, gx, a) : -1;
             off[i] = (o >= 0) ? (o + p * a.polstride) : -1;
             old[i] = (off[i] >= 0) ? atomicAdd(a.out + off[i], v) : 0.0f;
@@ -843,9 +845,10 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
 #pragma unroll
         for (int i = 0; i < 18; i++) {
             const int sl = i / 6, r = (i % 6) / 3, p = i % 3;
+            float &v = B.acc[(3 * r + p) * 96 + 32 * sl + lane];
             if (off[i] >= 0)
-                add_rounding_error(a, off[i], old[i], B.acc[sl][3 * r + p]);
-            B.acc[sl][3 * r + p] = 0.0f;
+                add_rounding_error(a, off[i], old[i], v);
+            v = 0.0f;
         }
     } else {
 #pragma unroll
@@ -858,7 +861,8 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
                 xin = gx < a.nx;
 #pragma unroll
             for (int r = 0; r < 2; r++) {
-                const float t = B.acc[sl][3 * r], q = B.acc[sl][3 * r + 1], u = B.acc[sl][3 * r + 2];
+                float *c = B.acc + 3 * r * 96 + 32 * sl + lane;
+                const float t = c[0], q = c[96], u = c[192];
                 const bool nz = (t != 0.0f) || (q != 0.0f) || (u != 0.0f);
                 if (__any_sync(kFullMask, nz) && nz && xin) {
                     if constexpr (FLUSH == kFlushHotF64) {
@@ -872,9 +876,9 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
                         }
                     }
                 }
-                B.acc[sl][3 * r] = 0.0f;
-                B.acc[sl][3 * r + 1] = 0.0f;
-                B.acc[sl][3 * r + 2] = 0.0f;
+                c[0] = 0.0f;
+                c[96] = 0.0f;
+                c[192] = 0.0f;
             }
         }
     }
@@ -882,10 +886,9 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
 
 // One cache line (lane = sample) on the band path, whose shape the plan has analysed: 'bw' is its band
 // word (gmm_common.cuh), with the fast bit set.  Returns false, having added nothing, if some sample
-// has |2a| > 1024 (those go the general way, through sincosf).  'tab' is the warp's table (bytes
-// 0..63 by column, 64 for a zero lane, 65..80 a sink).
+// has |2a| > 1024 (those go the general way, through sincosf).
 template<bool RESP, bool PERIODIC>
-__device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint8_t *tab, uint64_t bw, float y, float x,
+__device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint64_t bw, float y, float x,
                                           float al, float tv, uint32_t s)
 {
     const int lane = threadIdx.x & 31;
@@ -893,14 +896,12 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint8_t
     if (!__all_sync(kFullMask, fabsf(th) <= 1024.0f))
         return false;
     const unsigned su = (unsigned) bw;                   // bit i: sample i in the column of sample i - 1
-    const int kmin = (int) ((bw >> kBandKminShift) & 127u);
-    const int ncol = (int) ((bw >> kBandNcolShift) & 63u);
     const bool inc = (bw & kBandInc) != 0ull;
     const bool r3 = (bw & kBandRun3) != 0ull;
     // dy = y - R0 and xr = x - x0 are exact (integers R0 <= y, x0 <= x; the plan checked both).
-    const float dy = y - (float) B.R0;
+    const float dy = y - B.R0f;
     float fk;
-    const float xr = x - (float) B.x0;
+    const float xr = x - B.x0f;
     const int k = floor_nonneg(xr, &fk);
     const float dx = xr - fk;   // = x - floor(x), exactly
 
@@ -934,69 +935,62 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint8_t
     const bool sprev = (inc ? sl : (sl >> 1)) & 1u;
     const bool snext = (inc ? (sl >> 1) : sl) & 1u;
     const bool last = !snext;   // the last sample of its column holds the column's totals
-    float SA[6], SB[6];         // totals of this lane's column (weights 1 - dx) and the next (dx)
+    const float wap = sprev ? 1.0f - dxp : 0.0f, wbp = sprev ? dxp : 0.0f;
+    const float wa = 1.0f - dx;
+    // The last sample of each column's run adds the column's totals: weights 1 - dx into its column
+    // k, dx into k + 1.  Those lanes have distinct k, so two rounds of plain read-add-writes (columns
+    // k, then k + 1) never put two lanes on one word.  (k is clamped: a plan used with pointing other
+    // than its own gives wrong sums, never an access outside the accumulator.)
+    const int kc = (int) min((unsigned) k, 94u);
     if (!r3) {
-        // At most two samples per column: the last one adds the previous one's share.
-        const bool lp = last && sprev;
-        const float wa = last ? 1.0f - dx : 0.0f, wb = last ? dx : 0.0f;
-        const float wap = lp ? 1.0f - dxp : 0.0f, wbp = lp ? dxp : 0.0f;
+        // At most two samples per column: the last one adds the previous one's share too.
+        __syncwarp();
+        if (last) {
+            float *c = B.acc + kc;
 #pragma unroll
-        for (int p = 0; p < 6; p++) {
-            SA[p] = fmaf(wap, Vp[p], wa * V[p]);
-            SB[p] = fmaf(wbp, Vp[p], wb * V[p]);
+            for (int p = 0; p < 6; p++)
+                c[96 * p] = fmaf(wa, V[p], fmaf(wap, Vp[p], c[96 * p]));
         }
-    } else {
-        // Up to four: pairs first, then the pair two samples back if it is in the same column.
-        const float wap = sprev ? 1.0f - dxp : 0.0f, wbp = sprev ? dxp : 0.0f;
+        __syncwarp();
+        if (last) {
+            float *c = B.acc + kc + 1;
 #pragma unroll
-        for (int p = 0; p < 6; p++) {
-            SA[p] = fmaf(wap, Vp[p], (1.0f - dx) * V[p]);
-            SB[p] = fmaf(wbp, Vp[p], dx * V[p]);
+            for (int p = 0; p < 6; p++)
+                c[96 * p] = fmaf(dx, V[p], fmaf(wbp, Vp[p], c[96 * p]));
         }
-        const int src2 = (lane + (inc ? 30 : 2)) & 31;
-        const unsigned sp2 = inc ? (lane > 0 ? (su >> (lane - 1)) : 0u) : ((lane < 30) ? (su >> (lane + 2)) : 0u);
-        const bool sprev2 = sprev && (sp2 & 1u);
-#pragma unroll
-        for (int p = 0; p < 6; p++) {
-            const float a2 = __shfl_sync(kFullMask, SA[p], src2);
-            const float b2 = __shfl_sync(kFullMask, SB[p], src2);
-            SA[p] = last ? (sprev2 ? SA[p] + a2 : SA[p]) : 0.0f;
-            SB[p] = last ? (sprev2 ? SB[p] + b2 : SB[p]) : 0.0f;
-        }
+        return true;
     }
-    // Column n (in scan order) of the line is kmin + n.  tab[2n] = the lane holding column n's own
-    // totals, tab[2n + 3] = the same lane (its dx share falls on column n + 1); the other lanes, whose
-    // totals are zero, write their number into tab[64] (any one of them will do).  (& 31: a plan
-    // used with pointing other than its own gives wrong sums, never an access outside the table.)
-    const int n = (k - kmin) & 31;
-    __syncwarp();   // the previous line's reads of the table are done
-    tab[last ? 2 * n : 64] = (uint8_t) lane;
-    tab[last ? 2 * n + 3 : 65 + (lane & 15)] = (uint8_t) lane;
+    // Runs of three or four: pair sums first, then the pair two samples back if it is in the same
+    // column (only the last lane of each run uses them, so the others' sums need not be correct).
+    float SA[6], SB[6];
+#pragma unroll
+    for (int p = 0; p < 6; p++) {
+        SA[p] = fmaf(wap, Vp[p], wa * V[p]);
+        SB[p] = fmaf(wbp, Vp[p], dx * V[p]);
+    }
+    const int src2 = (lane + (inc ? 30 : 2)) & 31;
+    const unsigned sp2 = inc ? (lane > 0 ? (su >> (lane - 1)) : 0u) : ((lane < 30) ? (su >> (lane + 2)) : 0u);
+    const bool sprev2 = sprev && (sp2 & 1u);
+#pragma unroll
+    for (int p = 0; p < 6; p++) {
+        const float a2 = __shfl_sync(kFullMask, SA[p], src2);
+        const float b2 = __shfl_sync(kFullMask, SB[p], src2);
+        SA[p] = sprev2 ? SA[p] + a2 : SA[p];
+        SB[p] = sprev2 ? SB[p] + b2 : SB[p];
+    }
     __syncwarp();
-    const int nA = (lane - kmin) & 31;   // this lane's column kmin + nA is congruent to lane mod 32
-    const unsigned e = reinterpret_cast<const uint16_t *>(tab)[nA];
-    const int zl = tab[64];              // a lane whose totals are zero
-    const int srcA = (nA < ncol) ? (int) (e & 0xffu) : zl;
-    const int srcB = ((unsigned) (nA - 1) < (unsigned) ncol) ? (int) (e >> 8) : zl;
-    float C[6];
+    if (last) {
+        float *c = B.acc + kc;
 #pragma unroll
-    for (int p = 0; p < 6; p++)
-        C[p] = __shfl_sync(kFullMask, SA[p], srcA) + __shfl_sync(kFullMask, SB[p], srcB);
-    // The line spans at most 32 columns, so at most two slots: the one of kmin and the next.
-    const int slo = kmin >> 5;
-    const bool hi = ((kmin + nA) >> 5) != slo;
-    if (slo == 0) {
+        for (int p = 0; p < 6; p++)
+            c[96 * p] += SA[p];
+    }
+    __syncwarp();
+    if (last) {
+        float *c = B.acc + kc + 1;
 #pragma unroll
-        for (int p = 0; p < 6; p++) {
-            B.acc[0][p] += hi ? 0.0f : C[p];
-            B.acc[1][p] += hi ? C[p] : 0.0f;
-        }
-    } else {
-#pragma unroll
-        for (int p = 0; p < 6; p++) {
-            B.acc[1][p] += (slo == 1 && !hi) ? C[p] : 0.0f;
-            B.acc[2][p] += (slo == 1) == hi ? C[p] : 0.0f;
-        }
+        for (int p = 0; p < 6; p++)
+            c[96 * p] += SB[p];
     }
     return true;
 }
@@ -1079,7 +1073,9 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
                      const uint32_t *__restrict__ cellmap, const uint64_t *__restrict__ band)
 {
     extern __shared__ float s_lines[];    // [BW][BP][4 rows][32]: y, x, alpha, TOD
-    __shared__ __align__(4) uint8_t s_tab[BW][96];
+    __shared__ float s_acc[BW][6 * 96];
+    __shared__ uint32_t s_wline[BW][64], s_wkey[BW][64];
+    __shared__ uint64_t s_wbw[BW][64];
     __shared__ uint32_t s_err[BW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t nw = (int64_t) gridDim.x * BW;
@@ -1089,55 +1085,54 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
     const uint32_t nsamp = (uint32_t) a.nsamp;
     const uint32_t nlines = nsamp >> 5;
     uint32_t err = a.partial ? 0u : check_plan_cells(cellmap, a);
-    uint8_t *tab = s_tab[warp];
     float *ring = s_lines + (size_t) warp * BP * 128;
     // This lane's 16-byte piece of every line: row lane/8 (y, x, alpha, TOD), samples 4 (lane%8) + [0, 4).
     const int row = lane >> 3, piece = 4 * (lane & 7);
     const float *__restrict__ src_row = (row < 3) ? (a.xp + (size_t) row * nsamp) : a.in;
 
     BandState B;
-#pragma unroll
-    for (int sl = 0; sl < 3; sl++)
-#pragma unroll
-        for (int p = 0; p < 6; p++)
-            B.acc[sl][p] = 0.0f;
+    B.acc = s_acc[warp];
+    for (int i = lane; i < 6 * 96; i += 32)
+        B.acc[i] = 0.0f;
+    __syncwarp();
     B.key = kNoKey;
     B.R0 = 0;
     B.x0 = 0;
-    int64_t run = 0;   // lines in the accumulator since its last flush (precision modes cap it)
+    B.R0f = 0.0f;
+    B.x0f = 0.0f;
+    int run = 0;   // lines in the accumulator since its last flush (precision modes cap it)
     // The cap of the current run: max_run_lines in the precision modes (only for hot owner cells in
     // the hot-cell mode, whose other cells reduce in float as the plain path does); 0: none.
-    int64_t cap = (FLUSH == kFlushF32) ? 0 : a.max_run_lines;
+    const int mrl = (a.max_run_lines < 0x7fffffff) ? (int) a.max_run_lines : 0x7fffffff;
+    int cap = (FLUSH == kFlushF32) ? 0 : mrl;
+    const int nq = (int) n;   // a warp's range is far below 2^31 entries
 
-    // Owner words of entries [32 G, 32 G + 64) of this warp's range: lane i holds entry 32 G + i (A)
-    // and 32 (G + 1) + i (B), decoded as (line, key); lines >= nlines (a plan that does not belong to
-    // this xpointing) are flagged and skipped.
-    auto decode = [&](int64_t g, uint32_t &line, uint32_t &key, uint64_t &bw) {
-        const int64_t q = 32 * g + lane;
-        const uint64_t w = (q < n) ? __ldg(owner_mt + e0 + q) : 0ull;
-        bw = (q < n) ? __ldg(band + e0 + q) : 0ull;
-        line = (q < n) ? (uint32_t) ((w >> 20) & kClMask) : 0xffffffffu;
-        key = (uint32_t) (w & kCellMask) | ((uint32_t) ((w >> kBandShift) & 63u) << 20);
-        if ((q < n) && (line >= nlines)) {
+    // The warp's decoded owner entries, two groups of 32 in turn: entry q at [q & 63].  Lines >=
+    // nlines (a plan that does not belong to this xpointing) are flagged and skipped (0xffffffff).
+    uint32_t *wline = s_wline[warp], *wkey = s_wkey[warp];
+    uint64_t *wbw = s_wbw[warp];
+    auto decode = [&](int g) {
+        const int q = 32 * g + lane;
+        const uint64_t w = (q < nq) ? __ldg(owner_mt + e0 + q) : 0ull;
+        const uint64_t bw = (q < nq) ? __ldg(band + e0 + q) : 0ull;
+        uint32_t line = (q < nq) ? (uint32_t) ((w >> 20) & kClMask) : 0xffffffffu;
+        if ((q < nq) && (line >= nlines)) {
             err |= kErrInconsistentNmt;
             line = 0xffffffffu;
         }
+        wline[q & 63] = line;
+        wkey[q & 63] = (uint32_t) (w & kCellMask) | ((uint32_t) ((w >> kBandShift) & 63u) << 20);
+        wbw[q & 63] = bw;
     };
-    uint32_t lineA, keyA, lineB, keyB;
-    uint64_t bwA, bwB;
-    decode(0, lineA, keyA, bwA);
-    decode(1, lineB, keyB, bwB);
-    int64_t G = 0;
+    decode(0);
+    decode(1);
+    __syncwarp();
 
-    // Entry q's line (0xffffffff: none), for q in groups G and G + 1; warp-uniform.
-    auto line_of = [&](int64_t q) -> uint32_t {
-        return __shfl_sync(kFullMask, ((q >> 5) == G) ? lineA : lineB, (int) (q & 31));
-    };
     // Starts the copy of entry q's line into its ring slot (always commits one group, maybe empty).
-    auto issue = [&](int64_t q) {
-        const uint32_t line = (q < n) ? line_of(q) : 0xffffffffu;
+    auto issue = [&](int q) {
+        const uint32_t line = wline[q & 63];   // decoded (0xffffffff past the range's end)
         if (line != 0xffffffffu)
-            cp_async16(ring + (q & (BP - 1)) * 128 + 32 * row + piece, src_row + 32 * (size_t) line + piece);
+            cp_async16(ring + (q & (BP - 1)) * 128 + 32 * row + piece, src_row + (size_t) (32u * line + piece));
         cp_async_commit();
     };
 
@@ -1145,44 +1140,45 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
     for (int q = 0; q < BP - 1; q++)
         issue(q);
 #pragma unroll 1
-    for (int64_t q = 0; q < n; q++) {
-        if (((q & 31) == 0) && (q > 0)) {
-            lineA = lineB;
-            keyA = keyB;
-            bwA = bwB;
-            G++;
-            decode(G + 1, lineB, keyB, bwB);
-        }
-        issue(q + BP - 1);             // into the slot of line q - 1, released at the end of that step
-        cp_async_wait<BP - 1>();       // this lane's piece of line q has landed
-        __syncwarp();
-        const uint32_t line = __shfl_sync(kFullMask, lineA, (int) (q & 31));
-        const uint32_t key = __shfl_sync(kFullMask, keyA, (int) (q & 31));
-        const uint64_t bw = __shfl_sync(kFullMask, bwA, (int) (q & 31));
-        if (line != 0xffffffffu) {
-            const float *slot = ring + (q & (BP - 1)) * 128;
-            const float y = slot[lane], x = slot[32 + lane], al = slot[64 + lane], tv = slot[96 + lane];
-            const uint32_t s = (line << 5) + (uint32_t) lane;
-            if ((key != B.key) || ((cap > 0) && (run >= cap))) {
-                if (B.key != kNoKey)
-                    band_flush<PERIODIC, FLUSH>(a, B);
-                B.key = key;
-                B.R0 = ((int) ((key >> 10) & 1023u) << 6) + (int) (key >> 20);
-                B.x0 = (int) (key & 1023u) << 6;
-                run = 0;
-                if constexpr (FLUSH == kFlushHotF64) {
-                    const int iyc = (int) ((key >> 10) & 1023u), ixc = (int) (key & 1023u);
-                    const bool hot = (iyc < a.nycells) && (ixc < a.nxcells) &&
-                                     (__ldg(a.hot_slot + (int64_t) iyc * a.nxcells + ixc) >= 0);
-                    cap = hot ? a.max_run_lines : 0;
+    for (int q0 = 0; q0 < nq; q0 += 32) {
+        if (q0 > 0)
+            decode((q0 >> 5) + 1);     // over the group before q0's, which no one reads any more
+        const int qe = min(q0 + 32, nq);
+#pragma unroll 1
+        for (int q = q0; q < qe; q++) {
+            issue(q + BP - 1);         // into the slot of line q - 1, released at the end of that step
+            cp_async_wait<BP - 1>();   // this lane's piece of line q has landed
+            __syncwarp();
+            const uint32_t line = wline[q & 63];
+            if (line != 0xffffffffu) {
+                const uint32_t key = wkey[q & 63];
+                const uint64_t bw = wbw[q & 63];
+                const float *slot = ring + (q & (BP - 1)) * 128;
+                const float y = slot[lane], x = slot[32 + lane], al = slot[64 + lane], tv = slot[96 + lane];
+                const uint32_t s = (line << 5) + (uint32_t) lane;
+                if ((key != B.key) || ((cap > 0) && (run >= cap))) {
+                    if (B.key != kNoKey)
+                        band_flush<PERIODIC, FLUSH>(a, B);
+                    B.key = key;
+                    B.R0 = ((int) ((key >> 10) & 1023u) << 6) + (int) (key >> 20);
+                    B.x0 = (int) (key & 1023u) << 6;
+                    B.R0f = (float) B.R0;
+                    B.x0f = (float) B.x0;
+                    run = 0;
+                    if constexpr (FLUSH == kFlushHotF64) {
+                        const int iyc = (int) ((key >> 10) & 1023u), ixc = (int) (key & 1023u);
+                        const bool hot = (iyc < a.nycells) && (ixc < a.nxcells) &&
+                                         (__ldg(a.hot_slot + (int64_t) iyc * a.nxcells + ixc) >= 0);
+                        cap = hot ? mrl : 0;
+                    }
                 }
+                if ((bw & kBandFast) && band_line<RESP, PERIODIC>(a, B, bw, y, x, al, tv, s))
+                    run++;
+                else
+                    band_general_sample<RESP, PERIODIC, FLUSH>(a, y, x, al, tv, s, err);
             }
-            if ((bw & kBandFast) && band_line<RESP, PERIODIC>(a, B, tab, bw, y, x, al, tv, s))
-                run++;
-            else
-                band_general_sample<RESP, PERIODIC, FLUSH>(a, y, x, al, tv, s, err);
+            __syncwarp();              // everyone is done with this slot before it is refilled
         }
-        __syncwarp();                  // everyone is done with this slot before it is refilled
     }
     cp_async_wait<0>();
     if (B.key != kNoKey)

@@ -137,3 +137,37 @@ def test_bands_absent_cells_and_response(g, kernel_knob):
         g.tod2map(out, tg, xg, plan, partial_pixelization=True, response=torch.from_numpy(resp).cuda())
         rl1, mx = rel_stats(out.arr.cpu().numpy(), want_r)
         assert rl1 < RL1_TOL and mx < MAX_TOL, ("response", which, rl1, mx)
+
+
+def test_absent_cell_in_every_cell_row(g, kernel_knob):
+    """The not-in-pixelization check covers the plan's whole cell bitmap on both tod2map kernels and
+    in map2tod, whatever their block sizes: scans through cell rows 0..15 of a 1024-row map, one absent
+    cell in each of rows 5, 12 and 15."""
+    import torch
+    rng = np.random.default_rng(12)
+    ny, nx, periodic = 1024, 512, True
+    for row in (5, 12, 15):
+        xp = bounce_scan(rng, 8, 4096, ny, nx, periodic, 0.6, 0.0)
+        xp[0] += 64.0 * row + 20.0 - xp[0].min()          # into cell row 'row'
+        xg = torch.from_numpy(xp).cuda()
+        pp = g.PointingPrePlan(xg, ny, nx, periodic_xcoord=periodic)
+        plan = g.PointingPlan(pp, xg)
+        cx = int(np.floor(xp[1, 0, 0] / 64.0))
+        o = np.full((16, 8), -1, np.int64)
+        k = 0
+        for iy in range(16):
+            for ix in range(8):
+                if (iy, ix) != (row, cx):
+                    o[iy, ix] = 3 * 4096 * k
+                    k += 1
+        lp = g.LocalPixelization(ny, nx, o, 64, 4096, periodic)
+        tg = torch.from_numpy(rng.standard_normal(xp.shape[1:]).astype(np.float32)).cuda()
+        for which in KERNELS:
+            kernel_knob(which)
+            out = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+            with pytest.raises(RuntimeError, match="not in LocalPixelization"):
+                g.tod2map(out, tg, xg, plan, partial_pixelization=False)
+        with pytest.raises(RuntimeError, match="not in LocalPixelization"):
+            g.map2tod(torch.zeros(xp.shape[1:], device="cuda"), g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda")),
+                      xg, plan, partial_pixelization=False)
+
