@@ -1188,83 +1188,134 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
 
 // ------------------------------------------------------------------------------------------------
 // Unplanned operators (map2tod_unplanned.cu:17-71, tod2map_unplanned.cu:17-66): one pass over the
-// samples, map accesses straight to global memory.  Four consecutive samples per thread with
-// 16-byte loads when the arrays are aligned.
-//
-// tod2map accumulates a thread's consecutive samples in a window of two adjacent map columns (rows
-// iy, iy+1, planes T, Q, U) held in registers; a column goes to the map (one global reduction per
-// pixel and plane) when the window moves past it.  A scan crosses a column every 1/speed samples,
-// so the L2 performs about half the reductions of one per sample and neighbour, which bound this
-// kernel.  Every pixel a sample touches is flushed once, so the not-in-pixelization check is the
-// per-sample one.
+// samples, map accesses straight to global memory.
 
-struct ColumnWindow {
-    int iy, cx;             // rows iy, iy + 1 and columns cx, cx + 1; cx < 0: empty
-    float c0[6], c1[6];     // column cx and cx + 1: [row * 3 + plane]
-};
-
-__device__ __forceinline__ void window_flush(const OpArgs &a, int iy, int ix, float *v, uint32_t &err)
+// Unplanned tod2map by cache lines: one warp per 32 consecutive samples (lane = sample), the next
+// line's loads issued before this one is processed.  A line whose samples all lie in one pixel row
+// pair (same iy0, ix1 = ix0 + 1) and move by 0 or 1 column per sample in one direction with at most
+// four samples per column (a raster scan between 0.25 and 1 px/sample, except at turnarounds) sums
+// the samples of each column by one or two shuffle steps, and only the last lane of each column's
+// run adds into the map: 12 reductions per column instead of per sample, on distinct addresses.  Other lines add
+// sample by sample (map_accumulator, gpu_mm_internals.hpp:299-355).  Error bits as per sample: the
+// run's samples touch the pixels its last lane adds to.
+template<bool PERIODIC>
+__device__ __forceinline__ void unplanned_t2m_line(const OpArgs &a, bool valid, float y, float x, float al, float tv,
+                                                   uint32_t &err)
 {
+    const int lane = threadIdx.x & 31;
+    Located L;
+    const uint32_t e = locate(y, x, a.ny, a.nx, PERIODIC, L);
+    err |= valid ? e : 0u;
+    float sn, cs;
+    sincos2a(al, &sn, &cs);
+    const float t = tv, q = tv * cs, u = tv * sn;
+    const int iyA = __shfl_sync(kFullMask, L.iy0, 0);
+    const int dk = L.ix0 - __shfl_up_sync(kFullMask, L.ix0, 1);
+    const bool ok = valid && (e == 0u) && (L.iy0 == iyA) && (L.ix1 == L.ix0 + 1);
+    const unsigned same = __ballot_sync(kFullMask, (lane > 0) && (dk == 0));
+    const unsigned up = __ballot_sync(kFullMask, (lane > 0) && (dk == 1));
+    const unsigned down = __ballot_sync(kFullMask, (lane > 0) && (dk == -1));
+    const unsigned bad = __ballot_sync(kFullMask, !ok);
+    const unsigned r3 = same & (same >> 1);   // some column holds three or more samples
+    const bool fast = (bad == 0u) && ((same | up | down) == 0xfffffffeu) && ((up == 0u) || (down == 0u)) &&
+                      ((r3 & (r3 >> 2)) == 0u);
+    if (!fast) {
+        if (valid) {
+            const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
+            global_accum(a, a.out, L.iy0, L.ix0, t, q, u, wy0 * wx0, err);
+            global_accum(a, a.out, L.iy0, L.ix1, t, q, u, wy0 * L.dx, err);
+            global_accum(a, a.out, L.iy1, L.ix0, t, q, u, L.dy * wx0, err);
+            global_accum(a, a.out, L.iy1, L.ix1, t, q, u, L.dy * L.dx, err);
+        }
+        return;
+    }
+    // Scan order: lane order if x increases, reversed if it decreases.
+    const bool inc = down == 0u;
+    const float wy0 = 1.0f - L.dy;
+    const float V[6] = {wy0 * t, wy0 * q, wy0 * u, L.dy * t, L.dy * q, L.dy * u};
+    const int src = (lane + (inc ? 31 : 1)) & 31;
+    float Vp[6];
 #pragma unroll
-    for (int r = 0; r < 2; r++) {
-        const int64_t off = global_pixel_offset(iy + r, ix, a);
-        if (off >= 0) {
-            atomicAdd(a.out + off, v[3 * r]);
-            atomicAdd(a.out + off + a.polstride, v[3 * r + 1]);
-            atomicAdd(a.out + off + 2 * a.polstride, v[3 * r + 2]);
+    for (int p = 0; p < 6; p++)
+        Vp[p] = __shfl_sync(kFullMask, V[p], src);
+    const float dxp = __shfl_sync(kFullMask, L.dx, src);
+    const unsigned sl = same >> lane;
+    const bool sprev = (inc ? sl : (sl >> 1)) & 1u;
+    const bool snext = (inc ? (sl >> 1) : sl) & 1u;
+    // Column totals over the run so far (weights 1 - dx for this column, dx for the next): this
+    // sample and the previous one if it is in the same column; for runs of three or four, plus the
+    // pair two samples back.
+    const float wap = sprev ? 1.0f - dxp : 0.0f, wbp = sprev ? dxp : 0.0f;
+    float SA[6], SB[6];
+#pragma unroll
+    for (int p = 0; p < 6; p++) {
+        SA[p] = fmaf(wap, Vp[p], (1.0f - L.dx) * V[p]);
+        SB[p] = fmaf(wbp, Vp[p], L.dx * V[p]);
+    }
+    if (r3 != 0u) {
+        const int src2 = (lane + (inc ? 30 : 2)) & 31;
+        const unsigned sp2 = inc ? (lane > 0 ? (same >> (lane - 1)) : 0u) : ((lane < 30) ? (same >> (lane + 2)) : 0u);
+        const bool sprev2 = sprev && (sp2 & 1u);
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+            const float a2 = __shfl_sync(kFullMask, SA[p], src2);
+            const float b2 = __shfl_sync(kFullMask, SB[p], src2);
+            SA[p] = sprev2 ? SA[p] + a2 : SA[p];
+            SB[p] = sprev2 ? SB[p] + b2 : SB[p];
+        }
+    }
+    if (snext)
+        return;   // not the last sample of its column: the last one adds this one's share
+    const int64_t o00 = global_pixel_offset(L.iy0, L.ix0, a), o01 = global_pixel_offset(L.iy0, L.ix1, a);
+    const int64_t o10 = global_pixel_offset(L.iy1, L.ix0, a), o11 = global_pixel_offset(L.iy1, L.ix1, a);
+    const int64_t o[4] = {o00, o10, o01, o11};
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        if (o[c] >= 0) {
+            const int r = c & 1;     // row of o[c]; columns: own (c < 2) or next
+#pragma unroll
+            for (int p = 0; p < 3; p++)
+                atomicAdd(a.out + o[c] + p * a.polstride, (c < 2) ? SA[3 * r + p] : SB[3 * r + p]);
         } else {
             err |= a.partial ? 0u : kErrNotInPixelization;
         }
     }
-#pragma unroll
-    for (int k = 0; k < 6; k++)
-        v[k] = 0.0f;
 }
 
-// Adds one located sample (t, q, u = its T, Q, U factors) into the window, moving or restarting
-// the window as needed; samples whose x neighbours wrap around the map go straight to the map.
-__device__ __forceinline__ void window_add(const OpArgs &a, ColumnWindow &W, const Located &L, float t, float q,
-                                           float u, uint32_t &err)
-{
-    const float wy0 = 1.0f - L.dy, wx0 = 1.0f - L.dx;
-    const float w00 = wy0 * wx0, w01 = wy0 * L.dx, w10 = L.dy * wx0, w11 = L.dy * L.dx;
-    if (L.ix1 != L.ix0 + 1) {
-        global_accum(a, a.out, L.iy0, L.ix0, t, q, u, w00, err);
-        global_accum(a, a.out, L.iy0, L.ix1, t, q, u, w01, err);
-        global_accum(a, a.out, L.iy1, L.ix0, t, q, u, w10, err);
-        global_accum(a, a.out, L.iy1, L.ix1, t, q, u, w11, err);
-        return;
-    }
-    const bool same_row = (W.cx >= 0) && (L.iy0 == W.iy);
-    if (same_row && (L.ix0 == W.cx + 1)) {
-        window_flush(a, W.iy, W.cx, W.c0, err);
-#pragma unroll
-        for (int k = 0; k < 6; k++) {
-            W.c0[k] = W.c1[k];
-            W.c1[k] = 0.0f;
-        }
-        W.cx += 1;
-    } else if (!(same_row && (L.ix0 == W.cx))) {
-        if (W.cx >= 0) {
-            window_flush(a, W.iy, W.cx, W.c0, err);
-            window_flush(a, W.iy, W.cx + 1, W.c1, err);
-        }
-        W.iy = L.iy0;
-        W.cx = L.ix0;
-    }
-    const float f[3] = {t, q, u};
-#pragma unroll
-    for (int p = 0; p < 3; p++) {
-        W.c0[p] += w00 * f[p];
-        W.c1[p] += w01 * f[p];
-        W.c0[3 + p] += w10 * f[p];
-        W.c1[3 + p] += w11 * f[p];
-    }
-}
-
-template<bool TOD2MAP, int V>
+template<bool PERIODIC>
 __global__ void __launch_bounds__(256)
-unplanned_kernel(OpArgs a)
+unplanned_tod2map_lines(OpArgs a)
+{
+    __shared__ uint32_t s_err[8];
+    uint32_t err = 0;
+    const int lane = threadIdx.x & 31;
+    const int64_t nl = (a.nsamp + 31) / 32;
+    const int64_t nw = ((int64_t) gridDim.x * blockDim.x) >> 5;
+    int64_t l = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    auto load = [&](int64_t line, float &y, float &x, float &al, float &tv) -> bool {
+        const int64_t s = 32 * line + lane;
+        const bool v = (line < nl) && (s < a.nsamp);
+        y = v ? __ldcs(a.xp + s) : 0.0f;
+        x = v ? __ldcs(a.xp + a.nsamp + s) : 0.0f;
+        al = v ? __ldcs(a.xp + 2 * a.nsamp + s) : 0.0f;
+        tv = v ? __ldcs(a.in + s) : 0.0f;
+        return v;
+    };
+    float y, x, al, tv;
+    bool v = load(l, y, x, al, tv);
+    for (; l < nl; l += nw) {
+        float y2, x2, al2, tv2;
+        const bool v2 = load(l + nw, y2, x2, al2, tv2);
+        unplanned_t2m_line<PERIODIC>(a, v, y, x, al, tv, err);
+        y = y2; x = x2; al = al2; tv = tv2; v = v2;
+    }
+    block_publish_err(err, s_err, a.errword);
+}
+
+// Unplanned map2tod: V consecutive samples per thread (16-byte loads and stores when V = 4).
+template<int V>
+__global__ void __launch_bounds__(256)
+unplanned_map2tod_kernel(OpArgs a)
 {
     __shared__ uint32_t s_err[8];
     uint32_t err = 0;
@@ -1283,9 +1334,8 @@ unplanned_kernel(OpArgs a)
                 y[4 * h] = yy.x; y[4 * h + 1] = yy.y; y[4 * h + 2] = yy.z; y[4 * h + 3] = yy.w;
                 x[4 * h] = xx.x; x[4 * h + 1] = xx.y; x[4 * h + 2] = xx.z; x[4 * h + 3] = xx.w;
                 al[4 * h] = aa.x; al[4 * h + 1] = aa.y; al[4 * h + 2] = aa.z; al[4 * h + 3] = aa.w;
-                if (TOD2MAP || a.accum) {
-                    const float4 tt = TOD2MAP ? __ldcs(reinterpret_cast<const float4 *>(a.in + sh))
-                                              : *reinterpret_cast<const float4 *>(a.out + sh);
+                if (a.accum) {
+                    const float4 tt = *reinterpret_cast<const float4 *>(a.out + sh);
                     tv[4 * h] = tt.x; tv[4 * h + 1] = tt.y; tv[4 * h + 2] = tt.z; tv[4 * h + 3] = tt.w;
                 } else {
                     tv[4 * h] = tv[4 * h + 1] = tv[4 * h + 2] = tv[4 * h + 3] = 0.0f;
@@ -1295,46 +1345,28 @@ unplanned_kernel(OpArgs a)
             y[0] = __ldcs(a.xp + s0);
             x[0] = __ldcs(a.xp + a.nsamp + s0);
             al[0] = __ldcs(a.xp + 2 * a.nsamp + s0);
-            tv[0] = TOD2MAP ? __ldcs(a.in + s0) : (a.accum ? a.out[s0] : 0.0f);
+            tv[0] = a.accum ? a.out[s0] : 0.0f;
         }
-        ColumnWindow W;
-        W.iy = 0;
-        W.cx = -1;
-#pragma unroll
-        for (int k = 0; k < 6; k++)
-            W.c0[k] = W.c1[k] = 0.0f;
 #pragma unroll
         for (int k = 0; k < V; k++) {
             Located L;
             err |= locate(y[k], x[k], a.ny, a.nx, a.periodic, L);
             float sn, cs;
             sincos2a(al[k], &sn, &cs);
-            if constexpr (TOD2MAP) {
-                const float t = tv[k], q = t * cs, u = t * sn;
-                window_add(a, W, L, t, q, u, err);
-            } else {
-                const float e00 = global_eval(a, a.in, L.iy0, L.ix0, 1.0f, cs, sn, err);
-                const float e01 = global_eval(a, a.in, L.iy0, L.ix1, 1.0f, cs, sn, err);
-                const float e10 = global_eval(a, a.in, L.iy1, L.ix0, 1.0f, cs, sn, err);
-                const float e11 = global_eval(a, a.in, L.iy1, L.ix1, 1.0f, cs, sn, err);
-                const float rr = bilinear(L.dy, L.dx, e00, e01, e10, e11);
-                r[k] = a.accum ? (tv[k] + rr) : rr;
-            }
+            const float e00 = global_eval(a, a.in, L.iy0, L.ix0, 1.0f, cs, sn, err);
+            const float e01 = global_eval(a, a.in, L.iy0, L.ix1, 1.0f, cs, sn, err);
+            const float e10 = global_eval(a, a.in, L.iy1, L.ix0, 1.0f, cs, sn, err);
+            const float e11 = global_eval(a, a.in, L.iy1, L.ix1, 1.0f, cs, sn, err);
+            const float rr = bilinear(L.dy, L.dx, e00, e01, e10, e11);
+            r[k] = a.accum ? (tv[k] + rr) : rr;
         }
-        if constexpr (TOD2MAP) {
-            if (W.cx >= 0) {
-                window_flush(a, W.iy, W.cx, W.c0, err);
-                window_flush(a, W.iy, W.cx + 1, W.c1, err);
-            }
-        } else {
-            if constexpr (V >= 4) {
+        if constexpr (V >= 4) {
 #pragma unroll
-                for (int h = 0; h < V / 4; h++)
-                    __stcs(reinterpret_cast<float4 *>(a.out + s0 + 4 * h),
-                           make_float4(r[4 * h], r[4 * h + 1], r[4 * h + 2], r[4 * h + 3]));
-            } else {
-                __stcs(a.out + s0, r[0]);
-            }
+            for (int h = 0; h < V / 4; h++)
+                __stcs(reinterpret_cast<float4 *>(a.out + s0 + 4 * h),
+                       make_float4(r[4 * h], r[4 * h + 1], r[4 * h + 2], r[4 * h + 3]));
+        } else {
+            __stcs(a.out + s0, r[0]);
         }
     }
     block_publish_err(err, s_err, a.errword);
@@ -1458,15 +1490,24 @@ __global__ void fold_compensation_kernel(float *__restrict__ lmap, float *__rest
 template<bool TOD2MAP>
 cudaError_t launch_unplanned_impl(const OpArgs &a, cudaStream_t stream)
 {
-    const bool aligned = ((((uintptr_t) a.xp) | ((uintptr_t) a.out) | ((uintptr_t) a.in)) & 15) == 0;
-    const bool vec = aligned && ((a.nsamp & 3) == 0);
-    const int64_t nvec = vec ? a.nsamp / 4 : a.nsamp;
-    int64_t g = 8 * (int64_t) device_sm_count();
-    g = std::max<int64_t>(1, std::min<int64_t>(g, (nvec + 255) / 256));
-    if (vec)
-        unplanned_kernel<TOD2MAP, 4><<<(unsigned) g, 256, 0, stream>>>(a);
-    else
-        unplanned_kernel<TOD2MAP, 1><<<(unsigned) g, 256, 0, stream>>>(a);
+    if constexpr (TOD2MAP) {
+        int64_t g = 8 * (int64_t) device_sm_count();
+        g = std::max<int64_t>(1, std::min<int64_t>(g, (a.nsamp + 255) / 256));
+        if (a.periodic)
+            unplanned_tod2map_lines<true><<<(unsigned) g, 256, 0, stream>>>(a);
+        else
+            unplanned_tod2map_lines<false><<<(unsigned) g, 256, 0, stream>>>(a);
+    } else {
+        const bool aligned = ((((uintptr_t) a.xp) | ((uintptr_t) a.out)) & 15) == 0;
+        const bool vec = aligned && ((a.nsamp & 3) == 0);
+        const int64_t nvec = vec ? a.nsamp / 4 : a.nsamp;
+        int64_t g = 8 * (int64_t) device_sm_count();
+        g = std::max<int64_t>(1, std::min<int64_t>(g, (nvec + 255) / 256));
+        if (vec)
+            unplanned_map2tod_kernel<4><<<(unsigned) g, 256, 0, stream>>>(a);
+        else
+            unplanned_map2tod_kernel<1><<<(unsigned) g, 256, 0, stream>>>(a);
+    }
     return cudaGetLastError();
 }
 

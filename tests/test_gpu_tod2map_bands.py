@@ -1,5 +1,6 @@
 """Planned tod2map on both of its kernels -- row bands (the default for single-TOD plans) and
-shared-memory tiles -- against the oracle, on scans chosen to reach every branch of the band path:
+shared-memory tiles -- and unplanned tod2map against the oracle, on scans chosen to reach every
+branch of the band path and of the unplanned line path:
 scan speeds giving one to four samples per pixel column and more (which the band path leaves to
 its per-sample route), both scan directions, turnarounds, x wraparound, lines that drift across a
 pixel row, absent cells, and the per-detector response.
@@ -95,6 +96,11 @@ def test_bands_vs_tiles_vs_oracle(g, kernel_knob, case):
         g.tod2map(out, tg, xg, plan)
         rl1, mx = rel_stats(out.arr.cpu().numpy(), want)
         assert rl1 < RL1_TOL and mx < MAX_TOL, (which, rl1, mx)
+    # The unplanned operator's line path takes the same scans (runs of one to four samples per column).
+    out = g.LocalMap(lp, torch.from_numpy(m0).cuda())
+    g.tod2map(out, tg, xg, None)
+    rl1, mx = rel_stats(out.arr.cpu().numpy(), want)
+    assert rl1 < RL1_TOL and mx < MAX_TOL, ("unplanned", rl1, mx)
 
 
 def test_bands_absent_cells_and_response(g, kernel_knob):
