@@ -108,6 +108,9 @@ class PointingServer:
         self._next_stream = 0
         self._lock = threading.Lock()
         self._wake = threading.Condition(self._lock)   # signalled by submit() and close()
+        # Held by whichever thread admits and launches: the worker, or submit() when it finds the
+        # server idle and launches its request at once (no wait for the worker to wake up).
+        self._launch_mutex = threading.Lock()
         self._submitted = collections.deque()
         self._waiting = collections.deque()
         self._inflight = collections.deque()               # (event, requests, bytes, keepalive, error words, n), launch order
@@ -154,11 +157,38 @@ class PointingServer:
         ready = torch.cuda.Event()
         ready.record(stream)
         fut = concurrent.futures.Future()
+        req = {"kind": kind, "id": tod_id, "tod": tod, "t0": time.perf_counter(), "fut": fut, "ready": ready,
+               "stream": stream}
+        direct = False
         with self._lock:
-            self._submitted.append({"kind": kind, "id": tod_id, "tod": tod, "t0": time.perf_counter(), "fut": fut,
-                                    "ready": ready, "stream": stream})
-            self._wake.notify()
+            idle = not (self._submitted or self._waiting or self._launching or self._stop)
+            if idle and self._launch_mutex.acquire(blocking=False):
+                direct = True
+                self._waiting.append(req)
+                self._take_freed()
+                self._launching = True
+            else:
+                self._submitted.append(req)
+                self._wake.notify()
+        if direct:
+            # An idle server launches the request from the caller's thread (the same admission and
+            # launch as the worker's); anything left waiting goes to the worker.
+            try:
+                self._launch()
+            except Exception as e:   # _launch has failed the requests of that launch only
+                self.errors.append(repr(e))
+            finally:
+                with self._lock:
+                    self._launching = False
+                    if self._waiting or self._submitted:
+                        self._wake.notify()
+                self._launch_mutex.release()
         return fut
+
+    def _take_freed(self):
+        # With self._lock and self._launch_mutex held: memory that completions released.
+        self._used -= self._freed
+        self._freed = 0
 
     def drain(self, timeout=60.0):
         """Waits until every submitted request has completed."""
@@ -239,19 +269,19 @@ class PointingServer:
     def _run(self):
         try:
             while not self._stop:
-                with self._lock:
-                    while self._submitted:
-                        self._waiting.append(self._submitted.popleft())
-                    self._used -= self._freed
-                    self._freed = 0
-                    self._launching = bool(self._waiting)
-                try:
-                    launched = self._launch()
-                except Exception as e:   # _launch has failed the requests of that launch only
-                    launched = False
-                    self.errors.append(repr(e))
-                finally:
-                    self._launching = False
+                with self._launch_mutex:
+                    with self._lock:
+                        while self._submitted:
+                            self._waiting.append(self._submitted.popleft())
+                        self._take_freed()
+                        self._launching = bool(self._waiting)
+                    try:
+                        launched = self._launch()
+                    except Exception as e:   # _launch has failed the requests of that launch only
+                        launched = False
+                        self.errors.append(repr(e))
+                    finally:
+                        self._launching = False
                 if not launched:
                     # Nothing to launch: sleep until a request arrives or a completion frees memory
                     # (requests waiting for memory also retry after a short timeout).
