@@ -921,13 +921,14 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint64_
         fu = tv * sn;
     }
     const float wy0 = 1.0f - dy;
-    const float V[6] = {wy0 * ft, wy0 * fq, wy0 * fu, dy * ft, dy * fq, dy * fu};
+    const float f[3] = {ft, fq, fu};
     // The previous sample in scan order (lane -+ 1); unused where it does not exist.
     const int src = (lane + (inc ? 31 : 1)) & 31;
-    float Vp[6];
+    float fp[3];
 #pragma unroll
-    for (int p = 0; p < 6; p++)
-        Vp[p] = __shfl_sync(kFullMask, V[p], src);
+    for (int p = 0; p < 3; p++)
+        fp[p] = __shfl_sync(kFullMask, f[p], src);
+    const float dyp = __shfl_sync(kFullMask, dy, src);
     const float dxp = __shfl_sync(kFullMask, dx, src);
     // Same column as the previous / next sample in scan order: bits 0 and 1 of su >> lane, swapped
     // for decreasing x.
@@ -943,23 +944,34 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint64_
     // than its own gives wrong sums, never an access outside the accumulator.)
     const int kc = (int) min((unsigned) k, 94u);
     if (!r3) {
-        // At most two samples per column: the last one adds the previous one's share too.
+        // At most two samples per column: the last one adds the previous one's share too.  Bilinear
+        // weights per (row, column) of this sample and of the previous one.
+        const float wyp = 1.0f - dyp;
+        const float a0 = wa * wy0, a1 = wa * dy, b0 = dx * wy0, b1 = dx * dy;
+        const float pa0 = wap * wyp, pa1 = wap * dyp, pb0 = wbp * wyp, pb1 = wbp * dyp;
         __syncwarp();
         if (last) {
             float *c = B.acc + kc;
 #pragma unroll
-            for (int p = 0; p < 6; p++)
-                c[96 * p] = fmaf(wa, V[p], fmaf(wap, Vp[p], c[96 * p]));
+            for (int p = 0; p < 3; p++) {
+                c[96 * p] = fmaf(a0, f[p], fmaf(pa0, fp[p], c[96 * p]));
+                c[96 * (3 + p)] = fmaf(a1, f[p], fmaf(pa1, fp[p], c[96 * (3 + p)]));
+            }
         }
         __syncwarp();
         if (last) {
             float *c = B.acc + kc + 1;
 #pragma unroll
-            for (int p = 0; p < 6; p++)
-                c[96 * p] = fmaf(dx, V[p], fmaf(wbp, Vp[p], c[96 * p]));
+            for (int p = 0; p < 3; p++) {
+                c[96 * p] = fmaf(b0, f[p], fmaf(pb0, fp[p], c[96 * p]));
+                c[96 * (3 + p)] = fmaf(b1, f[p], fmaf(pb1, fp[p], c[96 * (3 + p)]));
+            }
         }
         return true;
     }
+    const float V[6] = {wy0 * ft, wy0 * fq, wy0 * fu, dy * ft, dy * fq, dy * fu};
+    const float wyp = 1.0f - dyp;
+    const float Vp[6] = {wyp * fp[0], wyp * fp[1], wyp * fp[2], dyp * fp[0], dyp * fp[1], dyp * fp[2]};
     // Runs of three or four: pair sums first, then the pair two samples back if it is in the same
     // column (only the last lane of each run uses them, so the others' sums need not be correct).
     float SA[6], SB[6];
