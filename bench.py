@@ -310,6 +310,11 @@ def precision_study(max_run_lines=32):
         "fp32_compensated_flush": lambda: (g.tod2map_compensated(lmap, comp, tod, xp, plan, max_run_lines=max_run_lines),
                                            g.fold_compensation(lmap, comp)),
         "fp64_map": lambda: g.tod2map_f64(f64, lp, tod, xp, plan, max_run_lines=max_run_lines),
+        # The same two modes with partials of up to 8x as many lines: fewer flushes, longer float sums.
+        "fp32_compensated_flush_long_runs": lambda: (
+            g.tod2map_compensated(lmap, comp, tod, xp, plan, max_run_lines=8 * max_run_lines),
+            g.fold_compensation(lmap, comp)),
+        "fp64_map_long_runs": lambda: g.tod2map_f64(f64, lp, tod, xp, plan, max_run_lines=8 * max_run_lines),
     }
     results = {}
     for name, fn in calls.items():
@@ -327,8 +332,10 @@ def precision_study(max_run_lines=32):
         f64.zero_()
         fn()
         torch.cuda.synchronize()
-        out = (f64 if name == "fp64_map" else f32).cpu().numpy().astype(np.float64)
+        out = (f64 if name.startswith("fp64_map") else f32).cpu().numpy().astype(np.float64)
         results[name] = {"ms": round(ms, 4), "gsamples_s": round(nsamp / (ms * 1e-3) / 1e9, 3), "out": out}
+        if name.endswith("_long_runs"):
+            results[name]["max_run_lines"] = 8 * max_run_lines
     xp_h = xp.cpu().numpy()
     tod_h = tod.cpu().numpy()
     want = np.zeros(n, np.float64)

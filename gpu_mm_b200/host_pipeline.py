@@ -179,7 +179,7 @@ class HostPipeline:
             n = nd * nt
             b_out, b_in = self._slot_batches(k, nd)
             # h2d: overwrite the slot once the compute that last read it is done.
-            h2d = self._h2d[i % 2]
+            h2d = self._h2d[i % len(self._h2d)]
             h2d.wait_event(self._free[k])
             with torch.cuda.stream(h2d):
                 xv = self._xp[k][:3 * n].view(3, nd, nt)
