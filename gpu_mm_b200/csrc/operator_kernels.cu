@@ -80,6 +80,16 @@ __device__ void tile_offsets(int64_t *tab, const Tile &T, const OpArgs &a)
     }
 }
 
+// cp.async of 16 bytes, global -> shared (L2 only), and its group bookkeeping.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const uint32_t d = (uint32_t) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template<int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Global-memory pixel offset (map_evaluator / map_accumulator addressing,
 // gpu_mm_internals.hpp:258-275), or -1 if the cell is absent.
 __device__ __forceinline__ int64_t global_pixel_offset(int iy, int ix, const OpArgs &a)
@@ -118,7 +128,7 @@ __device__ void load_tile(float *tile, const int64_t *tab, const OpArgs &a, cons
     constexpr int NG = TY * (TX / 4);   // column groups
     const bool vec_ok = ((((uintptr_t) lmap) & 15) == 0) && ((a.ystride & 3) == 0) && ((a.polstride & 3) == 0);
 #pragma unroll 4
-    for (int gi = threadIdx.x; gi < NG; gi += NT) {
+    for (int gi = threadIdx.x; gi < NG; gi += blockDim.x) {
         const int r = gi / (TX / 4), c = 4 * (gi % (TX / 4));
         const int64_t *tb = tab + (r >> 6) * TX + c;
         const int64_t b0 = tb[0];
@@ -1069,15 +1079,6 @@ __device__ __forceinline__ void band_general_sample(const OpArgs &a, float y, fl
     }
 }
 
-// cp.async of 16 bytes, global -> shared (L2 only), and its group bookkeeping.
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-    const uint32_t d = (uint32_t) __cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template<int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template<bool RESP, bool PERIODIC, int FLUSH>
 __global__ void __launch_bounds__(BNT, 2)
