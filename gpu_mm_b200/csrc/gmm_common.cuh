@@ -24,8 +24,8 @@ constexpr uint64_t kMflag = 1ull << 46;
 constexpr uint64_t kZflag = 1ull << 47;
 
 // Owner words of single-TOD plans (one per cache line: its lowest cell | line << 20 | mflag << 46)
-// carry the line's row band in bits 48-53: the row of its first sample's upper bilinear neighbours,
-// relative to the owner cell's first row, clamped to [0, 63].  The owner list is sorted by
+// carry the line's row band in bits 48-53: the lowest row of its samples' upper bilinear neighbours
+// (locate's row clamped to [0, ny - 2]), relative to the owner cell's first row, clamped to [0, 63].  The owner list is sorted by
 // (cell, band, line).
 constexpr int kBandShift = 48;
 constexpr int kBandBits = 6;
@@ -153,7 +153,7 @@ __device__ __forceinline__ void sincos2a(float alpha, float *s, float *c)
 
 // Band word of a line of a single-TOD plan (one per owner entry, stored in owner-list order): the
 // shape of the line as the tod2map band path needs it, computed once from the pointing when the
-// plan is built.  The band path accumulates a line in the rows R0, R0 + 1 and the columns
+// plan is built.  The band path accumulates a line in the rows R0 .. R0 + 2 and the columns
 // x0 + [0, 96) of its (cell, band) (R0 = 64 iycell + band, x0 = 64 ixcell); column k = floor(x) - x0.
 //   bits 0-31  bit i set iff sample i lies in the same column as sample i - 1 (i >= 1)
 //   bits 32-38 the first column in scan order, kmin (0..94)
@@ -161,22 +161,26 @@ __device__ __forceinline__ void sincos2a(float alpha, float *s, float *c)
 //   bit  45    x increases along the line (scan order = lane order; else reversed)
 //   bit  46    the line takes the band path (all conditions of band_line_word below hold)
 //   bit  47    some column holds three or four consecutive samples
+//   bit  48    the samples' upper rows are R0 and R0 + 1 (the line crosses a pixel row), not R0 only
 constexpr int kBandKminShift = 32, kBandNcolShift = 39;
-constexpr uint64_t kBandInc = 1ull << 45, kBandFast = 1ull << 46, kBandRun3 = 1ull << 47;
+constexpr uint64_t kBandInc = 1ull << 45, kBandFast = 1ull << 46, kBandRun3 = 1ull << 47, kBandTwoRows = 1ull << 48;
 
 // The band word of one cache line, by the full warp (lane = sample).  The line takes the band path
-// (bit 46) iff every sample has y in [R0, R0 + 1) with R0 <= ny - 2 (upper neighbours in row R0; no
-// clamp in locate), x in [x0, x0 + 95) and x < x_hi (nx if periodic: no fold; nx - 2 otherwise:
-// in range), and the column moves along the line in one direction by 0 or 1 per sample, stays in
-// one column for at most four consecutive samples, and repeats at least once (so the line spans at
-// most 32 columns).  dy = y - R0 and xr = x - x0 are exact; non-negative floats compare as unsigned
-// integers (negative values and NaN fail).  The word is 0 when the line does not take the path.
+// (bit 46) iff every sample has y in [R0, R0 + 2) -- upper neighbours in row R0 or R0 + 1 -- with
+// the rows inside the map (R0 <= ny - 2 if all are in R0, else R0 <= ny - 3: no clamp in locate),
+// x in [x0, x0 + 95) and x < x_hi (nx if periodic: no fold; nx - 2 otherwise: in range), and the
+// column moves along the line in one direction by 0 or 1 per sample, stays in one column for at
+// most four consecutive samples (two if the line crosses a row), and repeats at least once (so the
+// line spans at most 32 columns).  dy = y - R0 and xr = x - x0 are exact; non-negative floats
+// compare as unsigned integers (negative values and NaN fail).  The word is 0 when the line does
+// not take the path.
 __device__ __forceinline__ uint64_t band_line_word(float y, float x, int R0, int x0, int ny, float x_hi)
 {
     const int lane = threadIdx.x & 31;
     const float dy = y - (float) R0;
     const float xr = x - (float) x0;
-    const bool ok = (R0 <= ny - 2) && ((unsigned) __float_as_int(dy) < 0x3f800000u) &&
+    const bool two = __any_sync(kFullMask, (unsigned) __float_as_int(dy) >= 0x3f800000u);
+    const bool ok = (R0 <= ny - (two ? 3 : 2)) && ((unsigned) __float_as_int(dy) < 0x40000000u) &&
                     ((unsigned) __float_as_int(xr) < 0x42be0000u) &&
                     ((unsigned) __float_as_int(x) < (unsigned) __float_as_int(x_hi));
     const int k = (int) floorf(xr);
@@ -188,13 +192,13 @@ __device__ __forceinline__ uint64_t band_line_word(float y, float x, int R0, int
     const unsigned r3 = su & (su >> 1);
     const int k0 = __shfl_sync(kFullMask, k, 0), k31 = __shfl_sync(kFullMask, k, 31);
     if ((bad != 0u) || ((su | up | down) != 0xfffffffeu) || ((up != 0u) && (down != 0u)) || (su == 0u) ||
-        ((r3 & (r3 >> 2)) != 0u))
+        ((r3 & (r3 >> 2)) != 0u) || (two && (r3 != 0u)))
         return 0ull;
     const bool inc = down == 0u;
     const int kmin = inc ? k0 : k31;
     const int ncol = (inc ? k31 : k0) - kmin + 1;
     return (uint64_t) su | ((uint64_t) kmin << kBandKminShift) | ((uint64_t) ncol << kBandNcolShift) |
-           (inc ? kBandInc : 0ull) | kBandFast | ((r3 != 0u) ? kBandRun3 : 0ull);
+           (inc ? kBandInc : 0ull) | kBandFast | ((r3 != 0u) ? kBandRun3 : 0ull) | (two ? kBandTwoRows : 0ull);
 }
 
 // OR-reduce an error word over the block and publish it with one atomicOr per block (only if

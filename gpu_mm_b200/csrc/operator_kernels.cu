@@ -815,12 +815,14 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
 constexpr int BW = 12;                 // warps per CTA (2 CTAs per SM; 16 measured no faster)
 constexpr int BNT = BW * 32;
 constexpr int BP = 8;                  // line slots per warp (a power of two)
-constexpr size_t kBandSmem = (size_t) BW * BP * 128 * sizeof(float);
+constexpr int kBandRows = 3;          // accumulator rows R0 .. R0 + 2
+constexpr size_t kBandSmem = (size_t) BW * BP * 128 * sizeof(float) + (size_t) BW * 3 * kBandRows * 96 * sizeof(float);
 constexpr uint32_t kNoKey = 0xffffffffu;
 
 struct BandState {
-    float *acc;         // the warp's accumulator in shared memory: [row * 3 + plane][96 columns]
+    float *acc;         // the warp's accumulator in shared memory: [row * 3 + plane][96 columns], rows R0 + [0, 3)
     uint32_t key;       // cell | band << 20 of the accumulated lines, or kNoKey
+    bool row2;          // row R0 + 2 may hold non-zero values (a line crossing a row was added)
     int R0, x0;         // rows R0, R0 + 1; columns x0 + [0, 96) (unwrapped; mod nx with PERIODIC)
     float R0f, x0f;     // the same as floats
 };
@@ -834,31 +836,42 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
 {
     const int lane = threadIdx.x & 31;
     if constexpr (FLUSH == kFlushCompensated) {
-        // The returning atomics of all eighteen values are issued before any two-sum uses one, so
-        // that their round trips overlap (one after the other they would cost eighteen latencies).
-        int64_t off[18];
-        float old[18];
+        // Row by row: the returning atomics of a row's nine values are issued before any two-sum uses
+        // one, so that their round trips overlap (one after the other they would cost nine latencies).
 #pragma unroll
-        for (int i = 0; i < 18; i++) {
-            const int sl = i / 6, r = (i % 6) / 3, p = i % 3;
-            int gx = B.x0 + 32 * sl + lane;
-            bool xin = true;
-            if constexpr (PERIODIC)
-                gx %= a.nx;
-            else
-                xin = gx < a.nx;
-            const float v = B.acc[(3 * r + p) * 96 + 32 * sl + lane];
-            const int64_t o = (xin && (v != 0.0f)) ? global_pixel_offset(B.R0 + r, gx, a) : -1;
-            off[i] = (o >= 0) ? (o + p * a.polstride) : -1;
-            old[i] = (off[i] >= 0) ? atomicAdd(a.out + off[i], v) : 0.0f;
-        }
+        for (int r = 0; r < kBandRows; r++) {
+            if ((r == 2) && !B.row2)
+                break;
+            float v[9];
+            bool nz = false;
 #pragma unroll
-        for (int i = 0; i < 18; i++) {
-            const int sl = i / 6, r = (i % 6) / 3, p = i % 3;
-            float &v = B.acc[(3 * r + p) * 96 + 32 * sl + lane];
-            if (off[i] >= 0)
-                add_rounding_error(a, off[i], old[i], v);
-            v = 0.0f;
+            for (int i = 0; i < 9; i++) {
+                v[i] = B.acc[(3 * r + i % 3) * 96 + 32 * (i / 3) + lane];
+                nz = nz || (v[i] != 0.0f);
+            }
+            if (!__any_sync(kFullMask, nz))
+                continue;
+            int64_t off[9];
+            float old[9];
+#pragma unroll
+            for (int i = 0; i < 9; i++) {
+                const int sl = i / 3, p = i % 3;
+                int gx = B.x0 + 32 * sl + lane;
+                bool xin = true;
+                if constexpr (PERIODIC)
+                    gx %= a.nx;
+                else
+                    xin = gx < a.nx;
+                const int64_t o = (xin && (v[i] != 0.0f)) ? global_pixel_offset(B.R0 + r, gx, a) : -1;
+                off[i] = (o >= 0) ? (o + p * a.polstride) : -1;
+                old[i] = (off[i] >= 0) ? atomicAdd(a.out + off[i], v[i]) : 0.0f;
+            }
+#pragma unroll
+            for (int i = 0; i < 9; i++) {
+                if (off[i] >= 0)
+                    add_rounding_error(a, off[i], old[i], v[i]);
+                B.acc[(3 * r + i % 3) * 96 + 32 * (i / 3) + lane] = 0.0f;
+            }
         }
     } else {
 #pragma unroll
@@ -870,7 +883,9 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
             else
                 xin = gx < a.nx;
 #pragma unroll
-            for (int r = 0; r < 2; r++) {
+            for (int r = 0; r < kBandRows; r++) {
+                if ((r == 2) && !B.row2)
+                    break;
                 float *c = B.acc + 3 * r * 96 + 32 * sl + lane;
                 const float t = c[0], q = c[96], u = c[192];
                 const bool nz = (t != 0.0f) || (q != 0.0f) || (u != 0.0f);
@@ -892,6 +907,7 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
             }
         }
     }
+    B.row2 = false;
 }
 
 // One cache line (lane = sample) on the band path, whose shape the plan has analysed: 'bw' is its band
@@ -953,29 +969,50 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint64_
     // k, then k + 1) never put two lanes on one word.  (k is clamped: a plan used with pointing other
     // than its own gives wrong sums, never an access outside the accumulator.)
     const int kc = (int) min((unsigned) k, 94u);
-    if (!r3) {
-        // At most two samples per column: the last one adds the previous one's share too.  Bilinear
-        // weights per (row, column) of this sample and of the previous one.
-        const float wyp = 1.0f - dyp;
-        const float a0 = wa * wy0, a1 = wa * dy, b0 = dx * wy0, b1 = dx * dy;
-        const float pa0 = wap * wyp, pa1 = wap * dyp, pb0 = wbp * wyp, pb1 = wbp * dyp;
+    // At most two samples per column (no r3): the last one adds the previous one's share too, with
+    // the bilinear weights per (row, column) of both samples, in two rounds of read-add-writes at
+    // rows 'c' (the accumulator's rows r0, r0 + 1) and columns kc, then kc + 1.
+    auto rounds = [&](float *c, const float *ff, const float *ffp, float ry, float rdy, float ryp, float rdyp) {
+        const float a0 = wa * ry, a1 = wa * rdy, b0 = dx * ry, b1 = dx * rdy;
+        const float pa0 = wap * ryp, pa1 = wap * rdyp, pb0 = wbp * ryp, pb1 = wbp * rdyp;
         __syncwarp();
         if (last) {
-            float *c = B.acc + kc;
 #pragma unroll
             for (int p = 0; p < 3; p++) {
-                c[96 * p] = fmaf(a0, f[p], fmaf(pa0, fp[p], c[96 * p]));
-                c[96 * (3 + p)] = fmaf(a1, f[p], fmaf(pa1, fp[p], c[96 * (3 + p)]));
+                c[kc + 96 * p] = fmaf(a0, ff[p], fmaf(pa0, ffp[p], c[kc + 96 * p]));
+                c[kc + 96 * (3 + p)] = fmaf(a1, ff[p], fmaf(pa1, ffp[p], c[kc + 96 * (3 + p)]));
             }
         }
         __syncwarp();
         if (last) {
-            float *c = B.acc + kc + 1;
 #pragma unroll
             for (int p = 0; p < 3; p++) {
-                c[96 * p] = fmaf(b0, f[p], fmaf(pb0, fp[p], c[96 * p]));
-                c[96 * (3 + p)] = fmaf(b1, f[p], fmaf(pb1, fp[p], c[96 * (3 + p)]));
+                c[kc + 1 + 96 * p] = fmaf(b0, ff[p], fmaf(pb0, ffp[p], c[kc + 1 + 96 * p]));
+                c[kc + 1 + 96 * (3 + p)] = fmaf(b1, ff[p], fmaf(pb1, ffp[p], c[kc + 1 + 96 * (3 + p)]));
             }
+        }
+    };
+    if (!r3) {
+        if (!(bw & kBandTwoRows)) {
+            rounds(B.acc, f, fp, wy0, dy, 1.0f - dyp, dyp);
+            return true;
+        }
+        B.row2 = true;
+        // The line crosses a pixel row: samples with upper row R0 + 1 (dy >= 1) go to the
+        // accumulator's rows 1, 2 in a second pass, each pass with the other row's samples at zero
+        // (the columns' runs are the same in both passes).  dy - 1 is exact for dy in [1, 2).
+        const bool row1 = dy >= 1.0f;
+        const float dyl = row1 ? dy - 1.0f : dy;
+        const float dylp = __shfl_sync(kFullMask, dyl, src);
+#pragma unroll
+        for (int pass = 0; pass < 2; pass++) {
+            float fm[3], fmp[3];
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                fm[p] = (row1 == (pass == 1)) ? f[p] : 0.0f;
+                fmp[p] = __shfl_sync(kFullMask, fm[p], src);
+            }
+            rounds(B.acc + 3 * 96 * pass, fm, fmp, 1.0f - dyl, dyl, 1.0f - dylp, dylp);
         }
         return true;
     }
@@ -1085,8 +1122,7 @@ __global__ void __launch_bounds__(BNT, 2)
 planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner,
                      const uint32_t *__restrict__ cellmap, const uint64_t *__restrict__ band)
 {
-    extern __shared__ float s_lines[];    // [BW][BP][4 rows][32]: y, x, alpha, TOD
-    __shared__ float s_acc[BW][6 * 96];
+    extern __shared__ __align__(16) float s_lines[];   // [BW][BP][4 rows][32] (y, x, alpha, TOD), then accumulators
     __shared__ uint32_t s_wline[BW][64], s_wkey[BW][64];
     __shared__ uint64_t s_wbw[BW][64];
     __shared__ uint32_t s_err[BW];
@@ -1104,11 +1140,12 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
     const float *__restrict__ src_row = (row < 3) ? (a.xp + (size_t) row * nsamp) : a.in;
 
     BandState B;
-    B.acc = s_acc[warp];
-    for (int i = lane; i < 6 * 96; i += 32)
+    B.acc = s_lines + (size_t) BW * BP * 128 + (size_t) warp * 3 * kBandRows * 96;
+    for (int i = lane; i < 3 * kBandRows * 96; i += 32)
         B.acc[i] = 0.0f;
     __syncwarp();
     B.key = kNoKey;
+    B.row2 = false;
     B.R0 = 0;
     B.x0 = 0;
     B.R0f = 0.0f;

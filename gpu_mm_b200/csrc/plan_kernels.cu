@@ -253,13 +253,14 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
 #pragma unroll
             for (int k = 0; k < 6; k++)
                 s_slots[li][k][lane] = ls.slots[k];
+            // Lowest upper footprint row of the line's samples (locate's clamp to [0, ny-2]).
+            const int brow = __reduce_min_sync(kFullMask, min(max(__float2int_rz(y[j]), 0), ny - 2));
             if (lane == 0) {
 #pragma unroll
                 for (int k = 0; k < 6; k++)
                     s_amask[li][k] = ls.amask[k];
                 s_cnt[li] = cnt;
-                // Upper footprint row of the line's first sample (locate's clamp to [0, ny-2]).
-                s_brow[li] = min(max(__float2int_rz(y[j]), 0), ny - 2);
+                s_brow[li] = brow;
             }
         }
         __syncthreads();
@@ -321,7 +322,7 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
                 pos += __popc(am);
             }
             minc = __reduce_min_sync(kFullMask, minc);
-            // Row band: the first sample's row within the owner cell's tile rows, clamped to [0, 63].
+            // Row band: the line's lowest row within the owner cell's rows, clamped to [0, 63].
             const int band = min(max(s_brow[li] - (int) ((minc >> 10) << 6), 0), 63);
             const uint64_t bw = band_line_word(y[j], x[j], (int) ((minc >> 10) << 6) + band, (int) ((minc & 1023u) << 6),
                                                ny, periodic ? (float) nx : (float) (nx - 2));

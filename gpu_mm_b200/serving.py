@@ -124,6 +124,7 @@ class PointingServer:
         self.latencies = {"plan": [], "map2tod": [], "tod2map": []}
         self.samples_done = 0
         self.launches = 0
+        self.direct_launches = 0                           # launches made by submit() on an idle server
         self.evictions = 0
         self.iterations = []                               # (requests launched, host seconds)
         self.errors = []
@@ -164,6 +165,7 @@ class PointingServer:
             idle = not (self._submitted or self._waiting or self._launching or self._stop)
             if idle and self._launch_mutex.acquire(blocking=False):
                 direct = True
+                self.direct_launches += 1
                 self._waiting.append(req)
                 self._take_freed()
                 self._launching = True
@@ -227,6 +229,7 @@ class PointingServer:
             out["all"] = {"n": len(allv), "p50_ms": round(float(np.percentile(a, 50)), 3),
                           "p99_ms": round(float(np.percentile(a, 99)), 3)}
         out["launches"] = self.launches
+        out["direct_launches"] = self.direct_launches
         out["evictions"] = self.evictions
         if self.iterations:
             it = np.asarray(self.iterations, dtype=np.float64)

@@ -400,7 +400,7 @@ def owner_words(xpointing, nypix_global, mt, owner_bits):
     One word per cache line: the line's lowest cell | line << 20 | mflag << 46 | band << 48, sorted
     stably by (cell, band), i.e. in (cell, band, line) order.  'mt' and 'owner_bits' are plan()'s
     outputs (the owner bit marks the first mt word of each line in (cell, line) order, which is the
-    line's lowest cell).  The band is the upper bilinear row of the line's first sample (locate's
+    line's lowest cell).  The band is the lowest upper bilinear row of the line's samples (locate's
     clamp of trunc(y) to [0, ny-2]) minus 64 * iycell of the owner, clamped to [0, 63]."""
     xp = np.ascontiguousarray(xpointing, dtype=np.float32)
     n = _nsamp(xp)
@@ -408,9 +408,9 @@ def owner_words(xpointing, nypix_global, mt, owner_bits):
     bits = np.unpackbits(np.asarray(owner_bits).view(np.uint8), bitorder="little")[:len(mt)].astype(bool)
     words = mt[bits] & np.uint64((1 << 47) - 1)          # cell, line, mflag (no zflag)
     lines = ((words >> np.uint64(20)) & np.uint64((1 << 26) - 1)).astype(np.int64)
-    y = xp.reshape(3, n)[0][32 * lines].astype(np.float64)
+    y = xp.reshape(3, n)[0][32 * lines[:, None] + np.arange(32)[None, :]].astype(np.float64)
     y = np.nan_to_num(y, nan=0.0, posinf=float(nypix_global), neginf=-1.0)
-    iy0 = np.clip(np.trunc(np.clip(y, -1.0, float(nypix_global))), 0, nypix_global - 2).astype(np.int64)
+    iy0 = np.clip(np.trunc(np.clip(y, -1.0, float(nypix_global))), 0, nypix_global - 2).astype(np.int64).min(axis=1)
     iyc = ((words >> np.uint64(10)) & np.uint64(1023)).astype(np.int64)
     band = np.clip(iy0 - 64 * iyc, 0, 63).astype(np.uint64)
     words = words | (band << np.uint64(48))
@@ -423,8 +423,8 @@ def band_words(xpointing, nypix_global, nxpix_global, periodic_xcoord, owner):
     gives it), as the plan builder must produce them (this implementation's own addition to the plan;
     no reference counterpart).  Bits: 0-31 same column as the previous sample; 32-38 first column in
     scan order, relative to the owner cell's x0; 39-44 number of columns; 45 x increases; 46 the line
-    takes the tod2map band path; 47 some column holds three or four consecutive samples.  Zero for
-    lines off that path."""
+    takes the tod2map band path; 47 some column holds three or four consecutive samples; 48 the
+    samples' upper rows are R0 and R0 + 1 (not R0 only).  Zero for lines off that path."""
     xp = np.ascontiguousarray(xpointing, dtype=np.float32)
     n = _nsamp(xp)
     owner = np.asarray(owner, dtype=np.uint64)
@@ -442,7 +442,9 @@ def band_words(xpointing, nypix_global, nxpix_global, periodic_xcoord, owner):
     # Range checks on the float bit patterns as unsigned integers, as the builder does: negative
     # values (-0.0 included) and NaN fail.
     bits = lambda v: np.ascontiguousarray(v, dtype=np.float32).view(np.uint32)
-    ok = ((R0[:, None] <= nypix_global - 2) & (bits(dy) < bits(np.float32(1.0))) & (bits(xr) < bits(np.float32(95.0)))
+    two = (bits(dy) >= bits(np.float32(1.0))).any(axis=1)
+    rmax = np.where(two, nypix_global - 3, nypix_global - 2)
+    ok = ((R0 <= rmax)[:, None] & (bits(dy) < bits(np.float32(2.0))) & (bits(xr) < bits(np.float32(95.0)))
           & (bits(x) < bits(x_hi)))
     k = np.floor(np.where(ok, xr, np.float32(0))).astype(np.int64)
     dk = np.diff(k, axis=1)
@@ -452,13 +454,13 @@ def band_words(xpointing, nypix_global, nxpix_global, periodic_xcoord, owner):
     down = ((dk == -1) * bit).sum(axis=1, dtype=np.uint64)
     r3 = su & (su >> np.uint64(1))
     fast = (ok.all(axis=1) & ((su | up | down) == np.uint64(0xFFFFFFFE)) & ~((up != 0) & (down != 0)) & (su != 0)
-            & ((r3 & (r3 >> np.uint64(2))) == 0))
+            & ((r3 & (r3 >> np.uint64(2))) == 0) & ~(two & (r3 != 0)))
     inc = down == 0
     kmin = np.where(inc, k[:, 0], k[:, 31])
     ncol = np.where(inc, k[:, 31], k[:, 0]) - kmin + 1
     w = (su | (kmin.astype(np.uint64) << np.uint64(32)) | (ncol.astype(np.uint64) << np.uint64(39))
          | (inc.astype(np.uint64) << np.uint64(45)) | (np.uint64(1) << np.uint64(46))
-         | ((r3 != 0).astype(np.uint64) << np.uint64(47)))
+         | ((r3 != 0).astype(np.uint64) << np.uint64(47)) | (two.astype(np.uint64) << np.uint64(48)))
     return np.where(fast, w, np.uint64(0))
 
 

@@ -208,3 +208,31 @@ def test_serving_waits_for_the_callers_stream(g):
     oracle.map2tod(want_t, m, xps[2], lp_o)
     rl1, mx = rel_stats(r.cpu().numpy(), want_t)
     assert rl1 < RL1_TOL and mx < MAX_TOL, (rl1, mx)
+
+
+def test_serving_idle_fast_path_and_batching(g):
+    """A request submitted to an idle server is launched by submit() itself (no wait for the worker);
+    a burst submitted at once is batched by the worker (fewer launches than requests); every map2tod
+    result equals the plain planned operator's."""
+    import torch
+    ny, nx = 256, 512
+    rng, xps, tods = pool(31, n=6)
+    lp = g.LocalPixelization.make_rectangle(ny, nx, True)
+    xg = {i: torch.from_numpy(x).cuda() for i, x in xps.items()}
+    m = torch.from_numpy(rng.standard_normal(3 * lp.npix).astype(np.float32)).cuda()
+    srv = g.PointingServer(xg, m, torch.zeros(3 * lp.npix, device="cuda"), lp, hbm_budget_bytes=1 << 30)
+    try:
+        r0 = srv.submit("map2tod", 0).result(timeout=30)
+        assert srv.direct_launches == 1
+        srv.drain()
+        futs = [(i % 6, srv.submit("map2tod", i % 6)) for i in range(24)]
+        outs = [(i, f.result(timeout=30)) for i, f in futs]
+        assert srv.launches < 1 + 24
+        srv.check()
+    finally:
+        srv.close()
+    lmap = g.LocalMap(lp, m)
+    for i, r in [(0, r0)] + outs:
+        alone = torch.empty(xps[i].shape[1:], device="cuda")
+        g.map2tod(alone, lmap, xg[i], g.PointingPlan(g.PointingPrePlan(xg[i], ny, nx), xg[i]))
+        assert torch.equal(r, alone)

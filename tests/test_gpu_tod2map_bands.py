@@ -2,8 +2,9 @@
 shared-memory tiles -- and unplanned tod2map against the oracle, on scans chosen to reach every
 branch of the band path and of the unplanned line path:
 scan speeds giving one to four samples per pixel column and more (which the band path leaves to
-its per-sample route), both scan directions, turnarounds, x wraparound, lines that drift across a
-pixel row, absent cells, and the per-detector response.
+its per-sample route), both scan directions, turnarounds, x wraparound, lines that cross a pixel
+row (the band path's two-row pass, y increasing and decreasing), absent cells, and the
+per-detector response.
 
 Tolerances are those of the other parity tests: rel-L1 < 1e-6 (the reference's metric,
 tests.py:220-224) and max|a-b| / max|b| < 1e-5.
@@ -49,7 +50,7 @@ def bounce_scan(rng, ndet, nt, ny, nx, periodic, speed, ydrift, spacing=2.0):
     t = np.arange(nt, dtype=np.float64)
     L = nx - 3.0 - spacing * ndet
     xp = np.zeros((3, ndet, nt))
-    y0 = rng.uniform(1.0, ny - 3.0 - abs(ydrift) * nt - 0.37 * ndet)
+    y0 = rng.uniform(1.0, ny - 3.0 - abs(ydrift) * nt - 0.37 * ndet) + max(0.0, -ydrift) * nt
     ph = rng.uniform(0, 2 * L)
     for d in range(ndet):
         x = np.abs(np.remainder(speed * t + ph, 2 * L) - L) + spacing * d
@@ -71,6 +72,8 @@ CASES = [
     (0.99, 0.0, True, 128, 600),
     (1.6, 0.0, True, 128, 600),        # faster than a pixel per sample: per-sample route
     (0.18, 0.0, True, 128, 256),       # five or more per column: per-sample route
+    (0.7, 0.02, True, 400, 1024),      # y drifts 0.64 px per line: most lines cross a pixel row
+    (0.6, -0.015, False, 400, 700),    # the same, y decreasing
 ]
 
 
@@ -83,6 +86,9 @@ def test_bands_vs_tiles_vs_oracle(g, kernel_knob, case):
     xg = torch.from_numpy(xp).cuda()
     pp = g.PointingPrePlan(xg, ny, nx, periodic_xcoord=periodic)
     plan = g.PointingPlan(pp, xg)
+    if abs(ydrift) >= 0.01:
+        bw = plan._get_band_words()
+        assert np.mean((bw >> np.uint64(48)) & np.uint64(1)) > 0.3   # lines on the two-row band path
     lp = g.LocalPixelization.make_rectangle(ny, nx, periodic)
     lp_o = oracle.Lpix.rectangle(ny, nx, periodic)
     t = rng.standard_normal(xp.shape[1:]).astype(np.float32)
