@@ -183,3 +183,42 @@ def test_absent_cell_in_every_cell_row(g, kernel_knob):
             g.map2tod(torch.zeros(xp.shape[1:], device="cuda"), g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda")),
                       xg, plan, partial_pixelization=False)
 
+
+
+def test_bands_response_on_row_crossing_lines(g, kernel_knob):
+    """The per-detector response on the band path's two-row pass (y drifting 0.64 px per line), both
+    kernels, and the precision modes on the same lines, against the oracle."""
+    import torch
+    rng = np.random.default_rng(17)
+    ny, nx, periodic = 400, 1024, True
+    xp = bounce_scan(rng, 12, 4096, ny, nx, periodic, 0.7, 0.02)
+    xg = torch.from_numpy(xp).cuda()
+    pp = g.PointingPrePlan(xg, ny, nx, periodic_xcoord=periodic)
+    plan = g.PointingPlan(pp, xg)
+    bw = plan._get_band_words()
+    assert np.mean((bw >> np.uint64(48)) & np.uint64(1)) > 0.3
+    lp = g.LocalPixelization.make_rectangle(ny, nx, periodic)
+    lp_o = oracle.Lpix.rectangle(ny, nx, periodic)
+    t = rng.standard_normal(xp.shape[1:]).astype(np.float32)
+    tg = torch.from_numpy(t).cuda()
+    resp = rng.uniform(0.5, 1.5, size=(2, 12)).astype(np.float32)
+    want_r = np.zeros(3 * lp.npix, np.float32)
+    oracle.response_tod2map(want_r, t, xp, resp, lp_o, False)
+    want = np.zeros(3 * lp.npix, np.float32)
+    oracle.tod2map(want, t, xp, lp_o)
+    for which in KERNELS:
+        kernel_knob(which)
+        out = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+        g.tod2map(out, tg, xg, plan, response=torch.from_numpy(resp).cuda())
+        rl1, mx = rel_stats(out.arr.cpu().numpy(), want_r)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, ("response", which, rl1, mx)
+        out = g.LocalMap(lp, torch.zeros(3 * lp.npix, device="cuda"))
+        comp = torch.zeros(3 * lp.npix, device="cuda")
+        g.tod2map_compensated(out, comp, tg, xg, plan, max_run_lines=5)
+        g.fold_compensation(out, comp)
+        rl1, mx = rel_stats(out.arr.cpu().numpy(), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, ("compensated", which, rl1, mx)
+        m64 = torch.zeros(3 * lp.npix, dtype=torch.float64, device="cuda")
+        g.tod2map_f64(m64, lp, tg, xg, plan, max_run_lines=5)
+        rl1, mx = rel_stats(m64.cpu().numpy().astype(np.float32), want)
+        assert rl1 < RL1_TOL and mx < MAX_TOL, ("float64", which, rl1, mx)
