@@ -196,10 +196,17 @@ def cpu_baseline(ndet_rows):
     nsamp = xp.size // 3
     cpu_reference_run(xp, tod, m, lp, nthreads, use_ref)   # warm
     dt = min(cpu_reference_run(xp, tod, m, lp, nthreads, use_ref) for _ in range(3))
+    # The reference's operators as it runs them (single-threaded, gpu_mm.hpp:227-228), on one core:
+    # the first 64 detectors (2^24 samples).
+    xp1, tod1, m1, lp1 = cpu_sample(64, ndet_rows)
+    n1 = xp1.size // 3
+    dt1 = min(cpu_reference_run(xp1, tod1, m1, lp1, 1, use_ref) for _ in range(2))
     return {"value": round(nsamp / dt / 1e9, 4), "unit": "Gsamples/s", "cores": nthreads,
             "kind": "reference" if use_ref else "port",
             "sample": f"{ndet} detectors ({nsamp} samples), map2tod + tod2map, "
-                      f"best of 3, {nthreads} threads"}
+                      f"best of 3, {nthreads} threads",
+            "single_core": {"value": round(n1 / dt1 / 1e9, 4), "unit": "Gsamples/s", "cores": 1,
+                            "sample": f"the first 64 detectors ({n1} samples), map2tod + tod2map, best of 2"}}
 
 
 def run_reference_arm(args):
