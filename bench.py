@@ -960,7 +960,8 @@ def main():
             "roofline": {"bound": "hbm", "kernel": f"planned_{dom}", "achieved": round(achieved, 1),
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
-                         "per_unit": "16 B/sample + 12 B/hit pixel (map2tod) or 24 B/hit pixel (tod2map)"},
+                         "per_unit": "16 B/sample + 12 B/hit pixel (map2tod) or 24 B/hit pixel (tod2map)",
+                         "frac_of_nominal_8tbs": round(achieved / 8000.0, 4)},
             "rooflines": per_kernel,
             "kernels_ms": {"planned_map2tod": round(m2t_ms, 4), "planned_tod2map": round(t2m_ms, 4),
                            **unplanned, "plan_build": round(statistics.mean(plan_ms), 4),
