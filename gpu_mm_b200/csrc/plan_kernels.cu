@@ -250,15 +250,23 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
                 }
             }
             const int li = warp * kLinesPerWarp + j;
+            // A line with one (cell, line) pair keeps only its cell (slot 0 at lane 0); the others
+            // keep their whole slot analysis.
+            if (cnt != 1) {
 #pragma unroll
-            for (int k = 0; k < 6; k++)
-                s_slots[li][k][lane] = ls.slots[k];
+                for (int k = 0; k < 6; k++)
+                    s_slots[li][k][lane] = ls.slots[k];
+            }
             // Lowest upper footprint row of the line's samples (locate's clamp to [0, ny-2]).
             const int brow = __reduce_min_sync(kFullMask, min(max(__float2int_rz(y[j]), 0), ny - 2));
             if (lane == 0) {
+                if (cnt != 1) {
 #pragma unroll
-                for (int k = 0; k < 6; k++)
-                    s_amask[li][k] = ls.amask[k];
+                    for (int k = 0; k < 6; k++)
+                        s_amask[li][k] = ls.amask[k];
+                } else {
+                    s_slots[li][0][0] = ls.slots[0];
+                }
                 s_cnt[li] = cnt;
                 s_brow[li] = brow;
             }
@@ -304,24 +312,32 @@ plan_emit_kernel(const float *__restrict__ xp, int64_t nsamp, int ny, int nx, bo
             const int cnt = s_cnt[li];
             const bool mflag = (cnt > 1);
             const uint64_t hi = ((uint64_t) l << 20) | (mflag ? kMflag : 0ull);
-            int pos = 0;
-            unsigned minc = 0xffffffffu;
+            unsigned minc;
+            if (cnt == 1) {
+                // One word, at lane 0: no mflag, so no zflag.
+                minc = (unsigned) s_slots[li][0][0];
+                if ((lane == 0) && (base < nmax))
+                    out[base] = (uint64_t) minc | hi;
+            } else {
+                int pos = 0;
+                minc = 0xffffffffu;
 #pragma unroll
-            for (int k = 0; k < 6; k++) {
-                const unsigned am = s_amask[li][k];
-                if ((am >> lane) & 1u) {
-                    const int rank = __popc(am & lt);
-                    const int64_t p = base + pos + rank;
-                    const bool zflag = mflag && (rank == 0) && (fill + pos < 32);
-                    const int slot = s_slots[li][k][lane];
-                    const uint64_t word = (uint64_t) (unsigned) slot | hi | (zflag ? kZflag : 0ull);
-                    if (p < nmax)
-                        out[p] = word;
-                    minc = min(minc, (unsigned) slot);
+                for (int k = 0; k < 6; k++) {
+                    const unsigned am = s_amask[li][k];
+                    if ((am >> lane) & 1u) {
+                        const int rank = __popc(am & lt);
+                        const int64_t p = base + pos + rank;
+                        const bool zflag = mflag && (rank == 0) && (fill + pos < 32);
+                        const int slot = s_slots[li][k][lane];
+                        const uint64_t word = (uint64_t) (unsigned) slot | hi | (zflag ? kZflag : 0ull);
+                        if (p < nmax)
+                            out[p] = word;
+                        minc = min(minc, (unsigned) slot);
+                    }
+                    pos += __popc(am);
                 }
-                pos += __popc(am);
+                minc = __reduce_min_sync(kFullMask, minc);
             }
-            minc = __reduce_min_sync(kFullMask, minc);
             // Row band: the line's lowest row within the owner cell's rows, clamped to [0, 63].
             const int band = min(max(s_brow[li] - (int) ((minc >> 10) << 6), 0), 63);
             const uint64_t bw = band_line_word(y[j], x[j], (int) ((minc >> 10) << 6) + band, (int) ((minc & 1023u) << 6),
