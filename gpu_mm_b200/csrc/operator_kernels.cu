@@ -820,12 +820,16 @@ constexpr size_t kBandSmem = (size_t) BW * BP * 128 * sizeof(float) + (size_t) B
 constexpr uint32_t kNoKey = 0xffffffffu;
 
 struct BandState {
-    float *acc;         // the warp's accumulator in shared memory: [row * 3 + plane][96 columns], rows R0 + [0, 3)
+    float *acc;         // the warp's accumulator in shared memory, rows R0 + [0, 3) (acc_tq, acc_u)
     uint32_t key;       // cell | band << 20 of the accumulated lines, or kNoKey
     bool row2;          // row R0 + 2 may hold non-zero values (a line crossing a row was added)
     int R0, x0;         // rows R0, R0 + 1; columns x0 + [0, 96) (unwrapped; mod nx with PERIODIC)
     float R0f, x0f;     // the same as floats
 };
+
+// Accumulator layout, per row r (288 floats): the (T, Q) pairs of the 96 columns, then their U.
+__device__ __forceinline__ float2 *acc_tq(float *acc, int r, int c) { return reinterpret_cast<float2 *>(acc + 288 * r) + c; }
+__device__ __forceinline__ float *acc_u(float *acc, int r, int c) { return acc + 288 * r + 192 + c; }
 
 // Adds the accumulator into the map (one addition per non-zero pixel and plane, in flush mode FLUSH)
 // and clears it.
@@ -845,10 +849,15 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
             float v[9];
             bool nz = false;
 #pragma unroll
-            for (int i = 0; i < 9; i++) {
-                v[i] = B.acc[(3 * r + i % 3) * 96 + 32 * (i / 3) + lane];
-                nz = nz || (v[i] != 0.0f);
+            for (int sl = 0; sl < 3; sl++) {
+                const float2 tq = *acc_tq(B.acc, r, 32 * sl + lane);
+                v[3 * sl] = tq.x;
+                v[3 * sl + 1] = tq.y;
+                v[3 * sl + 2] = *acc_u(B.acc, r, 32 * sl + lane);
             }
+#pragma unroll
+            for (int i = 0; i < 9; i++)
+                nz = nz || (v[i] != 0.0f);
             if (!__any_sync(kFullMask, nz))
                 continue;
             int64_t off[9];
@@ -867,10 +876,13 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
                 old[i] = (off[i] >= 0) ? atomicAdd(a.out + off[i], v[i]) : 0.0f;
             }
 #pragma unroll
-            for (int i = 0; i < 9; i++) {
+            for (int i = 0; i < 9; i++)
                 if (off[i] >= 0)
                     add_rounding_error(a, off[i], old[i], v[i]);
-                B.acc[(3 * r + i % 3) * 96 + 32 * (i / 3) + lane] = 0.0f;
+#pragma unroll
+            for (int sl = 0; sl < 3; sl++) {
+                *acc_tq(B.acc, r, 32 * sl + lane) = make_float2(0.0f, 0.0f);
+                *acc_u(B.acc, r, 32 * sl + lane) = 0.0f;
             }
         }
     } else {
@@ -886,8 +898,10 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
             for (int r = 0; r < kBandRows; r++) {
                 if ((r == 2) && !B.row2)
                     break;
-                float *c = B.acc + 3 * r * 96 + 32 * sl + lane;
-                const float t = c[0], q = c[96], u = c[192];
+                float2 *ctq = acc_tq(B.acc, r, 32 * sl + lane);
+                float *cu = acc_u(B.acc, r, 32 * sl + lane);
+                const float2 tq = *ctq;
+                const float t = tq.x, q = tq.y, u = *cu;
                 const bool nz = (t != 0.0f) || (q != 0.0f) || (u != 0.0f);
                 if (__any_sync(kFullMask, nz) && nz && xin) {
                     if constexpr (FLUSH == kFlushHotF64) {
@@ -901,9 +915,8 @@ __device__ __forceinline__ void band_flush(const OpArgs &a, BandState &B)
                         }
                     }
                 }
-                c[0] = 0.0f;
-                c[96] = 0.0f;
-                c[192] = 0.0f;
+                *ctq = make_float2(0.0f, 0.0f);
+                *cu = 0.0f;
             }
         }
     }
@@ -977,19 +990,31 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint64_
         const float pa0 = wap * ryp, pa1 = wap * rdyp, pb0 = wbp * ryp, pb1 = wbp * rdyp;
         __syncwarp();
         if (last) {
-#pragma unroll
-            for (int p = 0; p < 3; p++) {
-                c[kc + 96 * p] = fmaf(a0, ff[p], fmaf(pa0, ffp[p], c[kc + 96 * p]));
-                c[kc + 96 * (3 + p)] = fmaf(a1, ff[p], fmaf(pa1, ffp[p], c[kc + 96 * (3 + p)]));
-            }
+            float2 *t0 = acc_tq(c, 0, kc), *t1 = acc_tq(c, 1, kc);
+            float *u0 = acc_u(c, 0, kc), *u1 = acc_u(c, 1, kc);
+            float2 v0 = *t0, v1 = *t1;
+            v0.x = fmaf(a0, ff[0], fmaf(pa0, ffp[0], v0.x));
+            v0.y = fmaf(a0, ff[1], fmaf(pa0, ffp[1], v0.y));
+            v1.x = fmaf(a1, ff[0], fmaf(pa1, ffp[0], v1.x));
+            v1.y = fmaf(a1, ff[1], fmaf(pa1, ffp[1], v1.y));
+            *u0 = fmaf(a0, ff[2], fmaf(pa0, ffp[2], *u0));
+            *u1 = fmaf(a1, ff[2], fmaf(pa1, ffp[2], *u1));
+            *t0 = v0;
+            *t1 = v1;
         }
         __syncwarp();
         if (last) {
-#pragma unroll
-            for (int p = 0; p < 3; p++) {
-                c[kc + 1 + 96 * p] = fmaf(b0, ff[p], fmaf(pb0, ffp[p], c[kc + 1 + 96 * p]));
-                c[kc + 1 + 96 * (3 + p)] = fmaf(b1, ff[p], fmaf(pb1, ffp[p], c[kc + 1 + 96 * (3 + p)]));
-            }
+            float2 *t0 = acc_tq(c, 0, kc + 1), *t1 = acc_tq(c, 1, kc + 1);
+            float *u0 = acc_u(c, 0, kc + 1), *u1 = acc_u(c, 1, kc + 1);
+            float2 v0 = *t0, v1 = *t1;
+            v0.x = fmaf(b0, ff[0], fmaf(pb0, ffp[0], v0.x));
+            v0.y = fmaf(b0, ff[1], fmaf(pb0, ffp[1], v0.y));
+            v1.x = fmaf(b1, ff[0], fmaf(pb1, ffp[0], v1.x));
+            v1.y = fmaf(b1, ff[1], fmaf(pb1, ffp[1], v1.y));
+            *u0 = fmaf(b0, ff[2], fmaf(pb0, ffp[2], *u0));
+            *u1 = fmaf(b1, ff[2], fmaf(pb1, ffp[2], *u1));
+            *t0 = v0;
+            *t1 = v1;
         }
     };
     if (!r3) {
@@ -1012,7 +1037,7 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint64_
                 fm[p] = (row1 == (pass == 1)) ? f[p] : 0.0f;
                 fmp[p] = __shfl_sync(kFullMask, fm[p], src);
             }
-            rounds(B.acc + 3 * 96 * pass, fm, fmp, 1.0f - dyl, dyl, 1.0f - dylp, dylp);
+            rounds(B.acc + 288 * pass, fm, fmp, 1.0f - dyl, dyl, 1.0f - dylp, dylp);
         }
         return true;
     }
@@ -1039,17 +1064,23 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint64_
     }
     __syncwarp();
     if (last) {
-        float *c = B.acc + kc;
-#pragma unroll
-        for (int p = 0; p < 6; p++)
-            c[96 * p] += SA[p];
+        float2 *t0 = acc_tq(B.acc, 0, kc), *t1 = acc_tq(B.acc, 1, kc);
+        float2 v0 = *t0, v1 = *t1;
+        v0.x += SA[0]; v0.y += SA[1]; v1.x += SA[3]; v1.y += SA[4];
+        *acc_u(B.acc, 0, kc) += SA[2];
+        *acc_u(B.acc, 1, kc) += SA[5];
+        *t0 = v0;
+        *t1 = v1;
     }
     __syncwarp();
     if (last) {
-        float *c = B.acc + kc + 1;
-#pragma unroll
-        for (int p = 0; p < 6; p++)
-            c[96 * p] += SB[p];
+        float2 *t0 = acc_tq(B.acc, 0, kc + 1), *t1 = acc_tq(B.acc, 1, kc + 1);
+        float2 v0 = *t0, v1 = *t1;
+        v0.x += SB[0]; v0.y += SB[1]; v1.x += SB[3]; v1.y += SB[4];
+        *acc_u(B.acc, 0, kc + 1) += SB[2];
+        *acc_u(B.acc, 1, kc + 1) += SB[5];
+        *t0 = v0;
+        *t1 = v1;
     }
     return true;
 }
