@@ -326,6 +326,28 @@ __device__ __forceinline__ float tile_eval(const float *tile, int p, float ct, f
     return bilinear(dy, dx, e00, e01, e10, e11);
 }
 
+// tile_eval without a response for two samples at tile offsets p0, p1, with packed float pairs: the
+// same operations in the same order, so the same bits as two tile_eval calls.
+__device__ __forceinline__ float2 tile_eval2(const float *tile, int p0, int p1, float2 cq, float2 cu, float2 dy,
+                                             float2 dx)
+{
+    const float *a = tile + p0, *b = tile + p1;
+    float2 e[4];
+    const int off[4] = {0, 1, TS, TS + 1};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int o = off[i];
+        e[i] = __ffma2_rn(cu, make_float2(a[o + 2 * PS], b[o + 2 * PS]),
+                          __ffma2_rn(cq, make_float2(a[o + PS], b[o + PS]), make_float2(a[o], b[o])));
+    }
+    const float2 m1 = make_float2(-1.0f, -1.0f), one = make_float2(1.0f, 1.0f);
+    const float2 wy0 = __ffma2_rn(dy, m1, one), wx0 = __ffma2_rn(dx, m1, one);
+    float2 r = __fmul2_rn(__fmul2_rn(wy0, wx0), e[0]);
+    r = __ffma2_rn(__fmul2_rn(wy0, dx), e[1], r);
+    r = __ffma2_rn(__fmul2_rn(dy, wx0), e[2], r);
+    return __ffma2_rn(__fmul2_rn(dy, dx), e[3], r);
+}
+
 // Response factors of a sample as (ct, cq, cu) = (t_resp, p_resp cos 2a, p_resp sin 2a), or
 // (1, cos 2a, sin 2a) without a response.
 template<bool RESP>
@@ -756,11 +778,22 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
             if (__all_sync(kFullMask, fast || !ok)) {
                 if (ok) {
                     float r[4];
+                    if constexpr (RESP) {
 #pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        float ct, cq, cu;
-                        sample_factors<RESP>(a, s0 + k, S[k].sn, S[k].cs, ct, cq, cu);
-                        r[k] = tv[k] + tile_eval<RESP>(tile, S[k].p, ct, cq, cu, S[k].dy, S[k].dx);
+                        for (int k = 0; k < 4; k++) {
+                            float ct, cq, cu;
+                            sample_factors<RESP>(a, s0 + k, S[k].sn, S[k].cs, ct, cq, cu);
+                            r[k] = tv[k] + tile_eval<RESP>(tile, S[k].p, ct, cq, cu, S[k].dy, S[k].dx);
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; k += 2) {
+                            const float2 e = tile_eval2(tile, S[k].p, S[k + 1].p, make_float2(S[k].cs, S[k + 1].cs),
+                                                        make_float2(S[k].sn, S[k + 1].sn), make_float2(S[k].dy, S[k + 1].dy),
+                                                        make_float2(S[k].dx, S[k + 1].dx));
+                            r[k] = tv[k] + e.x;
+                            r[k + 1] = tv[k + 1] + e.y;
+                        }
                     }
                     __stcs(reinterpret_cast<float4 *>(ob + s0), make_float4(r[0], r[1], r[2], r[3]));
                 }
@@ -984,37 +1017,33 @@ __device__ __forceinline__ bool band_line(const OpArgs &a, BandState &B, uint64_
     const int kc = (int) min((unsigned) k, 94u);
     // At most two samples per column (no r3): the last one adds the previous one's share too, with
     // the bilinear weights per (row, column) of both samples, in two rounds of read-add-writes at
-    // rows 'c' (the accumulator's rows r0, r0 + 1) and columns kc, then kc + 1.
-    auto rounds = [&](float *c, const float *ff, const float *ffp, float ry, float rdy, float ryp, float rdyp) {
-        const float a0 = wa * ry, a1 = wa * rdy, b0 = dx * ry, b1 = dx * rdy;
-        const float pa0 = wap * ryp, pa1 = wap * rdyp, pb0 = wbp * ryp, pb1 = wbp * rdyp;
+    // rows 'c' (the accumulator's rows r0, r0 + 1) and columns kc, then kc + 1.  The (T, Q) pair of a
+    // pixel moves through the packed float-pair instructions (one fma.rn.f32x2 for two fmaf, the same
+    // rounding), as do the row weights.
+    auto rounds =[&](float *c, const float *ff, const float *ffp, float ry, float rdy, float ryp, float rdyp) {
+        const float2 r01 = make_float2(ry, rdy), p01 = make_float2(ryp, rdyp);
+        const float2 A = __fmul2_rn(make_float2(wa, wa), r01), Bq = __fmul2_rn(make_float2(dx, dx), r01);
+        const float2 PA = __fmul2_rn(make_float2(wap, wap), p01), PB = __fmul2_rn(make_float2(wbp, wbp), p01);
+        const float2 f01 = make_float2(ff[0], ff[1]), fp01 = make_float2(ffp[0], ffp[1]);
         __syncwarp();
         if (last) {
             float2 *t0 = acc_tq(c, 0, kc), *t1 = acc_tq(c, 1, kc);
             float *u0 = acc_u(c, 0, kc), *u1 = acc_u(c, 1, kc);
-            float2 v0 = *t0, v1 = *t1;
-            v0.x = fmaf(a0, ff[0], fmaf(pa0, ffp[0], v0.x));
-            v0.y = fmaf(a0, ff[1], fmaf(pa0, ffp[1], v0.y));
-            v1.x = fmaf(a1, ff[0], fmaf(pa1, ffp[0], v1.x));
-            v1.y = fmaf(a1, ff[1], fmaf(pa1, ffp[1], v1.y));
-            *u0 = fmaf(a0, ff[2], fmaf(pa0, ffp[2], *u0));
-            *u1 = fmaf(a1, ff[2], fmaf(pa1, ffp[2], *u1));
-            *t0 = v0;
-            *t1 = v1;
+            const float2 v0 = *t0, v1 = *t1;
+            *u0 = fmaf(A.x, ff[2], fmaf(PA.x, ffp[2], *u0));
+            *u1 = fmaf(A.y, ff[2], fmaf(PA.y, ffp[2], *u1));
+            *t0 = __ffma2_rn(make_float2(A.x, A.x), f01, __ffma2_rn(make_float2(PA.x, PA.x), fp01, v0));
+            *t1 = __ffma2_rn(make_float2(A.y, A.y), f01, __ffma2_rn(make_float2(PA.y, PA.y), fp01, v1));
         }
         __syncwarp();
         if (last) {
             float2 *t0 = acc_tq(c, 0, kc + 1), *t1 = acc_tq(c, 1, kc + 1);
             float *u0 = acc_u(c, 0, kc + 1), *u1 = acc_u(c, 1, kc + 1);
-            float2 v0 = *t0, v1 = *t1;
-            v0.x = fmaf(b0, ff[0], fmaf(pb0, ffp[0], v0.x));
-            v0.y = fmaf(b0, ff[1], fmaf(pb0, ffp[1], v0.y));
-            v1.x = fmaf(b1, ff[0], fmaf(pb1, ffp[0], v1.x));
-            v1.y = fmaf(b1, ff[1], fmaf(pb1, ffp[1], v1.y));
-            *u0 = fmaf(b0, ff[2], fmaf(pb0, ffp[2], *u0));
-            *u1 = fmaf(b1, ff[2], fmaf(pb1, ffp[2], *u1));
-            *t0 = v0;
-            *t1 = v1;
+            const float2 v0 = *t0, v1 = *t1;
+            *u0 = fmaf(Bq.x, ff[2], fmaf(PB.x, ffp[2], *u0));
+            *u1 = fmaf(Bq.y, ff[2], fmaf(PB.y, ffp[2], *u1));
+            *t0 = __ffma2_rn(make_float2(Bq.x, Bq.x), f01, __ffma2_rn(make_float2(PB.x, PB.x), fp01, v0));
+            *t1 = __ffma2_rn(make_float2(Bq.y, Bq.y), f01, __ffma2_rn(make_float2(PB.y, PB.y), fp01, v1));
         }
     };
     if (!r3) {
