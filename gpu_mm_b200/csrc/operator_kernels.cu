@@ -1183,8 +1183,7 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
                      const uint32_t *__restrict__ cellmap, const uint64_t *__restrict__ band)
 {
     extern __shared__ __align__(16) float s_lines[];   // [BW][BP][4 rows][32] (y, x, alpha, TOD), then accumulators
-    __shared__ uint32_t s_wline[BW][64], s_wkey[BW][64];
-    __shared__ uint64_t s_wbw[BW][64];
+    __shared__ uint4 s_wp[BW][64];   // per entry: line, key, band word (low, high)
     __shared__ uint32_t s_err[BW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t nw = (int64_t) gridDim.x * BW;
@@ -1219,28 +1218,36 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
 
     // The warp's decoded owner entries, two groups of 32 in turn: entry q at [q & 63].  Lines >=
     // nlines (a plan that does not belong to this xpointing) are flagged and skipped (0xffffffff).
-    uint32_t *wline = s_wline[warp], *wkey = s_wkey[warp];
-    uint64_t *wbw = s_wbw[warp];
+    uint4 *wp = s_wp[warp];
+    // The raw owner and band words of group g (this lane's entry), loaded one group before they are
+    // decoded, so that their memory latency is hidden behind a group of lines.
+    uint64_t raw_w = 0ull, raw_bw = 0ull;
+    auto load_raw = [&](int g) {
+        const int q = 32 * g + lane;
+        raw_w = (q < nq) ? __ldg(owner_mt + e0 + q) : 0ull;
+        raw_bw = (q < nq) ? __ldg(band + e0 + q) : 0ull;
+    };
     auto decode = [&](int g) {
         const int q = 32 * g + lane;
-        const uint64_t w = (q < nq) ? __ldg(owner_mt + e0 + q) : 0ull;
-        const uint64_t bw = (q < nq) ? __ldg(band + e0 + q) : 0ull;
+        const uint64_t w = raw_w, bw = raw_bw;
         uint32_t line = (q < nq) ? (uint32_t) ((w >> 20) & kClMask) : 0xffffffffu;
         if ((q < nq) && (line >= nlines)) {
             err |= kErrInconsistentNmt;
             line = 0xffffffffu;
         }
-        wline[q & 63] = line;
-        wkey[q & 63] = (uint32_t) (w & kCellMask) | ((uint32_t) ((w >> kBandShift) & 63u) << 20);
-        wbw[q & 63] = bw;
+        wp[q & 63] = make_uint4(line, (uint32_t) (w & kCellMask) | ((uint32_t) ((w >> kBandShift) & 63u) << 20),
+                                (uint32_t) bw, (uint32_t) (bw >> 32));
     };
+    load_raw(0);
     decode(0);
+    load_raw(1);
     decode(1);
+    load_raw(2);
     __syncwarp();
 
     // Starts the copy of entry q's line into its ring slot (always commits one group, maybe empty).
     auto issue = [&](int q) {
-        const uint32_t line = wline[q & 63];   // decoded (0xffffffff past the range's end)
+        const uint32_t line = wp[q & 63].x;   // decoded (0xffffffff past the range's end)
         if (line != 0xffffffffu)
             cp_async16(ring + (q & (BP - 1)) * 128 + 32 * row + piece, src_row + (size_t) (32u * line + piece));
         cp_async_commit();
@@ -1251,18 +1258,21 @@ planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t no
         issue(q);
 #pragma unroll 1
     for (int q0 = 0; q0 < nq; q0 += 32) {
-        if (q0 > 0)
+        if (q0 > 0) {
             decode((q0 >> 5) + 1);     // over the group before q0's, which no one reads any more
+            load_raw((q0 >> 5) + 2);
+        }
         const int qe = min(q0 + 32, nq);
 #pragma unroll 1
         for (int q = q0; q < qe; q++) {
             issue(q + BP - 1);         // into the slot of line q - 1, released at the end of that step
             cp_async_wait<BP - 1>();   // this lane's piece of line q has landed
             __syncwarp();
-            const uint32_t line = wline[q & 63];
+            const uint4 pw = wp[q & 63];
+            const uint32_t line = pw.x;
             if (line != 0xffffffffu) {
-                const uint32_t key = wkey[q & 63];
-                const uint64_t bw = wbw[q & 63];
+                const uint32_t key = pw.y;
+                const uint64_t bw = (uint64_t) pw.z | ((uint64_t) pw.w << 32);
                 const float *slot = ring + (q & (BP - 1)) * 128;
                 const float y = slot[lane], x = slot[32 + lane], al = slot[64 + lane], tv = slot[96 + lane];
                 const uint32_t s = (line << 5) + (uint32_t) lane;
