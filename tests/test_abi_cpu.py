@@ -151,8 +151,8 @@ def test_pybind_surface_has_reference_names():
 
 
 def test_drop_in_import_names():
-    """The reference's import names resolve to this build (SURVEY boundary: the module must import as
-    gpu_mm.gpu_mm_pybind11)."""
+    """The reference's import names resolve to this build: a caller of the reference writes
+    `import gpu_mm` and `from gpu_mm import gpu_mm_pybind11`, unchanged."""
     import importlib
     import gpu_mm_b200
     gm = importlib.import_module("gpu_mm")
