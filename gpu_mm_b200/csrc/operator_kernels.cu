@@ -845,11 +845,19 @@ planned_map2tod_v4(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nown
 // of the one being processed, so a warp keeps BP - 1 lines of memory traffic in flight while it
 // works without holding registers for them.
 
-constexpr int BW = 16;                 // warps per CTA (2 CTAs per SM: 32 warps, 55 registers each)
-constexpr int BNT = BW * 32;
-constexpr int BP = 4;                  // line slots per warp (a power of two; 8 with 12 warps measured 0.7 % slower)
 constexpr int kBandRows = 3;          // accumulator rows R0 .. R0 + 2
-constexpr size_t kBandSmem = (size_t) BW * BP * 128 * sizeof(float) + (size_t) BW * 3 * kBandRows * 96 * sizeof(float);
+
+// Geometry per flush mode: BW warps per CTA (2 CTAs per SM), BP line slots per warp (a power of
+// two).  16 warps with 4 slots (32 warps per SM) measured fastest for the float, float64 and hot-cell
+// flushes; the compensated flush waits on returning atomics at every flush, and its shorter warp
+// slices at 16 warps (more flushes per line) made it 9-11 % slower than 12 warps with 8 slots.
+template<int FLUSH>
+struct BandGeo {
+    static constexpr int BW = (FLUSH == kFlushCompensated) ? 12 : 16;
+    static constexpr int BP = (FLUSH == kFlushCompensated) ? 8 : 4;
+    static constexpr int BNT = BW * 32;
+    static constexpr size_t kSmem = (size_t) BW * BP * 128 * sizeof(float) + (size_t) BW * 3 * kBandRows * 96 * sizeof(float);
+};
 constexpr uint32_t kNoKey = 0xffffffffu;
 
 struct BandState {
@@ -1178,10 +1186,11 @@ __device__ __forceinline__ void band_general_sample(const OpArgs &a, float y, fl
 
 
 template<bool RESP, bool PERIODIC, int FLUSH>
-__global__ void __launch_bounds__(BNT, 2)
+__global__ void __launch_bounds__(BandGeo<FLUSH>::BNT, 2)
 planned_tod2map_band(OpArgs a, const uint64_t *__restrict__ owner_mt, int64_t nowner,
                      const uint32_t *__restrict__ cellmap, const uint64_t *__restrict__ band)
 {
+    constexpr int BW = BandGeo<FLUSH>::BW, BP = BandGeo<FLUSH>::BP;
     extern __shared__ __align__(16) float s_lines[];   // [BW][BP][4 rows][32] (y, x, alpha, TOD), then accumulators
     __shared__ uint4 s_wp[BW][64];   // per entry: line, key, band word (low, high)
     __shared__ uint32_t s_err[BW];
@@ -1548,13 +1557,14 @@ cudaError_t launch_tod2map_band_impl(const OpArgs &a, const uint64_t *owner_mt, 
                                      const uint32_t *cellmap, const uint64_t *band, cudaStream_t stream)
 {
     static std::atomic<uint64_t> attr_done{0};
-    cudaError_t e = set_smem_limit(planned_tod2map_band<RESP, PERIODIC, FLUSH>, kBandSmem, attr_done);
+    using Geo = BandGeo<FLUSH>;
+    cudaError_t e = set_smem_limit(planned_tod2map_band<RESP, PERIODIC, FLUSH>, Geo::kSmem, attr_done);
     if (e != cudaSuccess)
         return e;
     const int per_sm = (a.ctas_per_sm > 0) ? a.ctas_per_sm : 2;
-    int64_t g = (nowner + 32 * BW - 1) / (32 * BW);
+    int64_t g = (nowner + 32 * Geo::BW - 1) / (32 * Geo::BW);
     g = std::max<int64_t>(1, std::min<int64_t>(g, (int64_t) per_sm * device_sm_count()));
-    planned_tod2map_band<RESP, PERIODIC, FLUSH><<<(unsigned) g, BNT, kBandSmem, stream>>>(a, owner_mt, nowner, cellmap,
+    planned_tod2map_band<RESP, PERIODIC, FLUSH><<<(unsigned) g, Geo::BNT, Geo::kSmem, stream>>>(a, owner_mt, nowner, cellmap,
                                                                                          band);
     return cudaGetLastError();
 }
