@@ -849,8 +849,9 @@ constexpr int kBandRows = 3;          // accumulator rows R0 .. R0 + 2
 
 // Geometry per flush mode: BW warps per CTA (2 CTAs per SM), BP line slots per warp (a power of
 // two).  16 warps with 4 slots (32 warps per SM) measured fastest for the float, float64 and hot-cell
-// flushes; the compensated flush waits on returning atomics at every flush, and its shorter warp
-// slices at 16 warps (more flushes per line) made it 9-11 % slower than 12 warps with 8 slots.
+// flushes.  The compensated flush waits on returning atomics at every flush and needs 80 registers:
+// at 16 warps (64 registers at most, and shorter warp slices, so more flushes per line) it measured
+// 9-11 % slower than with 12 warps and 8 slots.
 template<int FLUSH>
 struct BandGeo {
     static constexpr int BW = (FLUSH == kFlushCompensated) ? 12 : 16;
