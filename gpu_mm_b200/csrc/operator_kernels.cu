@@ -293,6 +293,44 @@ __device__ __forceinline__ float global_eval(const OpArgs &a, const float *__res
     return pol_eval<RESP>(ct, cq, cu, t, q, u);
 }
 
+// Local-map offsets (plane T) of a located sample's four neighbours, in the order (iy0, ix0),
+// (iy0, ix1), (iy1, ix0), (iy1, ix1), or -1 where a neighbour is outside the map or in an absent
+// cell: global_pixel_offset of each, with one cell_offsets lookup when all four lie in one cell and
+// ix1 = ix0 + 1 (every footprint except those on a cell edge or across the x wrap-around).
+__device__ __forceinline__ void neighbour_offsets(const Located &L, const OpArgs &a, int64_t off[4])
+{
+    const int cy = L.iy0 >> 6, cx = L.ix0 >> 6;
+    if (((L.iy1 >> 6) == cy) && ((L.ix1 >> 6) == cx) && (L.ix1 == L.ix0 + 1)) {
+        int64_t base = -1;
+        if ((cy < a.nycells) && (cx < a.nxcells))
+            base = __ldg(a.cell_offsets + (int64_t) cy * a.nxcells + cx);
+        const int64_t o = base + (int64_t) (L.iy0 & 63) * a.ystride + (L.ix0 & 63);
+        const bool in = base >= 0;
+        off[0] = in ? o : -1;
+        off[1] = in ? o + 1 : -1;
+        off[2] = in ? o + a.ystride : -1;
+        off[3] = in ? o + a.ystride + 1 : -1;
+    } else {
+        off[0] = global_pixel_offset(L.iy0, L.ix0, a);
+        off[1] = global_pixel_offset(L.iy0, L.ix1, a);
+        off[2] = global_pixel_offset(L.iy1, L.ix0, a);
+        off[3] = global_pixel_offset(L.iy1, L.ix1, a);
+    }
+}
+
+// global_eval without a response at a neighbour offset from neighbour_offsets (the same loads,
+// error bit and arithmetic).
+__device__ __forceinline__ float eval_at(const OpArgs &a, const float *__restrict__ lmap, int64_t off, float cq,
+                                         float cu, uint32_t &err)
+{
+    const bool valid = off >= 0;
+    const float t = valid ? __ldg(lmap + off) : 0.0f;
+    const float q = valid ? __ldg(lmap + off + a.polstride) : 0.0f;
+    const float u = valid ? __ldg(lmap + off + 2 * a.polstride) : 0.0f;
+    err |= (valid || a.partial) ? 0u : kErrNotInPixelization;
+    return pol_eval<false>(1.0f, cq, cu, t, q, u);
+}
+
 template<int FLUSH = kFlushF32>
 __device__ __forceinline__ void global_accum(const OpArgs &a, float *__restrict__ lmap, int iy, int ix,
                                              float t, float q, float u, float w, uint32_t &err)
@@ -1396,9 +1434,9 @@ __device__ __forceinline__ void unplanned_t2m_line(const OpArgs &a, bool valid, 
     }
     if (snext)
         return;   // not the last sample of its column: the last one adds this one's share
-    const int64_t o00 = global_pixel_offset(L.iy0, L.ix0, a), o01 = global_pixel_offset(L.iy0, L.ix1, a);
-    const int64_t o10 = global_pixel_offset(L.iy1, L.ix0, a), o11 = global_pixel_offset(L.iy1, L.ix1, a);
-    const int64_t o[4] = {o00, o10, o01, o11};
+    int64_t nb[4];
+    neighbour_offsets(L, a, nb);
+    const int64_t o[4] = {nb[0], nb[2], nb[1], nb[3]};   // (iy0, ix0), (iy1, ix0), (iy0, ix1), (iy1, ix1)
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         if (o[c] >= 0) {
@@ -1483,10 +1521,12 @@ unplanned_map2tod_kernel(OpArgs a)
             err |= locate(y[k], x[k], a.ny, a.nx, a.periodic, L);
             float sn, cs;
             sincos2a(al[k], &sn, &cs);
-            const float e00 = global_eval(a, a.in, L.iy0, L.ix0, 1.0f, cs, sn, err);
-            const float e01 = global_eval(a, a.in, L.iy0, L.ix1, 1.0f, cs, sn, err);
-            const float e10 = global_eval(a, a.in, L.iy1, L.ix0, 1.0f, cs, sn, err);
-            const float e11 = global_eval(a, a.in, L.iy1, L.ix1, 1.0f, cs, sn, err);
+            int64_t off[4];
+            neighbour_offsets(L, a, off);
+            const float e00 = eval_at(a, a.in, off[0], cs, sn, err);
+            const float e01 = eval_at(a, a.in, off[1], cs, sn, err);
+            const float e10 = eval_at(a, a.in, off[2], cs, sn, err);
+            const float e11 = eval_at(a, a.in, off[3], cs, sn, err);
             const float rr = bilinear(L.dy, L.dx, e00, e01, e10, e11);
             r[k] = a.accum ? (tv[k] + rr) : rr;
         }
