@@ -104,9 +104,10 @@ int gmm_get_sort_digit_bits(void);
  * atomic per sample and pixel); here there are two, which give the same result within float
  * rounding:
  *   GMM_TOD2MAP_BANDS (default): lines grouped by (cell, row band) in the plan; each warp sums a
- *     band's lines in registers and adds them to the map once per band;
- *   GMM_TOD2MAP_TILES: shared-memory tile of each cell plus halo, as the precision modes and
- *     batches use.
+ *     band's lines in its own shared-memory accumulator and adds them to the map once per band
+ *     (every flush mode);
+ *   GMM_TOD2MAP_TILES: shared-memory tile of each cell plus halo, as batches use (and single-TOD
+ *     calls whose xpointing or TOD is not 16-byte aligned).
  * A tuning knob: the bands kernel is faster for raster scans, the tiles kernel for pointing that
  * is not (e.g. scans faster than one pixel per sample or rotated against the pixel grid). */
 #define GMM_TOD2MAP_BANDS 0
