@@ -74,6 +74,14 @@ __device__ __forceinline__ int count_line_cells(float y, float x, int ny, int nx
     const uint32_t e = locate(y, x, ny, nx, periodic, L);
     const int cy0 = L.iy0 >> 6, cy1 = L.iy1 >> 6;            // iy1 >= iy0
     const int cx0 = L.ix0 >> 6, cx1 = L.ix1 >> 6;            // cx1 < cx0 when x wraps
+    // Most lines lie in one cell (a line is 32 samples, a cell 64 pixels wide): one pair, found with
+    // a shuffle and a vote, as analyse_line does.
+    const int c = (cy0 << 10) | cx0;
+    const int c0 = __shfl_sync(kFullMask, c, 0);   // every lane takes part, before any short cut
+    if (__all_sync(kFullMask, (cy0 == cy1) && (cx0 == cx1) && (c == c0))) {
+        err |= e;
+        return 1;
+    }
     const int rmin = __reduce_min_sync(kFullMask, cy0);
     const int rmax = __reduce_max_sync(kFullMask, cy1);
     const int cmin = __reduce_min_sync(kFullMask, min(cx0, cx1));
