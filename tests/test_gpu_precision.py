@@ -130,7 +130,7 @@ def test_precision_argument_checks(g):
 def test_precision_modes_full_size_high_hit(g):
     """The high-hit precision workload at its full size: 64 detectors x 2^22 samples (2^28) confined to
     the 512x512 box [256, 768)^2 of a 3x1024x1024 map (~1000 hits/pixel), tod = 1e3 + N(0,1), against
-    the FP64 oracle over the whole TOD.  Bars: the north star's 1e-5 max relative error for the float
+    the FP64 oracle over the whole TOD.  Bars: a 1e-5 max relative error for the float
     path (both tod2map kernels); 1e-6 max and 2e-7 rms for the compensated and float64-map modes on
     both kernels, with float partials of at most 32 lines (max_run_lines)."""
     import ctypes
